@@ -1,0 +1,185 @@
+/*
+ * tipt.h -- C ABI of the B200 lattice Langevin stepper (libtipt.so).
+ *
+ * Drop-in replacement for the numba hot path of
+ *   R: simulation/latticeSimeRescale_numba.py   (real scalar field)
+ *   C: simulation/latticeSimComplex_numba.py    (complex field, U(1) / Z_N)
+ * Each entry point names the reference function it replaces (file:line).
+ *
+ * Conventions
+ *  - Arrays are C-order (nx, ny, nz) device buffers, site = i*ny*nz + j*nz + k,
+ *    periodic in all three directions; nz = 1 (or ny = nz = 1) gives the 2-D
+ *    (1-D) lattice exactly as the reference's 7-point stencil degenerates.
+ *  - State storage (`storage`): TIPT_F64 = double; TIPT_F32 = float with the
+ *    reference's mixed FP32-storage / FP64-arithmetic semantics; TIPT_F32C =
+ *    float2 {hi, lo} pairs per site (value hi + lo, compensated updates).
+ *  - The reference updates phi, pi in place through scratch phi_tmp, pi_tmp.
+ *    The fused kernels here read (phi, pi) and write (phi_out, pi_out), which
+ *    must not overlap the inputs (ping-pong); the Python host restores the
+ *    in-place semantics by swapping the storages.
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  No entry point
+ *    allocates device memory, synchronises the device or reads device memory on
+ *    the host; all are capturable into CUDA graphs.  Scratch is caller-owned.
+ *  - Every entry returns a tipt_status; tipt_last_error() gives the detail.
+ */
+#ifndef TIPT_H
+#define TIPT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum {
+    TIPT_OK = 0,
+    TIPT_ERR_ARG = 1,         /* null pointer, bad size, aliasing, bad enum */
+    TIPT_ERR_STORAGE = 2,     /* storage not supported by this entry point */
+    TIPT_ERR_ALIGN = 3,       /* pointer not aligned to its element size */
+    TIPT_ERR_CUDA = 4,        /* a CUDA launch or runtime call failed */
+    TIPT_ERR_UNSUPPORTED = 5, /* a mode or size this build does not handle */
+    TIPT_ERR_TIMEOUT = 6      /* a bounded device-side wait ran out */
+} tipt_status;
+
+enum { TIPT_F64 = 0, TIPT_F32 = 1, TIPT_F32C = 2 };
+
+/* V' sources (R:805-849 build_vprime_table, lookup R:1923-1930). */
+enum {
+    TIPT_VP_TABLE = 0,   /* 1-D uniform FP64 table: table[npts] */
+    TIPT_VP_TABLE2D = 1, /* 2-D FP64 table [nT][npts]; rows blended at T, then lerped in phi */
+    TIPT_VP_POLY = 2     /* V'(x) = c1 x + c2 x^2 + c3 x^3 (zero-coupling inline V', R:2228) */
+};
+
+typedef struct {
+    int32_t kind;          /* TIPT_VP_* */
+    int32_t npts;          /* table points along phi (>= 2) */
+    const double* table;   /* device pointer */
+    double tmin, dinv;     /* phi origin and 1/spacing (R:849) */
+    int32_t nT;            /* 2-D: rows along T (>= 2) */
+    int32_t pad_;
+    double T_min, T_dinv;  /* 2-D: T origin and 1/spacing */
+    double T;              /* 2-D: temperature at which rows are blended */
+    double c1, c2, c3;     /* polynomial coefficients */
+} tipt_vsource;
+
+/* Per-step scalars of the host loop (R:3674-3768): dt, dx, eta_eff, mu and
+ * inv_a2 as passed to rk2_step_table; noise_scale = ns of R:3714-3718 for the
+ * inline hash noise (kick ns*z per midpoint step, 0.5*ns*z per half step);
+ * noise_step = the step counter n used as the hash's step (R:3742);
+ * noise_seed = 0 reproduces the reference key exactly. */
+typedef struct {
+    double dt, dx, eta_eff, mu, inv_a2;
+    double noise_scale;
+    uint64_t noise_step;
+    uint64_t noise_seed;
+} tipt_step_params;
+
+/* Symmetry-breaking terms of the complex field.  zn_*: the reference's
+ * _ZN_PARAMS = [N, delta_V, active] (C:226-231, force C:2137-2158).
+ * eps4: eps * Re(Phi^4) (no reference counterpart). */
+typedef struct {
+    double zn_n, zn_dv, zn_active;
+    double eps4;
+} tipt_complex_terms;
+
+const char* tipt_version(void);
+const char* tipt_status_string(int status);
+/* Detail of the last failing call on this host thread. */
+const char* tipt_last_error(void);
+
+/* ----------------------------------------------------------------- noise */
+
+/* _hash_rng_pair (R:2322-2336, C:2747-2761) plus the Box-Muller z of
+ * R:2519-2521 for n device-resident keys.  u1, u2, z are device arrays; any
+ * of them may be NULL. */
+int tipt_hash_rng_pair(const uint64_t* keys, int64_t n, double* u1, double* u2, double* z,
+                       void* stream);
+
+/* Counter-based replacement of generate_noise_field (R:1348-1361), whose
+ * per-thread MT19937 stream is not reproducible: out[site] = scale * z with
+ * z from key(site, step, mul, seed) (R:2511-2520 seeding).  component 0 = the
+ * cos branch, 1 = the sin branch (C:2968-2970).  out_storage: TIPT_F64 or
+ * TIPT_F32. */
+int tipt_generate_noise_field(int out_storage, void* out, int64_t nx, int64_t ny, int64_t nz,
+                              double scale, uint64_t step, uint64_t mul, uint64_t seed,
+                              int component, void* stream);
+
+/* ------------------------------------------------------------ real field */
+
+/* rk2_step_table (R:1875-1966), the reference default integrator
+ * (rk2_nonfused, R:301-303): one midpoint RK2 step of size dt,
+ *   k = inv_a2*lap(phi) - eta_eff*pi - V'(phi)/mu^2,
+ *   phi~ = phi + dt/2 pi, pi~ = pi + dt/2 k(phi, pi),
+ *   phi' = phi + dt pi~, pi' = pi + dt k(phi~, pi~) + noise,
+ * fused into one launch.  noise: a device array in the state precision
+ * (double for F64 and F32C, float for F32) as the reference passes it, or
+ * NULL for inline hash noise noise_scale * z(site, noise_step, 73856093,
+ * noise_seed). */
+int tipt_rk2_step_table(int storage, const void* phi, const void* pi, void* phi_out,
+                        void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                        const tipt_step_params* sp, const tipt_vsource* vp, const void* noise,
+                        void* stream);
+
+/* rk2_fused_table (R:1708-1872): two dt/2 midpoint halves, the first with
+ * vp_T, the second with vp_Tm; array noise adds 0.5*noise in each half
+ * (R:1806, R:1872).  With noise == NULL the halves use the inline hash of
+ * rk2_fused_single_pass: 0.5*ns*z at multiplier 73856093, then 19349669
+ * (R:2511-2522, R:2636-2647).  mid_phi / mid_pi hold the state between the
+ * halves (the reference's phi_tmp / pi_tmp). */
+int tipt_rk2_fused_table(int storage, const void* phi, const void* pi, void* phi_out,
+                         void* pi_out, void* mid_phi, void* mid_pi, int64_t nx, int64_t ny,
+                         int64_t nz, const tipt_step_params* sp, const tipt_vsource* vp_T,
+                         const tipt_vsource* vp_Tm, const void* noise, void* stream);
+
+/* --------------------------------------------------------- complex field */
+
+/* Complex rk2_step_table (C:2067-2215): the real step for Phi = phi1 + i phi2
+ * with V'(rho) from vp (rho = |Phi|), projected onto the components
+ * (C:2137-2139), plus the terms in ct.  Array noise: noise1 / noise2 as the
+ * reference passes them; NULL: one hash pair per site, z1 = r cos -> pi1,
+ * z2 = r sin -> pi2 (C:2958-2974). */
+int tipt_complex_rk2_step_table(int storage, const void* phi1, const void* phi2,
+                                const void* pi1, const void* pi2, void* phi1_out,
+                                void* phi2_out, void* pi1_out, void* pi2_out, int64_t nx,
+                                int64_t ny, int64_t nz, const tipt_step_params* sp,
+                                const tipt_vsource* vp, const tipt_complex_terms* ct,
+                                const void* noise1, const void* noise2, void* stream);
+
+/* compute_winding_number (C:2683-2744; tools/winding.py:15-64) on the FP64
+ * value of the stored fields (the reference casts to FP64, C:4627-4629).
+ * Outputs (each may be NULL):
+ *   w_site[N] float   -- sum over the XY, XZ, YZ plaquettes anchored at the
+ *                         site, each plaquette's integer winding (the
+ *                         reference's float value rounded),
+ *   w3[3][N] int8     -- per-orientation integer windings (XY, XZ, YZ),
+ *   pierced[cap] uint32 -- compacted list of pierced plaquettes, entry =
+ *                         site*3 + orientation, in no particular order,
+ *   counts[5] int64   -- device: pierced XY, XZ, YZ; sites with |w| > 0.5
+ *                         (the reference string count, C:4661); list length
+ *                         written (<= cap).  Zeroed by the call. */
+int tipt_compute_winding_number(int storage, const void* phi1, const void* phi2, int64_t nx,
+                                int64_t ny, int64_t nz, float* w_site, int8_t* w3,
+                                uint32_t* pierced, int64_t pierced_cap, int64_t* counts,
+                                void* stream);
+
+/* ----------------------------------------------------------- observables */
+
+/* compute_energy_densities (R:2270-2319) plus the host loop's per-step
+ * reductions (phi.min/max R:3655-3660, NaN guard R:3882-3944) and the
+ * converted fraction: out[10] (device, double) = E_kin, E_grad, E_pot,
+ * <phi>, <phi^2>, <pi^2>, fraction(phi > thr), min phi, max phi,
+ * non-finite count.  FP64 accumulation in a fixed order (deterministic for
+ * given sizes).  workspace: caller-owned device memory of
+ * tipt_observables_workspace_size(nx, ny, nz) bytes.  pi may be NULL. */
+int64_t tipt_observables_workspace_size(int64_t nx, int64_t ny, int64_t nz);
+int tipt_observables(int storage, const void* phi, const void* pi, int64_t nx, int64_t ny,
+                     int64_t nz, double dx, double inv_a2, double lam, double mphi, double mu,
+                     double thr, double* out, void* workspace, int64_t workspace_bytes,
+                     void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TIPT_H */

@@ -1,0 +1,437 @@
+"""GPU parity: the CUDA kernels (through the C ABI) against the reference's golden
+fixtures and the CPU oracle on the same seeded inputs.
+
+Tolerances: FP64 storage 1e-14 absolute after one step and 1e-12 relative to the
+field scale after ten (the reference is fastmath numba: FMA contraction and
+reassociation rule out bitwise equality); reference-FP32 storage 2e-6 absolute
+(store-rounding flips); FP32-compensated storage 2e-6 relative to the FP64 oracle
+(forces are FP32, state updates FP64-accurate)."""
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+from oracle import oracle as O  # noqa: E402
+from thermal_inflation_phase_transition_b200 import _lib as L  # noqa: E402
+from thermal_inflation_phase_transition_b200 import complex_field as CF  # noqa: E402
+from thermal_inflation_phase_transition_b200 import real_field as RF  # noqa: E402
+from thermal_inflation_phase_transition_b200.observables import observables  # noqa: E402
+
+CASES = ("2d", "3d", "odd")
+DEV = "cuda"
+
+
+def cu(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    return (t.to(dtype) if dtype is not None else t).to(DEV)
+
+
+def as_state(a, storage):
+    """numpy float64/float32 field -> CUDA tensor in the requested storage."""
+    if storage == "f64":
+        return cu(np.asarray(a, np.float64))
+    if storage == "f32":
+        return cu(np.asarray(a, np.float32))
+    return RF.to_f32c(cu(np.asarray(a, np.float64)))
+
+
+def to_np(t):
+    if t.dim() == 4:
+        return RF.from_f32c(t).cpu().numpy()
+    return t.double().cpu().numpy()
+
+
+# ---------------------------------------------------------------- noise --
+def test_hash_pairs_bit_exact(golden):
+    g = golden("hash_pairs.npz")
+    keys = cu(g["seeds"].view(np.int64))
+    u1, u2, z = RF.hash_rng_pair(keys)
+    torch.cuda.synchronize()
+    assert np.array_equal(u1.cpu().numpy(), g["u1"])
+    assert np.array_equal(u2.cpu().numpy(), g["u2"])
+    zz = z.cpu().numpy()
+    # z = sqrt(-2 ln u1) cos(2 pi u2) in FP64: CUDA's log/cos are within 1-2 ulp
+    # of glibc's, so z agrees bit for bit on most keys and within 4 ulp on all
+    ulp = np.spacing(np.abs(g["z_cos"]))
+    err = np.abs(zz - g["z_cos"]) / ulp
+    assert err.max() <= 4, err.max()
+    assert np.mean(err == 0) > 0.5
+    # float32 rounding of z agrees except on rounding-boundary keys
+    assert np.mean(zz.astype(np.float32) == g["z_cos"].astype(np.float32)) > 0.999
+
+
+@pytest.mark.parametrize("shape", [(17, 9, 5), (32, 24, 1), (64, 64, 64)])
+@pytest.mark.parametrize("component", [0, 1])
+def test_noise_field(shape, component):
+    out = torch.empty(shape, dtype=torch.float64, device=DEV)
+    RF.generate_noise_field(out, 0.7, 123, mul=RF.K_PASS4, hash_seed=5, component=component)
+    ref = O.noise_field(shape, 123, O.K_PASS4, 5, 0.7, component)
+    got = out.cpu().numpy()
+    np.testing.assert_allclose(got, ref, rtol=4e-15, atol=4e-15)
+    # statistics of the field: unit-variance Gaussian scaled by 0.7
+    if got.size > 100000:
+        assert abs(got.std() / 0.7 - 1) < 0.01 and abs(got.mean()) < 0.01
+
+
+def test_noise_f32_field():
+    out = torch.empty((8, 8, 8), dtype=torch.float32, device=DEV)
+    RF.generate_noise_field(out, 1.0, 9)
+    ref = O.noise_field((8, 8, 8), 9, O.K_PASS2, 0, 1.0, 0).astype(np.float32)
+    assert np.mean(out.cpu().numpy() == ref) > 0.99
+
+
+# ------------------------------------------------------- real midpoint ---
+def _gpu_step_table(g, tag, storage, nsteps, hash_noise=True):
+    dn = "f32" if storage == "f32" else "f64"
+    phi = as_state(g[f"{tag}_{dn}_phi0"], storage)
+    pi = as_state(g[f"{tag}_{dn}_pi0"], storage)
+    ptmp, vtmp = torch.empty_like(phi), torch.empty_like(pi)
+    tab = cu(g["table"])
+    for n in range(nsteps):
+        noise = None
+        if not hash_noise:
+            nf = O.noise_field(phi.shape[:3], n, scale=float(g["ns"]))
+            noise = cu(nf.astype(np.float32 if storage == "f32" else np.float64))
+        RF.rk2_step_table(phi, pi, float(g["dt"]), float(g["dx"]), float(g["eta"]),
+                          float(g["mu"]), noise, ptmp, vtmp, float(g["inv_a2"]), tab,
+                          float(g["tmin"]), float(g["dinv"]), int(g["npts"]),
+                          noise_scale=float(g["ns"]), noise_step=n)
+    torch.cuda.synchronize()
+    return to_np(phi), to_np(pi)
+
+
+@pytest.mark.parametrize("tag", CASES)
+@pytest.mark.parametrize("hash_noise", [True, False])
+def test_rk2_step_table_f64_vs_reference(golden, tag, hash_noise):
+    g = golden("rk2_step_table.npz")
+    phi, pi = _gpu_step_table(g, tag, "f64", 1, hash_noise)
+    np.testing.assert_allclose(phi, g[f"{tag}_f64_phi1"], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(pi, g[f"{tag}_f64_pi1"], rtol=0, atol=1e-14)
+    phi, pi = _gpu_step_table(g, tag, "f64", 10, hash_noise)
+    assert np.abs(phi - g[f"{tag}_f64_phi10"]).max() <= 1e-12 * np.abs(g[f"{tag}_f64_phi10"]).max()
+    assert np.abs(pi - g[f"{tag}_f64_pi10"]).max() <= 1e-12 * np.abs(g[f"{tag}_f64_pi10"]).max()
+
+
+@pytest.mark.parametrize("tag", CASES)
+def test_rk2_step_table_f32_vs_reference(golden, tag):
+    g = golden("rk2_step_table.npz")
+    phi, pi = _gpu_step_table(g, tag, "f32", 10, hash_noise=False)
+    np.testing.assert_allclose(phi, g[f"{tag}_f32_phi10"], rtol=0, atol=2e-6)
+    np.testing.assert_allclose(pi, g[f"{tag}_f32_pi10"], rtol=0, atol=2e-6)
+
+
+@pytest.mark.parametrize("tag", CASES)
+def test_rk2_step_table_f32c_vs_fp64(golden, tag):
+    g = golden("rk2_step_table.npz")
+    phi, pi = _gpu_step_table(g, tag, "f32c", 10)
+    ref_phi, ref_pi = g[f"{tag}_f64_phi10"], g[f"{tag}_f64_pi10"]
+    assert np.abs(phi - ref_phi).max() <= 2e-6 * np.abs(ref_phi).max()
+    assert np.abs(pi - ref_pi).max() <= 2e-6 * np.abs(ref_pi).max()
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 3, 1), (5, 1, 7), (1, 1, 9), (40, 36, 34)])
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_rk2_edge_shapes_vs_oracle(shape, storage):
+    rng = np.random.default_rng(7)
+    phi0 = rng.normal(0.5, 0.6, shape)
+    pi0 = rng.normal(0.0, 0.3, shape)
+    tab, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.01), 0.0, 3.0, 1024)
+    a, b = phi0.copy(), pi0.copy()
+    tmp = [np.empty(shape), np.empty(shape)]
+    phi, pi = as_state(phi0, storage), as_state(pi0, storage)
+    pt, vt = torch.empty_like(phi), torch.empty_like(pi)
+    for n in range(3):
+        O.rk2_step_table(a, b, 0.05, 1.0, 0.9, 1.0, None, *tmp, 1.0, tab, tmin, dinv, 1024,
+                         noise_scale=0.3, noise_step=n, noise_seed=3)
+        RF.rk2_step_table(phi, pi, 0.05, 1.0, 0.9, 1.0, None, pt, vt, 1.0, cu(tab), tmin, dinv,
+                          1024, noise_scale=0.3, noise_step=n, seed=3)
+    torch.cuda.synchronize()
+    tol = 1e-13 if storage == "f64" else 2e-6
+    np.testing.assert_allclose(to_np(phi), a, rtol=0, atol=tol * max(1.0, np.abs(a).max()))
+    np.testing.assert_allclose(to_np(pi), b, rtol=0, atol=tol * max(1.0, np.abs(b).max()))
+
+
+def test_rk2_2d_table_vs_oracle():
+    shape = (24, 20, 16)
+    rng = np.random.default_rng(8)
+    phi0, pi0 = rng.normal(0.6, 0.6, shape), rng.normal(0, 0.3, shape)
+    t2, tmin, dinv, Tmin, Tdinv = O.build_table_2d(O.toy_vprime, 0.0, 3.0, 4096, 0.95, 1.10, 256)
+    T = 1.0337
+    row = O.table_blend_row(t2, Tmin, Tdinv, T)
+    a, b = phi0.copy(), pi0.copy()
+    O.rk2_step_table(a, b, 0.05, 1.0, 1.0, 1.0, None, np.empty(shape), np.empty(shape), 1.0,
+                     row, tmin, dinv, 4096, noise_scale=0.3, noise_step=4, noise_seed=1)
+    for storage, tol in (("f64", 1e-14), ("f32c", 2e-6)):
+        phi, pi = as_state(phi0, storage), as_state(pi0, storage)
+        RF.rk2_step_table(phi, pi, 0.05, 1.0, 1.0, 1.0, None, torch.empty_like(phi),
+                          torch.empty_like(pi), 1.0, cu(t2), tmin, dinv, 4096, noise_scale=0.3,
+                          noise_step=4, seed=1, vp_T=T, vp_T_min=Tmin, vp_T_dinv=Tdinv)
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(to_np(phi), a, rtol=0, atol=tol * 2)
+        np.testing.assert_allclose(to_np(pi), b, rtol=0, atol=tol * 2)
+
+
+def test_large_table_from_global_memory():
+    """The reference default of 16384 FP64 points exceeds the shared-memory
+    staging limit for FP64 and is read from global memory."""
+    shape = (16, 16, 16)
+    rng = np.random.default_rng(9)
+    phi0, pi0 = rng.normal(0.6, 0.6, shape), rng.normal(0, 0.3, shape)
+    tab, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.0), -1.0, 4.0, 16384)
+    a, b = phi0.copy(), pi0.copy()
+    O.rk2_step_table(a, b, 0.05, 1.0, 1.0, 1.0, None, np.empty(shape), np.empty(shape), 1.0, tab,
+                     tmin, dinv, 16384, noise_scale=0.2, noise_step=1)
+    phi, pi = cu(phi0), cu(pi0)
+    RF.rk2_step_table(phi, pi, 0.05, 1.0, 1.0, 1.0, None, torch.empty_like(phi),
+                      torch.empty_like(pi), 1.0, cu(tab), tmin, dinv, 16384, noise_scale=0.2,
+                      noise_step=1)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(to_np(phi), a, atol=1e-14)
+    np.testing.assert_allclose(to_np(pi), b, atol=1e-14)
+
+
+@pytest.mark.parametrize("tag", CASES)
+@pytest.mark.parametrize("storage", ["f64", "f32"])
+def test_rk2_fused_table_vs_reference(golden, tag, storage):
+    g = golden("rk2_fused_table.npz")
+    dn = storage
+    phi = as_state(g[f"{tag}_{dn}_phi0"], storage)
+    pi = as_state(g[f"{tag}_{dn}_pi0"], storage)
+    pt, vt = torch.empty_like(phi), torch.empty_like(pi)
+    for n in range(5):
+        nf = O.noise_field(phi.shape[:3], n, scale=float(g["ns"]))
+        noise = cu(nf.astype(np.float32 if storage == "f32" else np.float64))
+        RF.rk2_fused_table(phi, pi, float(g["dt"]), float(g["dx"]), float(g["eta"]),
+                           float(g["mu"]), noise, pt, vt, float(g["inv_a2"]), cu(g["table_T"]),
+                           float(g["tmin_T"]), float(g["dinv_T"]), int(g["npts_T"]),
+                           cu(g["table_Tm"]), float(g["tmin_Tm"]), float(g["dinv_Tm"]),
+                           int(g["npts_Tm"]))
+    torch.cuda.synchronize()
+    tol = 1e-13 if storage == "f64" else 2e-6
+    np.testing.assert_allclose(to_np(phi), g[f"{tag}_{dn}_phi5"], rtol=0, atol=tol)
+    np.testing.assert_allclose(to_np(pi), g[f"{tag}_{dn}_pi5"], rtol=0, atol=tol)
+
+
+@pytest.mark.parametrize("tag", CASES)
+def test_rk2_fused_single_pass_vs_reference(golden, tag):
+    """The reference's inline-hash 4-pass kernel (zero thermal couplings)."""
+    g = golden("rk2_fused_single_pass.npz")
+    phi = cu(g[f"{tag}_phi0"])
+    pi = cu(g[f"{tag}_pi0"])
+    pt, vt = torch.empty_like(phi), torch.empty_like(pi)
+    for n in range(5):
+        RF.rk2_fused_single_pass(phi, pi, float(g["dt"]), float(g["dx"]), float(g["eta"]),
+                                 float(g["T"]), float(g["T_mid"]), float(g["mu"]), float(g["lam"]),
+                                 float(g["mphi"]), 0.0, 0.0, 0.0, 0.0, 0.0, float(g["ns"]), n, pt,
+                                 vt, float(g["inv_a2"]))
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(to_np(phi), g[f"{tag}_phi5"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(to_np(pi), g[f"{tag}_pi5"], rtol=0, atol=1e-13)
+
+
+def test_in_place_semantics_and_swap():
+    shape = (8, 8, 8)
+    phi = torch.randn(shape, dtype=torch.float64, device=DEV)
+    pi = torch.randn(shape, dtype=torch.float64, device=DEV)
+    ids = (id(phi), id(pi))
+    old = phi.clone()
+    pt, vt = torch.empty_like(phi), torch.empty_like(pi)
+    tab = cu(O.build_table(lambda x: O.toy_vprime(x, 1.0), 0, 3, 64)[0])
+    RF.rk2_step_table(phi, pi, 0.05, 1, 1, 1, None, pt, vt, 1, tab, 0.0, 63 / 3, 64)
+    torch.cuda.synchronize()
+    assert (id(phi), id(pi)) == ids
+    assert torch.equal(pt, old)  # the scratch now holds the previous state
+    assert not torch.equal(phi, old)
+
+
+def test_aliasing_is_rejected():
+    phi = torch.zeros((4, 4, 4), dtype=torch.float64, device=DEV)
+    pi = torch.zeros_like(phi)
+    tab = cu(np.zeros(8))
+    with pytest.raises(L.TiptError):
+        RF.rk2_step_table(phi, pi, 0.05, 1, 1, 1, None, phi, pi, 1, tab, 0.0, 1.0, 8)
+
+
+def test_config_2d_trajectory_fp64(golden):
+    """2-D 256^2, FP64, 2000 midpoint steps with hash noise: the <phi^2> curve and
+    the final field against the reference's own run."""
+    g = golden("config_2d_256.npz")
+    phi = cu(g["phi0"])
+    pi = torch.zeros_like(phi)
+    pt, vt = torch.empty_like(phi), torch.empty_like(pi)
+    tab = cu(g["table"])
+    ws = torch.empty(1 << 16, dtype=torch.float64, device=DEV)
+    obs = torch.empty((2000, 10), dtype=torch.float64, device=DEV)
+    noise0 = torch.empty_like(phi)
+    RF.generate_noise_field(noise0, float(g["ns"]), 0)
+    for n in range(2000):
+        RF.rk2_step_table(phi, pi, float(g["dt"]), float(g["dx"]), float(g["eta"]),
+                          float(g["mu"]), None, pt, vt, float(g["inv_a2"]), tab, float(g["tmin"]),
+                          float(g["dinv"]), int(g["npts"]), noise_scale=float(g["ns"]),
+                          noise_step=n)
+        observables(phi, pi, out=obs[n], workspace=ws)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(noise0.cpu().numpy(), g["noise0"], rtol=0, atol=4e-15)
+    o = obs.cpu().numpy()
+    rel = np.abs(o[:, 4] - g["phi2_mean"]) / g["phi2_mean"]
+    assert rel.max() < 1e-11, rel.max()
+    assert np.abs(o[:, 6] - g["frac_above_1"]).max() <= 1.0 / phi.numel()
+    assert np.abs(to_np(phi) - g["phi_final"]).max() < 1e-11
+
+
+# ---------------------------------------------------------------- complex --
+@pytest.mark.parametrize("zn", ["u1", "z4"])
+@pytest.mark.parametrize("tag", CASES)
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_complex_vs_reference(golden, zn, tag, storage):
+    g = golden("rk2_complex.npz")
+    k = f"{zn}_{tag}"
+    st = [as_state(g[f"{k}_{n}_0"], storage) for n in ("phi1", "phi2", "pi1", "pi2")]
+    tmp = [torch.empty_like(a) for a in st]
+    znp = tuple(g["zn_z4"]) if zn == "z4" else (0.0, 0.0, 0.0)
+    for n in range(5):
+        CF.rk2_step_table(*st, float(g["dt"]), float(g["dx"]), float(g["eta"]), float(g["mu"]),
+                          None, None, *tmp, float(g["inv_a2"]), cu(g["table"]), float(g["tmin"]),
+                          float(g["dinv"]), int(g["npts"]), zn=znp, noise_scale=float(g["ns"]),
+                          noise_step=n)
+    torch.cuda.synchronize()
+    for a, n in zip(st, ("phi1", "phi2", "pi1", "pi2")):
+        ref = g[f"{k}_{n}_5"]
+        tol = 1e-12 if storage == "f64" else 5e-6 * np.abs(ref).max()
+        np.testing.assert_allclose(to_np(a), ref, rtol=0, atol=tol)
+
+
+def test_complex_eps4_vs_oracle():
+    shape = (12, 10, 8)
+    rng = np.random.default_rng(12)
+    f = [rng.normal(0, 0.8, shape) for _ in range(2)] + [rng.normal(0, 0.3, shape) for _ in range(2)]
+    tab, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.0), 0.0, 4.0, 4096)
+    ref = [a.copy() for a in f]
+    O.rk2_step_table_complex(*ref, 0.05, 1.0, 1.0, 1.0, None, None,
+                             *[np.empty(shape) for _ in range(4)], 1.0, tab, tmin, dinv, 4096,
+                             eps4=1e-3, noise_scale=0.3, noise_step=11, noise_seed=2)
+    st = [cu(a) for a in f]
+    CF.rk2_step_table(*st, 0.05, 1.0, 1.0, 1.0, None, None, *[torch.empty_like(a) for a in st],
+                      1.0, cu(tab), tmin, dinv, 4096, eps4=1e-3, noise_scale=0.3, noise_step=11,
+                      seed=2)
+    torch.cuda.synchronize()
+    for a, r in zip(st, ref):
+        np.testing.assert_allclose(to_np(a), r, rtol=0, atol=1e-13)
+
+
+# ---------------------------------------------------------------- winding --
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_winding_vs_reference(golden, tag):
+    g = golden("winding.npz")
+    p1, p2 = cu(g[f"{tag}_phi1"]), cu(g[f"{tag}_phi2"])
+    w = torch.empty(p1.shape, dtype=torch.float32, device=DEV)
+    CF.compute_winding_number(p1, p2, w)
+    res = CF.compute_winding_number_full(p1, p2, pierced_cap=3 * p1.numel())
+    torch.cuda.synchronize()
+    ref = np.round(g[f"{tag}_w"])
+    assert np.array_equal(w.cpu().numpy(), ref)  # integer windings: bit-exact
+    c = res.host_counts()
+    assert c["n_strings"] == int(g[f"{tag}_n_strings"])
+    _, w3o, cnto = O.winding(g[f"{tag}_phi1"], g[f"{tag}_phi2"])
+    assert np.array_equal(res.w3.cpu().numpy(), w3o)
+    assert [c["pierced_xy"], c["pierced_xz"], c["pierced_yz"]] == list(cnto[:3])
+    lst = np.sort(res.pierced[: c["listed"]].cpu().numpy().astype(np.int64))
+    nz = np.argwhere(w3o.reshape(3, -1).T != 0)
+    want = np.sort(nz[:, 0] * 3 + nz[:, 1])
+    assert np.array_equal(lst, want)
+
+
+def test_winding_list_capacity_clamps():
+    g = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden",
+                                            "winding.npz"))
+    p1, p2 = cu(g["a_phi1"]), cu(g["a_phi2"])
+    res = CF.compute_winding_number_full(p1, p2, pierced_cap=5)
+    c = res.host_counts()
+    assert c["listed"] == 5 and c["string_length"] > 5
+
+
+def test_winding_f32c_storage_matches_f64():
+    rng = np.random.default_rng(3)
+    shape = (20, 18, 16)
+    th = rng.uniform(-np.pi, np.pi, shape)
+    p1, p2 = np.cos(th), np.sin(th)
+    r64 = CF.compute_winding_number_full(cu(p1), cu(p2))
+    r32c = CF.compute_winding_number_full(RF.to_f32c(cu(p1)), RF.to_f32c(cu(p2)))
+    torch.cuda.synchronize()
+    assert torch.equal(r64.w3, r32c.w3)
+
+
+# ------------------------------------------------------------ observables --
+@pytest.mark.parametrize("tag", CASES)
+def test_energies_vs_reference(golden, tag):
+    g = golden("energies.npz")
+    from thermal_inflation_phase_transition_b200.real_field import compute_energy_densities
+    e = compute_energy_densities(cu(g[f"{tag}_phi"]), cu(g[f"{tag}_pi"]), float(g["dx"]),
+                                 float(g["inv_a2"]), float(g["lam"]), float(g["mphi"]),
+                                 float(g["mu"]))
+    np.testing.assert_allclose(e, g[f"{tag}_E"], rtol=1e-13)
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f32c"])
+def test_observables_vs_oracle(storage):
+    rng = np.random.default_rng(21)
+    shape = (33, 17, 9)
+    phi, pi = rng.normal(0.7, 0.6, shape), rng.normal(0, 0.4, shape)
+    if storage == "f32":
+        phi, pi = phi.astype(np.float32).astype(np.float64), pi.astype(np.float32).astype(np.float64)
+    o = observables(as_state(phi, storage), as_state(pi, storage), dx=0.8, inv_a2=0.9, lam=0.1,
+                    mphi=0.2, mu=1.1, thr=1.0).cpu().numpy()
+    r = O.observables(phi, pi, 0.8, 0.9, 0.1, 0.2, 1.1, 1.0)
+    want = np.array([r[k] for k in O.OBS_NAMES])
+    tol = 1e-12 if storage != "f32c" else 1e-7
+    np.testing.assert_allclose(o, want, rtol=tol, atol=tol)
+
+
+def test_observables_counts_nonfinite():
+    phi = torch.zeros((8, 8, 8), dtype=torch.float64, device=DEV)
+    phi[1, 2, 3] = float("nan")
+    phi[4, 4, 4] = float("inf")
+    o = observables(phi, None).cpu().numpy()
+    assert o[9] == 2
+
+
+def test_observables_deterministic():
+    phi = torch.randn((64, 64, 64), dtype=torch.float64, device=DEV)
+    pi = torch.randn_like(phi)
+    a = observables(phi, pi).cpu().numpy()
+    b = observables(phi, pi).cpu().numpy()
+    assert np.array_equal(a, b)
+
+
+# ------------------------------------------------- full-size properties ---
+def test_fp32c_tracks_fp64_over_many_steps():
+    """FP32-compensated storage against the FP64 kernel over 1000 steps on 64^3
+    with the cooling 2-D table: <phi^2> relative error stays below 1e-6."""
+    shape = (64, 64, 64)
+    t2, tmin, dinv, Tmin, Tdinv = O.build_table_2d(O.toy_vprime, 0.0, 3.0, 4096, 0.97, 1.06, 256)
+    t2c = cu(t2)
+    rng = np.random.default_rng(5)
+    phi0 = rng.normal(0.0, 0.01, shape)
+    s64 = [cu(phi0), torch.zeros(shape, dtype=torch.float64, device=DEV)]
+    s32 = [RF.to_f32c(s64[0]), torch.zeros(shape + (2,), dtype=torch.float32, device=DEV)]
+    t64 = [torch.empty_like(a) for a in s64]
+    t32 = [torch.empty_like(a) for a in s32]
+    ws = torch.empty(1 << 16, dtype=torch.float64, device=DEV)
+    o64 = torch.empty((1000, 10), dtype=torch.float64, device=DEV)
+    o32 = torch.empty_like(o64)
+    for n in range(1000):
+        T = 1.05 - 0.07 * n / 1000
+        ns = math.sqrt(2 * T * 0.05)
+        for s, t, o in ((s64, t64, o64), (s32, t32, o32)):
+            RF.rk2_step_table(s[0], s[1], 0.05, 1.0, 1.0, 1.0, None, t[0], t[1], 1.0, t2c, tmin,
+                              dinv, 4096, noise_scale=ns, noise_step=n, seed=1, vp_T=T,
+                              vp_T_min=Tmin, vp_T_dinv=Tdinv)
+            observables(s[0], s[1], out=o[n], workspace=ws)
+    torch.cuda.synchronize()
+    a, b = o64.cpu().numpy(), o32.cpu().numpy()
+    rel = np.abs(a[:, 4] - b[:, 4]) / a[:, 4]
+    assert rel.max() < 1e-6, rel.max()

@@ -1,0 +1,102 @@
+"""ctypes binding of libtipt.so (the C ABI declared in include/tipt.h).
+
+There is no fallback: if the library is missing or a call fails, a Python
+exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libtipt.so")
+
+TIPT_F64, TIPT_F32, TIPT_F32C = 0, 1, 2
+VP_TABLE, VP_TABLE2D, VP_POLY = 0, 1, 2
+K_PASS2 = 73856093
+K_PASS4 = 19349669
+
+
+class TiptError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str):
+        super().__init__(f"{where}: status {status} ({detail})")
+        self.status = status
+
+
+class VSource(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("npts", C.c_int32), ("table", C.c_void_p),
+                ("tmin", C.c_double), ("dinv", C.c_double), ("nT", C.c_int32),
+                ("pad_", C.c_int32), ("T_min", C.c_double), ("T_dinv", C.c_double),
+                ("T", C.c_double), ("c1", C.c_double), ("c2", C.c_double), ("c3", C.c_double)]
+
+
+class StepParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("dx", C.c_double), ("eta_eff", C.c_double),
+                ("mu", C.c_double), ("inv_a2", C.c_double), ("noise_scale", C.c_double),
+                ("noise_step", C.c_uint64), ("noise_seed", C.c_uint64)]
+
+
+class ComplexTerms(C.Structure):
+    _fields_ = [("zn_n", C.c_double), ("zn_dv", C.c_double), ("zn_active", C.c_double),
+                ("eps4", C.c_double)]
+
+
+_p, _i64, _u64, _d, _i = C.c_void_p, C.c_int64, C.c_uint64, C.c_double, C.c_int
+
+# name -> argtypes (restype int unless listed in _RESTYPE)
+_SIGS = {
+    "tipt_version": [],
+    "tipt_status_string": [_i],
+    "tipt_last_error": [],
+    "tipt_hash_rng_pair": [_p, _i64, _p, _p, _p, _p],
+    "tipt_generate_noise_field": [_i, _p, _i64, _i64, _i64, _d, _u64, _u64, _u64, _i, _p],
+    "tipt_rk2_step_table": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
+                            C.POINTER(VSource), _p, _p],
+    "tipt_rk2_fused_table": [_i, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
+                             C.POINTER(StepParams), C.POINTER(VSource), C.POINTER(VSource), _p,
+                             _p],
+    "tipt_complex_rk2_step_table": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
+                                    C.POINTER(StepParams), C.POINTER(VSource),
+                                    C.POINTER(ComplexTerms), _p, _p, _p],
+    "tipt_compute_winding_number": [_i, _p, _p, _i64, _i64, _i64, _p, _p, _p, _i64, _p, _p],
+    "tipt_observables_workspace_size": [_i64, _i64, _i64],
+    "tipt_observables": [_i, _p, _p, _i64, _i64, _i64, _d, _d, _d, _d, _d, _d, _p, _p, _i64,
+                         _p],
+}
+_RESTYPE = {"tipt_version": C.c_char_p, "tipt_status_string": C.c_char_p,
+            "tipt_last_error": C.c_char_p, "tipt_observables_workspace_size": C.c_int64}
+
+_lib = None
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def lib():
+    """Load libtipt.so (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with "
+                "`python -m thermal_inflation_phase_transition_b200.build` (there is no CPU "
+                "fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _RESTYPE.get(name, C.c_int)
+        _lib = L
+    return _lib
+
+
+def check(status: int, where: str) -> None:
+    if status != 0:
+        L = lib()
+        raise TiptError(status, where, f"{L.tipt_status_string(status).decode()}: "
+                                       f"{L.tipt_last_error().decode()}")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args), name)

@@ -1,0 +1,100 @@
+"""Complex scalar field kernels with the reference's names and positional signatures.
+
+Reference: simulation/latticeSimComplex_numba.py (C).  Phi = phi1 + i phi2; each
+component is a CUDA tensor in one of the three storages (see real_field).
+
+Extensions over the reference signatures are keyword-only:
+  zn=(N, delta_V, active) -> the reference's _ZN_PARAMS (C:226-231), passed
+                             per call instead of frozen into the compiled kernel;
+  eps4                    -> eps * Re(Phi^4) symmetry breaking;
+  noise1=noise2=None      -> inline hash noise, one pair per site (C:2958-2974).
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _lib as L
+from ._common import (dims_of, need_cuda, ptr, same_layout, step_params, storage_of,
+                      stream_handle, swap_storage, table_source)
+
+
+def rk2_step_table(phi1, phi2, pi1, pi2, dt, dx, eta_eff, mu, noise1, noise2, phi1_tmp,
+                   phi2_tmp, pi1_tmp, pi2_tmp, inv_a2, vp_table, vp_tmin, vp_dinv, vp_npts, *,
+                   zn=(0.0, 0.0, 0.0), eps4=0.0, noise_scale=0.0, noise_step=0, seed=0):
+    """C:2067 rk2_step_table (complex): one midpoint step, in place (storage exchange
+    with the *_tmp tensors, as real_field.rk2_step_table)."""
+    st = storage_of(phi1)
+    arrs = (phi1, phi2, pi1, pi2, phi1_tmp, phi2_tmp, pi1_tmp, pi2_tmp)
+    names = ("phi1", "phi2", "pi1", "pi2", "phi1_tmp", "phi2_tmp", "pi1_tmp", "pi2_tmp")
+    need_cuda(*arrs, names=names)
+    same_layout(phi1, *arrs[1:], names=names[1:])
+    if (noise1 is None) != (noise2 is None):
+        raise ValueError("give both noise1 and noise2, or neither")
+    if noise1 is not None:
+        need_cuda(noise1, noise2, names=["noise1", "noise2"])
+        want = torch.float32 if st == L.TIPT_F32 else torch.float64
+        for n in (noise1, noise2):
+            if n.dtype != want or tuple(n.shape) != dims_of(phi1):
+                raise ValueError(f"noise arrays must be {want} with shape {dims_of(phi1)}")
+    nx, ny, nz = dims_of(phi1)
+    vs = table_source(vp_table, vp_tmin, vp_dinv, vp_npts)
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
+    ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
+    L.call("tipt_complex_rk2_step_table", st, ptr(phi1), ptr(phi2), ptr(pi1), ptr(pi2),
+           ptr(phi1_tmp), ptr(phi2_tmp), ptr(pi1_tmp), ptr(pi2_tmp), nx, ny, nz, sp, vs, ct,
+           ptr(noise1), ptr(noise2), stream_handle())
+    for a, b in ((phi1, phi1_tmp), (phi2, phi2_tmp), (pi1, pi1_tmp), (pi2, pi2_tmp)):
+        swap_storage(a, b)
+
+
+def rk2_step_table_into(state, out, dt, dx, eta_eff, mu, inv_a2, vsource, *, zn=(0.0, 0.0, 0.0),
+                        eps4=0.0, noise_scale=0.0, noise_step=0, seed=0, stream=None):
+    """Ping-pong form: state=(phi1, phi2, pi1, pi2) -> out=(phi1', phi2', pi1', pi2')."""
+    st = storage_of(state[0])
+    nx, ny, nz = dims_of(state[0])
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
+    ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
+    L.call("tipt_complex_rk2_step_table", st, *[ptr(a) for a in state], *[ptr(a) for a in out],
+           nx, ny, nz, sp, vsource, ct, None, None, stream_handle(stream))
+
+
+class WindingResult:
+    """Device outputs of compute_winding_number_full."""
+
+    def __init__(self, w_site, w3, pierced, counts):
+        self.w_site, self.w3, self.pierced, self.counts = w_site, w3, pierced, counts
+
+    def host_counts(self):
+        c = self.counts.tolist()
+        return {"pierced_xy": c[0], "pierced_xz": c[1], "pierced_yz": c[2], "n_strings": c[3],
+                "listed": c[4], "string_length": c[0] + c[1] + c[2]}
+
+
+def compute_winding_number(phi1, phi2, winding_out):
+    """C:2683 compute_winding_number(phi1, phi2, winding_out): per-site winding
+    (sum over the XY, XZ, YZ plaquettes) into float32 ``winding_out``."""
+    need_cuda(phi1, phi2, winding_out, names=["phi1", "phi2", "winding_out"])
+    st = storage_of(phi1)
+    if winding_out.dtype != torch.float32 or tuple(winding_out.shape) != dims_of(phi1):
+        raise ValueError("winding_out must be float32 with the lattice shape")
+    counts = torch.empty(5, dtype=torch.int64, device=phi1.device)
+    L.call("tipt_compute_winding_number", st, ptr(phi1), ptr(phi2), *dims_of(phi1),
+           ptr(winding_out), None, None, 0, ptr(counts), stream_handle())
+    return winding_out
+
+
+def compute_winding_number_full(phi1, phi2, *, w_site=True, w3=True, pierced_cap=0,
+                                stream=None):
+    """Winding with per-orientation int8 windings, a compacted list of pierced
+    plaquettes (site*3 + orientation, XY=0, XZ=1, YZ=2) and device counts."""
+    need_cuda(phi1, phi2, names=["phi1", "phi2"])
+    st = storage_of(phi1)
+    shape = dims_of(phi1)
+    dev = phi1.device
+    ws = torch.empty(shape, dtype=torch.float32, device=dev) if w_site else None
+    w3t = torch.empty((3,) + shape, dtype=torch.int8, device=dev) if w3 else None
+    pl = torch.empty(max(pierced_cap, 1), dtype=torch.int32, device=dev) if pierced_cap else None
+    counts = torch.empty(5, dtype=torch.int64, device=dev)
+    L.call("tipt_compute_winding_number", st, ptr(phi1), ptr(phi2), *shape, ptr(ws), ptr(w3t),
+           ptr(pl), int(pierced_cap), ptr(counts), stream_handle(stream))
+    return WindingResult(ws, w3t, pl, counts)

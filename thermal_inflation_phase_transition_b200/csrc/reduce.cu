@@ -1,0 +1,239 @@
+// Observable reductions: compute_energy_densities (R:2270-2319) plus <phi>,
+// <phi^2>, <pi^2>, the converted fraction, min/max and the non-finite count
+// of the host NaN guard (R:3882-3944).
+//
+// Two launches, both deterministic: (1) a fixed number of blocks G (a
+// function of the lattice size only) each reduce a contiguous range of
+// sites with warp shuffles into FP64 partials in the caller's workspace;
+// (2) one block folds the G partials in a fixed order.  The result does not
+// depend on the GPU or on timing.
+#include "tipt_device.cuh"
+#include "tipt_internal.h"
+
+namespace tipt {
+
+constexpr int kObs = 10;          // outputs
+constexpr int kRedThreads = 256;
+constexpr int kMaxRedBlocks = 1024;
+
+struct ObsAcc {
+    double kin, grad, pot, s1, s2, sq, above, nonfinite, mn, mx;
+};
+
+__device__ __forceinline__ void acc_init(ObsAcc& a) {
+    a.kin = a.grad = a.pot = a.s1 = a.s2 = a.sq = a.above = a.nonfinite = 0.0;
+    a.mn = INFINITY;
+    a.mx = -INFINITY;
+}
+
+__device__ __forceinline__ void acc_merge(ObsAcc& a, const ObsAcc& b) {
+    a.kin += b.kin;
+    a.grad += b.grad;
+    a.pot += b.pot;
+    a.s1 += b.s1;
+    a.s2 += b.s2;
+    a.sq += b.sq;
+    a.above += b.above;
+    a.nonfinite += b.nonfinite;
+    a.mn = fmin(a.mn, b.mn);
+    a.mx = fmax(a.mx, b.mx);
+}
+
+__device__ __forceinline__ ObsAcc acc_shfl_down(const ObsAcc& a, int off) {
+    ObsAcc b;
+    b.kin = __shfl_down_sync(0xffffffffu, a.kin, off);
+    b.grad = __shfl_down_sync(0xffffffffu, a.grad, off);
+    b.pot = __shfl_down_sync(0xffffffffu, a.pot, off);
+    b.s1 = __shfl_down_sync(0xffffffffu, a.s1, off);
+    b.s2 = __shfl_down_sync(0xffffffffu, a.s2, off);
+    b.sq = __shfl_down_sync(0xffffffffu, a.sq, off);
+    b.above = __shfl_down_sync(0xffffffffu, a.above, off);
+    b.nonfinite = __shfl_down_sync(0xffffffffu, a.nonfinite, off);
+    b.mn = __shfl_down_sync(0xffffffffu, a.mn, off);
+    b.mx = __shfl_down_sync(0xffffffffu, a.mx, off);
+    return b;
+}
+
+// Block-wide fixed-order reduction; result valid in thread 0.
+__device__ __forceinline__ ObsAcc block_reduce(ObsAcc a) {
+    __shared__ ObsAcc s_w[kRedThreads / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc_merge(a, acc_shfl_down(a, off));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) s_w[w] = a;
+    __syncthreads();
+    if (w == 0) {
+        if (l < kRedThreads / 32) a = s_w[l];
+        else acc_init(a);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc_merge(a, acc_shfl_down(a, off));
+    }
+    return a;
+}
+
+template <int S>
+__device__ __forceinline__ double load_val(const void* p, int64_t s) {
+    if constexpr (S == TIPT_F64) return __ldg(static_cast<const double*>(p) + s);
+    else if constexpr (S == TIPT_F32) return (double)__ldg(static_cast<const float*>(p) + s);
+    else return join_f32c(__ldg(static_cast<const float2*>(p) + s));
+}
+
+struct ObsParams {
+    const void* phi;
+    const void* pi;
+    int n0, n1, n2;
+    double inv_dx2, inv_a2, lam, m2, inv_mu2, thr;
+    double* partials;  // [G][kObs]
+    double* out;       // [kObs]
+};
+
+template <int S>
+__global__ void __launch_bounds__(kRedThreads) obs_partial_kernel(ObsParams p) {
+    const int64_t n12 = (int64_t)p.n1 * p.n2;
+    const int64_t N = (int64_t)p.n0 * n12;
+    const int64_t per = (N + gridDim.x - 1) / gridDim.x;
+    const int64_t lo = per * blockIdx.x;
+    const int64_t hi = lo + per < N ? lo + per : N;
+    ObsAcc a;
+    acc_init(a);
+    for (int64_t s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+        const int k = (int)(s % p.n2);
+        const int64_t r = s / p.n2;
+        const int j = (int)(r % p.n1);
+        const int i = (int)(r / p.n1);
+        const double ph = load_val<S>(p.phi, s);
+        const double pv = p.pi ? load_val<S>(p.pi, s) : 0.0;
+        // forward differences, R:2303-2308
+        const double fx = load_val<S>(p.phi, s + ((i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12)) - ph;
+        const double fy = load_val<S>(p.phi, s + ((j + 1 < p.n1) ? (int64_t)p.n2 : -(int64_t)(p.n1 - 1) * p.n2)) - ph;
+        const double fz = load_val<S>(p.phi, s + ((k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1))) - ph;
+        a.kin += 0.5 * pv * pv;
+        a.grad += 0.5 * p.inv_a2 * (fx * fx + fy * fy + fz * fz) * p.inv_dx2;
+        const double ph2 = ph * ph;
+        a.pot += (0.25 * p.lam * ph2 * ph2 - 0.5 * p.m2 * ph2) * p.inv_mu2;
+        a.s1 += ph;
+        a.s2 += ph2;
+        a.sq += pv * pv;
+        a.above += ph > p.thr ? 1.0 : 0.0;
+        a.nonfinite += (isfinite(ph) && isfinite(pv)) ? 0.0 : 1.0;
+        a.mn = fmin(a.mn, ph);
+        a.mx = fmax(a.mx, ph);
+    }
+    a = block_reduce(a);
+    if (threadIdx.x == 0) {
+        double* o = p.partials + (int64_t)blockIdx.x * kObs;
+        o[0] = a.kin;
+        o[1] = a.grad;
+        o[2] = a.pot;
+        o[3] = a.s1;
+        o[4] = a.s2;
+        o[5] = a.sq;
+        o[6] = a.above;
+        o[7] = a.mn;
+        o[8] = a.mx;
+        o[9] = a.nonfinite;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads) obs_final_kernel(ObsParams p, int G, double inv_n) {
+    ObsAcc a;
+    acc_init(a);
+    // fixed assignment: thread t folds partials t, t+256, ... in order
+    for (int b = threadIdx.x; b < G; b += blockDim.x) {
+        const double* o = p.partials + (int64_t)b * kObs;
+        ObsAcc c;
+        c.kin = o[0];
+        c.grad = o[1];
+        c.pot = o[2];
+        c.s1 = o[3];
+        c.s2 = o[4];
+        c.sq = o[5];
+        c.above = o[6];
+        c.mn = o[7];
+        c.mx = o[8];
+        c.nonfinite = o[9];
+        acc_merge(a, c);
+    }
+    a = block_reduce(a);
+    if (threadIdx.x == 0) {
+        p.out[0] = a.kin * inv_n;
+        p.out[1] = a.grad * inv_n;
+        p.out[2] = a.pot * inv_n;
+        p.out[3] = a.s1 * inv_n;
+        p.out[4] = a.s2 * inv_n;
+        p.out[5] = a.sq * inv_n;
+        p.out[6] = a.above * inv_n;
+        p.out[7] = a.mn;
+        p.out[8] = a.mx;
+        p.out[9] = a.nonfinite;
+    }
+}
+
+int obs_blocks(int64_t N) {
+    int64_t g = (N + 8191) / 8192;
+    if (g > kMaxRedBlocks) g = kMaxRedBlocks;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+int64_t obs_workspace_bytes(int64_t N) { return (int64_t)obs_blocks(N) * kObs * 8; }
+
+int launch_observables(int storage, const void* phi, const void* pi, int n0, int n1, int n2,
+                       double dx, double inv_a2, double lam, double mphi, double mu, double thr,
+                       double* out, double* partials, cudaStream_t st) {
+    ObsParams p;
+    p.phi = phi;
+    p.pi = pi;
+    p.n0 = n0;
+    p.n1 = n1;
+    p.n2 = n2;
+    p.inv_dx2 = 1.0 / (dx * dx);
+    p.inv_a2 = inv_a2;
+    p.lam = lam;
+    p.m2 = mphi * mphi;
+    p.inv_mu2 = 1.0 / (mu * mu);
+    p.thr = thr;
+    p.partials = partials;
+    p.out = out;
+    const int64_t N = (int64_t)n0 * n1 * n2;
+    const int G = obs_blocks(N);
+    switch (storage) {
+        case TIPT_F64: obs_partial_kernel<TIPT_F64><<<G, kRedThreads, 0, st>>>(p); break;
+        case TIPT_F32: obs_partial_kernel<TIPT_F32><<<G, kRedThreads, 0, st>>>(p); break;
+        default: obs_partial_kernel<TIPT_F32C><<<G, kRedThreads, 0, st>>>(p); break;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "observables partial launch");
+    obs_final_kernel<<<1, kRedThreads, 0, st>>>(p, G, 1.0 / (double)N);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "observables final launch");
+}
+
+}  // namespace tipt
+
+using namespace tipt;
+
+extern "C" int64_t tipt_observables_workspace_size(int64_t nx, int64_t ny, int64_t nz) {
+    if (nx < 1 || ny < 1 || nz < 1) return 0;
+    return obs_workspace_bytes(nx * ny * nz);
+}
+
+extern "C" int tipt_observables(int storage, const void* phi, const void* pi, int64_t nx,
+                                int64_t ny, int64_t nz, double dx, double inv_a2, double lam,
+                                double mphi, double mu, double thr, double* out,
+                                void* workspace, int64_t workspace_bytes, void* stream) {
+    int rc;
+    if ((rc = check_storage(storage)) || (rc = check_dims(nx, ny, nz))) return rc;
+    const int eb = elem_bytes(storage);
+    if ((rc = check_ptr(phi, eb, "phi")) || (rc = check_ptr(out, 8, "out")) ||
+        (rc = check_ptr(workspace, 8, "workspace")))
+        return rc;
+    if (pi && (rc = check_ptr(pi, eb, "pi"))) return rc;
+    const int64_t need = obs_workspace_bytes(nx * ny * nz);
+    if (workspace_bytes < need)
+        return fail(TIPT_ERR_ARG, "workspace of %lld bytes is smaller than the %lld needed",
+                    (long long)workspace_bytes, (long long)need);
+    return launch_observables(storage, phi, pi, (int)nx, (int)ny, (int)nz, dx, inv_a2, lam, mphi,
+                              mu, thr, out, static_cast<double*>(workspace),
+                              (cudaStream_t)stream);
+}

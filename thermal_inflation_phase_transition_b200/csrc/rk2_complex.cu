@@ -1,0 +1,329 @@
+// Complex-field fused midpoint RK2 stage (C:2067-2215 rk2_step_table) and
+// its entry point.  Same single-launch fusion as the real field: the midpoint
+// phi~_a = phi_a + h1*pi_a is pointwise, so both reference passes run on the
+// 7-point stencil of (phi1, phi2, pi1, pi2).
+#include <cstring>
+
+#include "rk2_real.cuh"
+#include "tipt_internal.h"
+
+namespace tipt {
+
+struct ComplexStageParams {
+    const void* f[4];   // phi1, phi2, pi1, pi2
+    void* o[4];
+    int n0, n1, n2;
+    double h1, h2, inv_dx2, eta, inv_mu2, inv_a2;
+    const void* noise1;
+    const void* noise2;
+    double ns_eff, nfac;
+    uint64_t step, mul, seed;
+    double zn_n, zn_dv, zn_active, eps4;
+    // V'(rho) source (1-D table or polynomial)
+    int vkind, npts;
+    const double* table;
+    double tmin, dinv;
+    double c1, c2, c3;
+    int table_in_smem;
+};
+
+// C:2137-2158 projection + Z_N (reference form), then eps*Re(Phi^4) whose
+// gradient is 4 eps (p1^3 - 3 p1 p2^2, 3 p1^2 p2 - p2^3).
+template <typename R>
+__device__ __forceinline__ void complex_force(const ComplexStageParams& p, const R* tab, R tmin,
+                                              R dinv, R p1, R p2, R& d1, R& d2) {
+    R rho = sqrt(p1 * p1 + p2 * p2);
+    R rho_safe = rho > R(1e-30) ? rho : R(1e-30);
+    R dvdr;
+    if (p.vkind == TIPT_VP_POLY) dvdr = poly_vprime<R>((R)p.c1, (R)p.c2, (R)p.c3, rho);
+    else dvdr = lerp_table<R>(tab, tmin, dinv, p.npts - 2, rho);
+    R a = dvdr * p1 / rho_safe;
+    R b = dvdr * p2 / rho_safe;
+    if (p.zn_active > 0.5 && p.zn_n > 0.5 && rho > R(1e-20)) {
+        R th = atan2(p2, p1);
+        R sn = sin((R)p.zn_n * th);
+        R ir = R(1) / rho_safe;
+        R ir2 = ir * ir;
+        a += -(R)p.zn_n * (R)p.zn_dv * sn * p2 * ir2;
+        b += (R)p.zn_n * (R)p.zn_dv * sn * p1 * ir2;
+    }
+    if (p.eps4 != 0.0) {
+        const R e4 = R(4) * (R)p.eps4;
+        a += e4 * (p1 * p1 * p1 - R(3) * p1 * p2 * p2);
+        b += e4 * (R(3) * p1 * p1 * p2 - p2 * p2 * p2);
+    }
+    d1 = a;
+    d2 = b;
+}
+
+template <typename NT>
+__device__ __forceinline__ void complex_noise(const ComplexStageParams& p, uint64_t site,
+                                              double& n1, double& n2) {
+    if (p.noise1) {
+        n1 = p.nfac * (double)static_cast<const NT*>(p.noise1)[site];
+        n2 = p.nfac * (double)static_cast<const NT*>(p.noise2)[site];
+    } else if (p.ns_eff != 0.0) {
+        double z1, z2;
+        gauss_pair(noise_key(site, p.step, p.mul, p.seed), z1, z2);
+        n1 = p.ns_eff * z1;
+        n2 = p.ns_eff * z2;
+    } else {
+        n1 = n2 = 0.0;
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using TT = typename std::conditional<S == TIPT_F32C, float, double>::type;
+    TT* s_tab = reinterpret_cast<TT*>(smem_raw);
+    if (p.table_in_smem) {
+        for (int q = threadIdx.x; q < p.npts; q += blockDim.x) s_tab[q] = (TT)__ldg(p.table + q);
+        __syncthreads();
+    }
+    const double* dtab = p.table_in_smem ? reinterpret_cast<const double*>(s_tab) : p.table;
+    const int64_t n12 = (int64_t)p.n1 * p.n2;
+    const int64_t N = (int64_t)p.n0 * n12;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(s % p.n2);
+        const int64_t r = s / p.n2;
+        const int j = (int)(r % p.n1);
+        const int i = (int)(r / p.n1);
+        const int64_t idx[7] = {
+            s,
+            s + ((i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12),
+            s + ((i > 0) ? -n12 : (int64_t)(p.n0 - 1) * n12),
+            s + ((j + 1 < p.n1) ? (int64_t)p.n2 : -(int64_t)(p.n1 - 1) * p.n2),
+            s + ((j > 0) ? -(int64_t)p.n2 : (int64_t)(p.n1 - 1) * p.n2),
+            s + ((k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1)),
+            s + ((k > 0) ? -1 : (int64_t)(p.n2 - 1))};
+        double n1, n2;
+        if constexpr (S == TIPT_F64) {
+            double a[4][7];
+#pragma unroll
+            for (int f = 0; f < 4; ++f)
+#pragma unroll
+                for (int q = 0; q < 7; ++q) a[f][q] = __ldg(static_cast<const double*>(p.f[f]) + idx[q]);
+            double lap[2], pt[2][7], lapt[2];
+#pragma unroll
+            for (int f = 0; f < 2; ++f) {
+                lap[f] = (a[f][1] + a[f][2] + a[f][3] + a[f][4] + a[f][5] + a[f][6] - 6.0 * a[f][0]) * p.inv_dx2;
+#pragma unroll
+                for (int q = 0; q < 7; ++q) pt[f][q] = a[f][q] + p.h1 * a[2 + f][q];
+                lapt[f] = (pt[f][1] + pt[f][2] + pt[f][3] + pt[f][4] + pt[f][5] + pt[f][6] - 6.0 * pt[f][0]) * p.inv_dx2;
+            }
+            double d1, d2;
+            complex_force<double>(p, dtab, p.tmin, p.dinv, a[0][0], a[1][0], d1, d2);
+            double k1a = p.inv_a2 * lap[0] - p.eta * a[2][0] - d1 * p.inv_mu2;
+            double k1b = p.inv_a2 * lap[1] - p.eta * a[3][0] - d2 * p.inv_mu2;
+            double pta = a[2][0] + p.h1 * k1a, ptb = a[3][0] + p.h1 * k1b;
+            complex_force<double>(p, dtab, p.tmin, p.dinv, pt[0][0], pt[1][0], d1, d2);
+            double k2a = p.inv_a2 * lapt[0] - p.eta * pta - d1 * p.inv_mu2;
+            double k2b = p.inv_a2 * lapt[1] - p.eta * ptb - d2 * p.inv_mu2;
+            complex_noise<double>(p, (uint64_t)s, n1, n2);
+            static_cast<double*>(p.o[0])[s] = a[0][0] + p.h2 * pta;
+            static_cast<double*>(p.o[1])[s] = a[1][0] + p.h2 * ptb;
+            static_cast<double*>(p.o[2])[s] = a[2][0] + (p.h2 * k2a + n1);
+            static_cast<double*>(p.o[3])[s] = a[3][0] + (p.h2 * k2b + n2);
+        } else if constexpr (S == TIPT_F32) {
+            // float32 storage, FP64 arithmetic after the float32 neighbour sums,
+            // float32-rounded midpoint state (as the reference's float32 mode)
+            float a[4][7];
+#pragma unroll
+            for (int f = 0; f < 4; ++f)
+#pragma unroll
+                for (int q = 0; q < 7; ++q) a[f][q] = __ldg(static_cast<const float*>(p.f[f]) + idx[q]);
+            double lap[2], lapt[2];
+            float pt[2][7];
+#pragma unroll
+            for (int f = 0; f < 2; ++f) {
+                float s6 = a[f][1] + a[f][2] + a[f][3] + a[f][4] + a[f][5] + a[f][6];
+                lap[f] = ((double)s6 - 6.0 * (double)a[f][0]) * p.inv_dx2;
+#pragma unroll
+                for (int q = 0; q < 7; ++q)
+                    pt[f][q] = __double2float_rn((double)a[f][q] + p.h1 * (double)a[2 + f][q]);
+                float s6b = pt[f][1] + pt[f][2] + pt[f][3] + pt[f][4] + pt[f][5] + pt[f][6];
+                lapt[f] = ((double)s6b - 6.0 * (double)pt[f][0]) * p.inv_dx2;
+            }
+            double d1, d2;
+            complex_force<double>(p, dtab, p.tmin, p.dinv, a[0][0], a[1][0], d1, d2);
+            double k1a = p.inv_a2 * lap[0] - p.eta * (double)a[2][0] - d1 * p.inv_mu2;
+            double k1b = p.inv_a2 * lap[1] - p.eta * (double)a[3][0] - d2 * p.inv_mu2;
+            float pta = __double2float_rn((double)a[2][0] + p.h1 * k1a);
+            float ptb = __double2float_rn((double)a[3][0] + p.h1 * k1b);
+            complex_force<double>(p, dtab, p.tmin, p.dinv, pt[0][0], pt[1][0], d1, d2);
+            double k2a = p.inv_a2 * lapt[0] - p.eta * (double)pta - d1 * p.inv_mu2;
+            double k2b = p.inv_a2 * lapt[1] - p.eta * (double)ptb - d2 * p.inv_mu2;
+            complex_noise<float>(p, (uint64_t)s, n1, n2);
+            static_cast<float*>(p.o[0])[s] = __double2float_rn((double)a[0][0] + p.h2 * (double)pta);
+            static_cast<float*>(p.o[1])[s] = __double2float_rn((double)a[1][0] + p.h2 * (double)ptb);
+            static_cast<float*>(p.o[2])[s] = __double2float_rn((double)a[2][0] + (p.h2 * k2a + n1));
+            static_cast<float*>(p.o[3])[s] = __double2float_rn((double)a[3][0] + (p.h2 * k2b + n2));
+        } else {
+            float2 a[4][7];
+#pragma unroll
+            for (int f = 0; f < 4; ++f)
+#pragma unroll
+                for (int q = 0; q < 7; ++q) a[f][q] = __ldg(static_cast<const float2*>(p.f[f]) + idx[q]);
+            const float h1 = (float)p.h1, inv_dx2 = (float)p.inv_dx2;
+            float lap[4];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                float dh = 0.f, dl = 0.f;
+#pragma unroll
+                for (int q = 1; q < 7; ++q) {
+                    dh += a[f][q].x - a[f][0].x;
+                    dl += a[f][q].y - a[f][0].y;
+                }
+                lap[f] = (dh + dl) * inv_dx2;
+            }
+            float c[4];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) c[f] = a[f][0].x + a[f][0].y;
+            const float* ftab = reinterpret_cast<const float*>(s_tab);
+            const float inv_a2 = (float)p.inv_a2, eta = (float)p.eta, inv_mu2 = (float)p.inv_mu2;
+            float d1, d2;
+            if (p.table_in_smem || p.vkind == TIPT_VP_POLY) {
+                complex_force<float>(p, ftab, (float)p.tmin, (float)p.dinv, c[0], c[1], d1, d2);
+            } else {
+                double e1, e2;
+                complex_force<double>(p, p.table, p.tmin, p.dinv, c[0], c[1], e1, e2);
+                d1 = (float)e1;
+                d2 = (float)e2;
+            }
+            float k1a = inv_a2 * lap[0] - eta * c[2] - d1 * inv_mu2;
+            float k1b = inv_a2 * lap[1] - eta * c[3] - d2 * inv_mu2;
+            float pta = c[2] + h1 * k1a, ptb = c[3] + h1 * k1b;
+            float q1 = a[0][0].x + (a[0][0].y + h1 * c[2]);
+            float q2 = a[1][0].x + (a[1][0].y + h1 * c[3]);
+            if (p.table_in_smem || p.vkind == TIPT_VP_POLY) {
+                complex_force<float>(p, ftab, (float)p.tmin, (float)p.dinv, q1, q2, d1, d2);
+            } else {
+                double e1, e2;
+                complex_force<double>(p, p.table, p.tmin, p.dinv, q1, q2, e1, e2);
+                d1 = (float)e1;
+                d2 = (float)e2;
+            }
+            float k2a = inv_a2 * (lap[0] + h1 * lap[2]) - eta * pta - d1 * inv_mu2;
+            float k2b = inv_a2 * (lap[1] + h1 * lap[3]) - eta * ptb - d2 * inv_mu2;
+            complex_noise<double>(p, (uint64_t)s, n1, n2);
+            const double pia = join_f32c(a[2][0]), pib = join_f32c(a[3][0]);
+            static_cast<float2*>(p.o[0])[s] = split_f32c(join_f32c(a[0][0]) + p.h2 * (pia + p.h1 * (double)k1a));
+            static_cast<float2*>(p.o[1])[s] = split_f32c(join_f32c(a[1][0]) + p.h2 * (pib + p.h1 * (double)k1b));
+            static_cast<float2*>(p.o[2])[s] = split_f32c(pia + ((double)(p.h2 * (double)k2a) + n1));
+            static_cast<float2*>(p.o[3])[s] = split_f32c(pib + ((double)(p.h2 * (double)k2b) + n2));
+        }
+    }
+}
+
+constexpr int64_t kMaxTableSmemC = 96 * 1024;
+
+template <int S>
+static int launch_complex_generic(ComplexStageParams p, int64_t smem, cudaStream_t st) {
+    auto kern = complex_stage_generic<S>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return fail_cuda(e, "complex_stage smem attribute");
+    }
+    const int64_t N = (int64_t)p.n0 * p.n1 * p.n2;
+    int64_t blocks = (N + 255) / 256;
+    const int64_t cap = (int64_t)num_sms() * 8;
+    if (blocks > cap) blocks = cap;
+    kern<<<(unsigned)blocks, 256, (size_t)smem, st>>>(p);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "complex_stage launch");
+}
+
+int launch_complex_stage(int storage, ComplexStageParams p, cudaStream_t st) {
+    int64_t tb = p.vkind == TIPT_VP_POLY ? 0 : (int64_t)p.npts * (storage == TIPT_F32C ? 4 : 8);
+    p.table_in_smem = (tb > 0 && tb <= kMaxTableSmemC) ? 1 : 0;
+    const int64_t smem = p.table_in_smem ? tb : 0;
+    switch (storage) {
+        case TIPT_F64: return launch_complex_generic<TIPT_F64>(p, smem, st);
+        case TIPT_F32: return launch_complex_generic<TIPT_F32>(p, smem, st);
+        case TIPT_F32C: return launch_complex_generic<TIPT_F32C>(p, smem, st);
+    }
+    return fail(TIPT_ERR_STORAGE, "unknown storage %d", storage);
+}
+
+}  // namespace tipt
+
+using namespace tipt;
+
+extern "C" int tipt_complex_rk2_step_table(int storage, const void* phi1, const void* phi2,
+                                           const void* pi1, const void* pi2, void* phi1_out,
+                                           void* phi2_out, void* pi1_out, void* pi2_out,
+                                           int64_t nx, int64_t ny, int64_t nz,
+                                           const tipt_step_params* sp, const tipt_vsource* vp,
+                                           const tipt_complex_terms* ct, const void* noise1,
+                                           const void* noise2, void* stream) {
+    int rc;
+    if ((rc = check_state(storage, phi1, phi2, phi1_out, phi2_out, nx, ny, nz)) ||
+        (rc = check_state(storage, pi1, pi2, pi1_out, pi2_out, nx, ny, nz)))
+        return rc;
+    {
+        const int64_t bytes = nx * ny * nz * elem_bytes(storage);
+        const void* ins[4] = {phi1, phi2, pi1, pi2};
+        const void* outs[4] = {phi1_out, phi2_out, pi1_out, pi2_out};
+        for (int a = 0; a < 4; ++a) {
+            for (int b = 0; b < 4; ++b)
+                if (overlap(outs[a], ins[b], bytes))
+                    return fail(TIPT_ERR_ARG, "an output array overlaps an input array");
+            for (int b = a + 1; b < 4; ++b)
+                if (overlap(outs[a], outs[b], bytes))
+                    return fail(TIPT_ERR_ARG, "two output arrays overlap");
+        }
+    }
+    if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
+    if ((rc = check_vsource(vp, "vp"))) return rc;
+    if (vp->kind == TIPT_VP_TABLE2D)
+        return fail(TIPT_ERR_UNSUPPORTED, "complex field takes a 1-D V'(rho) table");
+    if ((noise1 == nullptr) != (noise2 == nullptr))
+        return fail(TIPT_ERR_ARG, "noise1 and noise2 must both be given or both be NULL");
+    if (noise1 && ((rc = check_ptr(noise1, storage == TIPT_F32 ? 4 : 8, "noise1")) ||
+                   (rc = check_ptr(noise2, storage == TIPT_F32 ? 4 : 8, "noise2"))))
+        return rc;
+    ComplexStageParams p;
+    memset(&p, 0, sizeof(p));
+    p.f[0] = phi1;
+    p.f[1] = phi2;
+    p.f[2] = pi1;
+    p.f[3] = pi2;
+    p.o[0] = phi1_out;
+    p.o[1] = phi2_out;
+    p.o[2] = pi1_out;
+    p.o[3] = pi2_out;
+    p.n0 = (int)nx;
+    p.n1 = (int)ny;
+    p.n2 = (int)nz;
+    p.h1 = 0.5 * sp->dt;
+    p.h2 = sp->dt;
+    p.inv_dx2 = 1.0 / (sp->dx * sp->dx);
+    p.eta = sp->eta_eff;
+    p.inv_mu2 = 1.0 / (sp->mu * sp->mu);
+    p.inv_a2 = sp->inv_a2;
+    p.noise1 = noise1;
+    p.noise2 = noise2;
+    p.ns_eff = sp->noise_scale;
+    p.nfac = 1.0;
+    p.step = sp->noise_step;
+    p.mul = kPass2Mul;
+    p.seed = sp->noise_seed;
+    if (ct) {
+        p.zn_n = ct->zn_n;
+        p.zn_dv = ct->zn_dv;
+        p.zn_active = ct->zn_active;
+        p.eps4 = ct->eps4;
+    }
+    p.vkind = vp->kind;
+    p.npts = vp->npts;
+    p.table = vp->table;
+    p.tmin = vp->tmin;
+    p.dinv = vp->dinv;
+    p.c1 = vp->c1;
+    p.c2 = vp->c2;
+    p.c3 = vp->c3;
+    return launch_complex_stage(storage, p, (cudaStream_t)stream);
+}

@@ -1,0 +1,150 @@
+// Real-field fused midpoint RK2 stage kernels.
+//
+//  * rk2_stage_generic: one site per thread (grid-stride), any lattice shape
+//    and storage; loads the 7-point stencil of phi and pi straight from HBM
+//    through L1.  Used for shapes the marching kernel does not cover.
+//  * rk2_stage_march (rk2_march.cuh): the bandwidth kernel for n2 % 4 == 0.
+#include "rk2_real.cuh"
+#include "rk2_march.cuh"
+#include "tipt_internal.h"
+
+namespace tipt {
+
+template <int S>
+__global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using TT = typename std::conditional<S == TIPT_F32C, float, double>::type;
+    TT* s_tab = reinterpret_cast<TT*>(smem_raw);
+    if (p.table_in_smem) stage_table<TT>(p, s_tab);
+    const float tminf = (float)p.tmin, dinvf = (float)p.dinv;
+
+    const int64_t n12 = (int64_t)p.n1 * p.n2;
+    const int64_t N = (int64_t)p.n0 * n12;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(s % p.n2);
+        const int64_t r = s / p.n2;
+        const int j = (int)(r % p.n1);
+        const int i = (int)(r / p.n1);
+        const int64_t o_ip = (i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12;
+        const int64_t o_im = (i > 0) ? -n12 : (int64_t)(p.n0 - 1) * n12;
+        const int64_t o_jp = (j + 1 < p.n1) ? p.n2 : -(int64_t)(p.n1 - 1) * p.n2;
+        const int64_t o_jm = (j > 0) ? -(int64_t)p.n2 : (int64_t)(p.n1 - 1) * p.n2;
+        const int64_t o_kp = (k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1);
+        const int64_t o_km = (k > 0) ? -1 : (int64_t)(p.n2 - 1);
+        const int64_t idx[7] = {s, s + o_ip, s + o_im, s + o_jp, s + o_jm, s + o_kp, s + o_km};
+        if constexpr (S == TIPT_F64) {
+            const double* phi = static_cast<const double*>(p.phi);
+            const double* pi = static_cast<const double*>(p.pi);
+            double ph[7], pv[7];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                ph[q] = __ldg(phi + idx[q]);
+                pv[q] = __ldg(pi + idx[q]);
+            }
+            double a, b;
+            update_f64(p, reinterpret_cast<const double*>(s_tab), ph, pv,
+                       site_noise<double>(p, (uint64_t)s), a, b);
+            static_cast<double*>(p.phi_out)[s] = a;
+            static_cast<double*>(p.pi_out)[s] = b;
+        } else if constexpr (S == TIPT_F32) {
+            const float* phi = static_cast<const float*>(p.phi);
+            const float* pi = static_cast<const float*>(p.pi);
+            float ph[7], pv[7];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                ph[q] = __ldg(phi + idx[q]);
+                pv[q] = __ldg(pi + idx[q]);
+            }
+            float a, b;
+            update_f32(p, reinterpret_cast<const double*>(s_tab), ph, pv,
+                       site_noise<float>(p, (uint64_t)s), a, b);
+            static_cast<float*>(p.phi_out)[s] = a;
+            static_cast<float*>(p.pi_out)[s] = b;
+        } else {
+            const float2* phi = static_cast<const float2*>(p.phi);
+            const float2* pi = static_cast<const float2*>(p.pi);
+            float2 ph[7], pv[7];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                ph[q] = __ldg(phi + idx[q]);
+                pv[q] = __ldg(pi + idx[q]);
+            }
+            float2 a, b;
+            update_f32c(p, reinterpret_cast<const float*>(s_tab), tminf, dinvf, ph, pv,
+                        site_noise<double>(p, (uint64_t)s), a, b);
+            static_cast<float2*>(p.phi_out)[s] = a;
+            static_cast<float2*>(p.pi_out)[s] = b;
+        }
+    }
+}
+
+// Bytes of shared memory the V' row needs for storage S (0 if polynomial).
+static int64_t table_smem_bytes(int S, const RealStageParams& p) {
+    if (p.vkind == TIPT_VP_POLY) return 0;
+    return (int64_t)p.npts * (S == TIPT_F32C ? 4 : 8);
+}
+
+static int g_num_sms = 0;
+int num_sms() {
+    if (g_num_sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g_num_sms <= 0) g_num_sms = 148;
+    }
+    return g_num_sms;
+}
+
+template <int S>
+static int launch_generic(RealStageParams p, int64_t smem, cudaStream_t st) {
+    auto kern = rk2_stage_generic<S>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return fail_cuda(e, "rk2_stage_generic smem attribute");
+    }
+    const int64_t N = (int64_t)p.n0 * p.n1 * p.n2;
+    int64_t blocks = (N + 255) / 256;
+    const int64_t cap = (int64_t)num_sms() * 8;
+    if (blocks > cap) blocks = cap;
+    kern<<<(unsigned)blocks, 256, (size_t)smem, st>>>(p);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "rk2_stage_generic launch");
+}
+
+// Largest V' row staged in shared memory; longer 1-D tables are read from
+// global memory (L1/L2 resident), longer 2-D tables are rejected.
+constexpr int64_t kMaxTableSmem = 96 * 1024;
+
+int launch_real_stage(int storage, RealStageParams p, cudaStream_t st) {
+    const int64_t tb = table_smem_bytes(storage, p);
+    p.table_in_smem = (tb > 0 && tb <= kMaxTableSmem) ? 1 : 0;
+    if (p.vkind == TIPT_VP_TABLE2D && !p.table_in_smem)
+        return fail(TIPT_ERR_UNSUPPORTED, "2-D V' table row of %d points exceeds %lld bytes of "
+                    "shared memory", p.npts, (long long)kMaxTableSmem);
+    const int64_t smem = p.table_in_smem ? tb : 0;
+    if (march_supported(storage, p)) return launch_march(storage, p, smem, st);
+    switch (storage) {
+        case TIPT_F64: return launch_generic<TIPT_F64>(p, smem, st);
+        case TIPT_F32: return launch_generic<TIPT_F32>(p, smem, st);
+        case TIPT_F32C: return launch_generic<TIPT_F32C>(p, smem, st);
+    }
+    return fail(TIPT_ERR_STORAGE, "unknown storage %d", storage);
+}
+
+int launch_real_stage_generic_only(int storage, RealStageParams p, cudaStream_t st) {
+    const int64_t tb = table_smem_bytes(storage, p);
+    p.table_in_smem = (tb > 0 && tb <= kMaxTableSmem) ? 1 : 0;
+    if (p.vkind == TIPT_VP_TABLE2D && !p.table_in_smem)
+        return fail(TIPT_ERR_UNSUPPORTED, "2-D V' table too large for shared memory");
+    const int64_t smem = p.table_in_smem ? tb : 0;
+    switch (storage) {
+        case TIPT_F64: return launch_generic<TIPT_F64>(p, smem, st);
+        case TIPT_F32: return launch_generic<TIPT_F32>(p, smem, st);
+        case TIPT_F32C: return launch_generic<TIPT_F32C>(p, smem, st);
+    }
+    return fail(TIPT_ERR_STORAGE, "unknown storage %d", storage);
+}
+
+}  // namespace tipt

@@ -1,0 +1,174 @@
+// Real-field midpoint RK2 stage: per-site arithmetic for the three storages
+// and the launch parameters shared by the generic and the marching kernels.
+//
+// One midpoint stage advances (phi, pi) by h2 using the midpoint state at h1
+// (R:1902-1966, rk2_step_table: h1 = dt/2, h2 = dt, noise factor 1; each half
+// of rk2_fused_table R:1742-1872: h1 = h2 = dt/2, noise factor 1/2).
+// phi~ = phi + h1*pi depends on the site alone, so the second pass's
+// Laplacian of phi~ needs only (phi, pi) on the 7-point stencil: the two
+// reference passes fuse into one launch with a radius-1 halo and no scratch.
+#pragma once
+
+#include "tipt_device.cuh"
+
+namespace tipt {
+
+struct RealStageParams {
+    const void* phi;
+    const void* pi;
+    void* phi_out;
+    void* pi_out;
+    int n0, n1, n2;      // lattice extents (nx, ny, nz); n2 contiguous
+    double h1, h2;       // midpoint offset, advance
+    double inv_dx2, eta, inv_mu2, inv_a2;
+    const void* noise;   // array noise (storage precision) or nullptr
+    double ns_eff;       // hash noise amplitude incl. the 1/2 of half steps
+    double nfac;         // array-noise factor (1 or 1/2)
+    uint64_t step, mul, seed;
+    // V' source
+    int vkind;           // TIPT_VP_*
+    int npts;
+    const double* table; // 1-D row or 2-D [nT][npts]
+    double tmin, dinv;
+    int nT;
+    double T_min, T_dinv, T;
+    double c1, c2, c3;
+    int table_in_smem;   // 1: stage (and blend) the row into dynamic smem
+};
+
+// Row-blend weight of a 2-D table (same trunc/clamp/unclamped-weight rule
+// along T as along phi).
+__device__ __forceinline__ void table2d_row(const RealStageParams& p, int& it, double& w) {
+    double ft = (p.T - p.T_min) * p.T_dinv;
+    double c = ft > 0.0 ? ft : 0.0;
+    c = c < double(p.nT - 2) ? c : double(p.nT - 2);
+    it = (int)c;
+    w = ft - double(it);
+}
+
+// Stage the V' row into shared memory as TT (blending the two bracketing T
+// rows for a 2-D table).  Called by every thread of the block; ends with a
+// barrier.
+template <typename TT>
+__device__ __forceinline__ void stage_table(const RealStageParams& p, TT* s_tab) {
+    if (p.vkind == TIPT_VP_TABLE) {
+        for (int q = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+             q < p.npts; q += blockDim.x * blockDim.y * blockDim.z)
+            s_tab[q] = (TT)__ldg(p.table + q);
+    } else if (p.vkind == TIPT_VP_TABLE2D) {
+        int it;
+        double w;
+        table2d_row(p, it, w);
+        const double* a = p.table + (int64_t)it * p.npts;
+        const double* b = a + p.npts;
+        for (int q = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+             q < p.npts; q += blockDim.x * blockDim.y * blockDim.z) {
+            double va = __ldg(a + q), vb = __ldg(b + q);
+            s_tab[q] = (TT)(va + w * (vb - va));
+        }
+    }
+    __syncthreads();
+}
+
+// V'(x) in FP64 from the staged row, the global 1-D table, or the polynomial.
+__device__ __forceinline__ double vprime_d(const RealStageParams& p, const double* s_tab, double x) {
+    if (p.vkind == TIPT_VP_POLY) return poly_vprime<double>(p.c1, p.c2, p.c3, x);
+    const double* t = p.table_in_smem ? s_tab : p.table;
+    return lerp_table<double>(t, p.tmin, p.dinv, p.npts - 2, x);
+}
+
+// V'(x) in FP32 from a float row staged in shared memory (F32C storage).
+__device__ __forceinline__ float vprime_f(const RealStageParams& p, const float* s_tab, float x,
+                                          float tmin, float dinv) {
+    if (p.vkind == TIPT_VP_POLY)
+        return poly_vprime<float>((float)p.c1, (float)p.c2, (float)p.c3, x);
+    if (p.table_in_smem) return lerp_table<float>(s_tab, tmin, dinv, p.npts - 2, x);
+    return (float)lerp_table<double>(p.table, p.tmin, p.dinv, p.npts - 2, (double)x);
+}
+
+// Noise increment for one site (FP64): array value * nfac, or ns_eff * z.
+template <typename NT>
+__device__ __forceinline__ double site_noise(const RealStageParams& p, uint64_t site) {
+    if (p.noise) return p.nfac * (double)static_cast<const NT*>(p.noise)[site];
+    if (p.ns_eff == 0.0) return 0.0;
+    return p.ns_eff * gauss_cos(noise_key(site, p.step, p.mul, p.seed));
+}
+
+// --------------------------------------------------------------- F64 ----
+// Stencil order ip, im, jp, jm, kp, km as R:1913-1920.
+__device__ __forceinline__ void update_f64(const RealStageParams& p, const double* s_tab,
+                                           const double ph[7], const double pv[7], double noise,
+                                           double& phi_new, double& pi_new) {
+    const double c = ph[0];
+    double lap = (ph[1] + ph[2] + ph[3] + ph[4] + ph[5] + ph[6] - 6.0 * c) * p.inv_dx2;
+    double pt[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) pt[q] = ph[q] + p.h1 * pv[q];
+    double lap2 = (pt[1] + pt[2] + pt[3] + pt[4] + pt[5] + pt[6] - 6.0 * pt[0]) * p.inv_dx2;
+    double k1 = p.inv_a2 * lap - p.eta * pv[0] - vprime_d(p, s_tab, c) * p.inv_mu2;
+    double pit = pv[0] + p.h1 * k1;
+    double k2 = p.inv_a2 * lap2 - p.eta * pit - vprime_d(p, s_tab, pt[0]) * p.inv_mu2;
+    phi_new = c + p.h2 * pit;
+    pi_new = pv[0] + (p.h2 * k2 + noise);
+}
+
+// --------------------------------------------------------------- F32 ----
+// The reference's float32 mode (USE_FLOAT32, R:348): float32 neighbour sums,
+// FP64 for the rest, float32 stores -- including the stored midpoint state
+// phi~, pi~ that pass 2 reads (R:1932-1933).
+__device__ __forceinline__ void update_f32(const RealStageParams& p, const double* s_tab,
+                                           const float ph[7], const float pv[7], double noise,
+                                           float& phi_new, float& pi_new) {
+    const float c = ph[0];
+    float s6 = ph[1] + ph[2] + ph[3] + ph[4] + ph[5] + ph[6];
+    double lap = ((double)s6 - 6.0 * (double)c) * p.inv_dx2;
+    float pt[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) pt[q] = __double2float_rn((double)ph[q] + p.h1 * (double)pv[q]);
+    float s6b = pt[1] + pt[2] + pt[3] + pt[4] + pt[5] + pt[6];
+    double lap2 = ((double)s6b - 6.0 * (double)pt[0]) * p.inv_dx2;
+    double k1 = p.inv_a2 * lap - p.eta * (double)pv[0] - vprime_d(p, s_tab, (double)c) * p.inv_mu2;
+    float pit = __double2float_rn((double)pv[0] + p.h1 * k1);
+    double k2 = p.inv_a2 * lap2 - p.eta * (double)pit -
+                vprime_d(p, s_tab, (double)pt[0]) * p.inv_mu2;
+    phi_new = __double2float_rn((double)c + p.h2 * (double)pit);
+    pi_new = __double2float_rn((double)pv[0] + (p.h2 * k2 + noise));
+}
+
+// -------------------------------------------------------------- F32C ----
+// float2 {hi, lo} storage.  Forces in FP32 from hi/lo differences (the
+// Laplacian of a smooth field is a difference of nearly equal values, so
+// hi - hi is exact and the lo parts carry the rest); the state updates
+// phi + h2*pi~ and pi + h2*k + noise are accumulated in FP64 and split back,
+// so increments far below ulp_fp32(phi) are kept.
+__device__ __forceinline__ void update_f32c(const RealStageParams& p, const float* s_tab,
+                                            float tminf, float dinvf, const float2 ph[7],
+                                            const float2 pv[7], double noise, float2& phi_new,
+                                            float2& pi_new) {
+    const float h1 = (float)p.h1;
+    float dph = 0.f, dpl = 0.f, dvh = 0.f, dvl = 0.f;
+#pragma unroll
+    for (int q = 1; q < 7; ++q) {
+        dph += ph[q].x - ph[0].x;
+        dpl += ph[q].y - ph[0].y;
+        dvh += pv[q].x - pv[0].x;
+        dvl += pv[q].y - pv[0].y;
+    }
+    const float inv_dx2 = (float)p.inv_dx2;
+    float lap = (dph + dpl) * inv_dx2;
+    float lapv = (dvh + dvl) * inv_dx2;
+    float lap2 = lap + h1 * lapv;  // Laplacian of phi~ = phi + h1 pi
+    float phc = ph[0].x + ph[0].y;
+    float pvc = pv[0].x + pv[0].y;
+    const float inv_a2 = (float)p.inv_a2, eta = (float)p.eta, inv_mu2 = (float)p.inv_mu2;
+    float k1 = inv_a2 * lap - eta * pvc - vprime_f(p, s_tab, phc, tminf, dinvf) * inv_mu2;
+    float pit = pvc + h1 * k1;
+    float pht = ph[0].x + (ph[0].y + h1 * pvc);
+    float k2 = inv_a2 * lap2 - eta * pit - vprime_f(p, s_tab, pht, tminf, dinvf) * inv_mu2;
+    double pi_d = join_f32c(pv[0]);
+    double pit_d = pi_d + p.h1 * (double)k1;
+    phi_new = split_f32c(join_f32c(ph[0]) + p.h2 * pit_d);
+    pi_new = split_f32c(pi_d + ((double)(p.h2 * (double)k2) + noise));
+}
+
+}  // namespace tipt

@@ -178,6 +178,25 @@ int tipt_observables(int storage, const void* phi, const void* pi, int64_t nx, i
                      double thr, double* out, void* workspace, int64_t workspace_bytes,
                      void* stream);
 
+/* ------------------------------------------------------------ control */
+
+/* Real-field stage kernel selection: 0 automatic (the TMA marching kernel where
+ * the shape allows: contiguous extent a multiple of 4 in [8, 1024]), 1 the
+ * generic one-site-per-thread kernel, 2 the marching kernel or an error.  Both
+ * kernels produce bitwise identical results.  No reference counterpart
+ * (the reference's only knob is the CPU tile size, R:1969-1970). */
+int tipt_set_kernel_policy(int policy);
+
+/* Marching-kernel tile shape: rows per tile, planes per work item and ring
+ * stages (each 0 = automatic).  Performance only; used by the autotuner. */
+int tipt_set_march_tiles(int rows, int planes, int stages);
+
+/* Device status word set by bounded device-side waits that expired
+ * (TIPT_ERR_TIMEOUT), 0 otherwise; clear != 0 resets it.  Synchronises the
+ * device.  Counterpart of the reference's host NaN/divergence guard in spirit
+ * (R:3882-3944): failures are reported, never trapped. */
+int tipt_device_status(int* status, int clear);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,127 @@
+"""The TMA marching stage kernel against the generic stage kernel (bitwise: both
+run the same per-site arithmetic) and against the CPU oracle."""
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+from oracle import oracle as O  # noqa: E402
+from thermal_inflation_phase_transition_b200 import _lib as L  # noqa: E402
+from thermal_inflation_phase_transition_b200 import real_field as RF  # noqa: E402
+from thermal_inflation_phase_transition_b200._common import poly_source, table_source  # noqa: E402
+
+DEV = "cuda"
+
+
+@pytest.fixture(autouse=True)
+def _reset_policy():
+    yield
+    L.set_kernel_policy(0)
+    L.set_march_tiles(0, 0, 0)
+
+
+def _state(shape, storage, seed):
+    g = torch.Generator(device=DEV)
+    g.manual_seed(seed)
+    phi = 0.6 + 0.7 * torch.randn(shape, dtype=torch.float64, device=DEV, generator=g)
+    pi = 0.4 * torch.randn(shape, dtype=torch.float64, device=DEV, generator=g)
+    if storage == "f32c":
+        return RF.to_f32c(phi), RF.to_f32c(pi)
+    return phi, pi
+
+
+def _run(policy, shape, storage, steps=3, tiles=(0, 0), table2d=False):
+    L.set_kernel_policy(policy)
+    L.set_march_tiles(*tiles)
+    phi, pi = _state(shape, storage, 11)
+    if table2d:
+        t2, tmin, dinv, Tmin, Tdinv = O.build_table_2d(O.toy_vprime, 0.0, 3.0, 4096, 0.97, 1.06,
+                                                        64)
+        tab = torch.from_numpy(t2).to(DEV)
+    else:
+        t1, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.01), 0.0, 3.0, 4096)
+        tab = torch.from_numpy(t1).to(DEV)
+    a = [phi, pi]
+    b = [torch.empty_like(phi), torch.empty_like(pi)]
+    for n in range(steps):
+        T = 1.04 - 0.001 * n
+        vs = table_source(tab, tmin, dinv, 4096, T, Tmin, Tdinv) if table2d else \
+            table_source(tab, tmin, dinv, 4096)
+        RF.rk2_step_table_into(a[0], a[1], b[0], b[1], 0.05, 1.0, 0.9, 1.0, 1.0, vs,
+                               noise_scale=math.sqrt(2 * T * 0.05), noise_step=n, seed=7)
+        a, b = b, a
+    torch.cuda.synchronize()
+    return a
+
+
+SHAPES = [(16, 8, 64), (7, 8, 48), (70, 8, 16), (32, 32, 32), (9, 4, 512), (24, 32, 1),
+          (1, 16, 128), (128, 1, 1), (5, 12, 96),
+          # shared-memory rows that are not a multiple of 128 bytes (padded pitch)
+          (32, 24, 1), (8, 16, 40), (3, 8, 288)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("storage", ["f32c", "f64"])
+def test_march_equals_generic(shape, storage):
+    ref = _run(1, shape, storage)
+    got = _run(2, shape, storage)
+    assert torch.equal(ref[0], got[0]) and torch.equal(ref[1], got[1])
+    assert L.device_status() == 0
+
+
+@pytest.mark.parametrize("tiles", [(2, 1), (2, 3), (4, 5, 3), (8, 64), (16, 7, 5), (16, 40, 4)])
+def test_march_tilings_agree(tiles):
+    shape = (37, 16, 64)
+    ref = _run(1, shape, "f32c", steps=2)
+    got = _run(2, shape, "f32c", steps=2, tiles=tiles)
+    assert torch.equal(ref[0], got[0]) and torch.equal(ref[1], got[1])
+
+
+def test_march_2d_table():
+    shape = (20, 12, 96)
+    ref = _run(1, shape, "f32c", table2d=True)
+    got = _run(2, shape, "f32c", table2d=True)
+    assert torch.equal(ref[0], got[0]) and torch.equal(ref[1], got[1])
+
+
+def test_march_f64_vs_oracle():
+    shape = (18, 8, 32)
+    rng = np.random.default_rng(4)
+    phi0, pi0 = rng.normal(0.6, 0.7, shape), rng.normal(0, 0.4, shape)
+    tab, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.0), 0.0, 3.0, 4096)
+    a, b = phi0.copy(), pi0.copy()
+    for n in range(4):
+        O.rk2_step_table(a, b, 0.05, 1.0, 1.0, 1.0, None, np.empty(shape), np.empty(shape), 1.0,
+                         tab, tmin, dinv, 4096, noise_scale=0.31, noise_step=n, noise_seed=2)
+    L.set_kernel_policy(2)
+    phi, pi = torch.from_numpy(phi0).to(DEV), torch.from_numpy(pi0).to(DEV)
+    pt, vt = torch.empty_like(phi), torch.empty_like(pi)
+    for n in range(4):
+        RF.rk2_step_table(phi, pi, 0.05, 1.0, 1.0, 1.0, None, pt, vt, 1.0,
+                          torch.from_numpy(tab).to(DEV), tmin, dinv, 4096, noise_scale=0.31,
+                          noise_step=n, seed=2)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(phi.cpu().numpy(), a, atol=1e-13)
+    np.testing.assert_allclose(pi.cpu().numpy(), b, atol=1e-13)
+
+
+def test_fp32_box_muller_accuracy():
+    """F32C kicks: FP32 Box-Muller of the exact hash bits vs the FP64 z."""
+    shape = (64, 64, 64)
+    zero = torch.zeros(shape + (2,), dtype=torch.float32, device=DEV)
+    phi, pi = zero.clone(), zero.clone()
+    po, vo = torch.empty_like(phi), torch.empty_like(pi)
+    # V' = 0, dt = 0: pi' = kick = ns * z exactly
+    RF.rk2_step_table_into(phi, pi, po, vo, 0.0, 1.0, 0.0, 1.0, 1.0, poly_source(0, 0, 0),
+                           noise_scale=1.0, noise_step=17, seed=3)
+    torch.cuda.synchronize()
+    z32 = RF.from_f32c(vo).cpu().numpy()
+    z64 = O.noise_field(shape, 17, O.K_PASS2, 3, 1.0, 0)
+    err = np.abs(z32 - z64)
+    assert err.max() < 2e-6 * max(1.0, np.abs(z64).max())
+    rel = err / np.maximum(np.abs(z64), 1e-3)
+    assert np.median(rel) < 3e-7

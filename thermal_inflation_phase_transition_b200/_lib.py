@@ -62,6 +62,9 @@ _SIGS = {
     "tipt_observables_workspace_size": [_i64, _i64, _i64],
     "tipt_observables": [_i, _p, _p, _i64, _i64, _i64, _d, _d, _d, _d, _d, _d, _p, _p, _i64,
                          _p],
+    "tipt_set_kernel_policy": [_i],
+    "tipt_set_march_tiles": [_i, _i, _i],
+    "tipt_device_status": [C.POINTER(C.c_int), _i],
 }
 _RESTYPE = {"tipt_version": C.c_char_p, "tipt_status_string": C.c_char_p,
             "tipt_last_error": C.c_char_p, "tipt_observables_workspace_size": C.c_int64}
@@ -100,3 +103,20 @@ def check(status: int, where: str) -> None:
 
 def call(name: str, *args) -> None:
     check(getattr(lib(), name)(*args), name)
+
+
+def set_kernel_policy(policy: int) -> None:
+    """0 automatic, 1 generic stage kernel, 2 marching stage kernel (tests/tuning)."""
+    call("tipt_set_kernel_policy", int(policy))
+
+
+def set_march_tiles(rows: int = 0, planes: int = 0, stages: int = 0) -> None:
+    """Marching-kernel tile shape (0 = automatic); performance only."""
+    call("tipt_set_march_tiles", int(rows), int(planes), int(stages))
+
+
+def device_status(clear: bool = False) -> int:
+    """Device status word of bounded device waits (0 = ok).  Synchronises."""
+    v = C.c_int(0)
+    call("tipt_device_status", C.byref(v), int(bool(clear)))
+    return v.value

@@ -1,13 +1,528 @@
-// Marching (2.5-D blocked) real-field stage kernel.
+// Marching (2.5-D blocked) real-field midpoint stage for 8-byte storages
+// (F32C float2 pairs and F64), the bandwidth kernel of the stepper.
+//
+// Work item = (j-block of TJ rows, i-chunk of CI planes); a CTA owns full rows
+// along the contiguous axis n2, so the k-direction wrap stays inside shared
+// memory.  Per plane the CTA needs TJ+2 rows (one halo row each side, rows
+// taken modulo n1 = periodic wrap in j) of phi and pi.
+//
+// Warp roles.  The last warp is the producer: one lane loads each plane with
+// TMA (cp.async.bulk.tensor.3d, one BK x 1 x 1 box per row segment, every
+// coordinate reduced modulo its extent, so no copy leaves the tensor) into an
+// S-stage ring.  Stage s has a `full` mbarrier (producer's expect-tx arrival +
+// the copy bytes) and an `empty` mbarrier (one arrival per consumer warp).
+// Consumer warps compute plane i from the ring (j and k neighbours), a register
+// queue (prev, cur, next) of their own four sites (i neighbours) and release a
+// stage as soon as they have read it; there is no CTA-wide barrier in the
+// loop, so warps drift freely within the ring's slack.  Each consumer thread
+// owns the site pairs {2t, 2t+1} and {n2/2 + 2t, n2/2 + 2t + 1} of its row, so
+// the 16-byte shared loads and global stores of a warp are contiguous.
+//
+// Every mbarrier wait is bounded by the global timer (2 s); on expiry the
+// thread records TIPT_ERR_TIMEOUT in a device status word and returns; the
+// producer drains the copies it issued (bounded) before it exits.
+#include <cuda.h>
+
 #include "rk2_march.cuh"
 #include "tipt_internal.h"
 
 namespace tipt {
 
-bool march_supported(int, const RealStageParams&) { return false; }
+__device__ int g_device_status = 0;  // 0 ok; TIPT_ERR_TIMEOUT after a wait expired
 
-int launch_march(int, const RealStageParams&, int64_t, cudaStream_t) {
-    return fail(TIPT_ERR_UNSUPPORTED, "marching kernel not built");
+constexpr uint64_t kWaitNs = 2000000000ull;
+
+// ---------------------------------------------------------------- PTX -----
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: true when the phase completed, false after kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    if (mbar_test(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_test(bar, parity))
+        if (global_ns() - t0 > kWaitNs) return false;
+    return true;
+}
+__device__ __forceinline__ void tma_row(void* dst, const CUtensorMap* tm, int k, int j, int i,
+                                        uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(k), "r"(j), "r"(i), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// -------------------------------------------------------------- params -----
+struct MarchGeom {
+    int TJ;        // rows per tile
+    int CI;        // planes per i-chunk
+    int BK;        // TMA box width (elements), divides n2
+    int pitch;     // shared-memory row pitch (elements); pitch*8 is a multiple of 128
+    int S;         // ring stages
+    int nJB, nIC;  // j-blocks, i-chunks
+    int items;
+    int tab_bytes;    // staged V' row (bytes, 128-aligned)
+    int stage_bytes;  // one ring stage: phi and pi tiles
+};
+
+template <int S>
+struct MarchElem;
+template <>
+struct MarchElem<TIPT_F32C> {
+    using E = float2;
+    using TT = float;
+};
+template <>
+struct MarchElem<TIPT_F64> {
+    using E = double;
+    using TT = double;
+};
+
+// 16-byte pair loads/stores of two consecutive 8-byte elements.
+template <typename E>
+__device__ __forceinline__ void ld_pair_s(const E* p, E& a, E& b) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    a = *reinterpret_cast<const E*>(&v.x);
+    b = *reinterpret_cast<const E*>(&v.z);
+}
+template <typename E>
+__device__ __forceinline__ void st_pair_g(E* p, const E& a, const E& b) {
+    float4 v;
+    *reinterpret_cast<E*>(&v.x) = a;
+    *reinterpret_cast<E*>(&v.z) = b;
+    *reinterpret_cast<float4*>(p) = v;
+}
+template <typename E>
+__device__ __forceinline__ void ld_pair_g(const E* p, E& a, E& b) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    a = *reinterpret_cast<const E*>(&v.x);
+    b = *reinterpret_cast<const E*>(&v.z);
+}
+
+template <int S>
+__device__ __forceinline__ void site_update(const RealStageParams& p, const void* s_tab,
+                                            float tminf, float dinvf,
+                                            const typename MarchElem<S>::E ph[7],
+                                            const typename MarchElem<S>::E pv[7], uint64_t site,
+                                            typename MarchElem<S>::E& a,
+                                            typename MarchElem<S>::E& b) {
+    if constexpr (S == TIPT_F32C)
+        update_f32c(p, static_cast<const float*>(s_tab), tminf, dinvf, ph, pv,
+                    site_kick_f32c(p, site), a, b);
+    else
+        update_f64(p, static_cast<const double*>(s_tab), ph, pv, site_noise<double>(p, site), a,
+                   b);
+}
+
+// Launch bounds of the two block-size classes: up to 256 consumer threads
+// (two CTAs per SM) or up to 512 (one CTA per SM), plus the producer warp.
+// Ring position -> (stage, phase parity), advanced incrementally.
+struct RingPos {
+    uint32_t stage, phase;
+    __device__ __forceinline__ void next(uint32_t ns) {
+        if (++stage == ns) {
+            stage = 0;
+            phase ^= 1u;
+        }
+    }
+};
+
+// 17-18 warps per SM must fit the four 16K-register sub-partitions.
+constexpr int kMarchRegs = 96;
+
+template <int S, bool WIDE>
+__global__ void __maxnreg__(kMarchRegs)
+    rk2_stage_march(const __grid_constant__ CUtensorMap tm_phi,
+                    const __grid_constant__ CUtensorMap tm_pi, RealStageParams p, MarchGeom g) {
+    using E = typename MarchElem<S>::E;
+    using TT = typename MarchElem<S>::TT;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // carve from a 128-byte aligned base (TMA destinations need 128-byte
+    // alignment; the allocation carries 128 bytes of slack for this)
+    unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    TT* s_tab = reinterpret_cast<TT*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + g.tab_bytes);
+    uint64_t* empty = full + 8;
+    unsigned char* ring = smem + g.tab_bytes + 128;
+
+    const int n0 = p.n0, n1 = p.n1, n2 = p.n2;
+    const int pitch = g.pitch;
+    const int TJ = g.TJ;
+    const uint32_t NS = (uint32_t)g.S;
+    const int rows = TJ + 2;
+    const int tpr = n2 >> 2;          // consumer threads per row
+    const int nc = TJ * tpr;          // consumer threads (a multiple of 32)
+    const int t = threadIdx.x;
+
+    if (t == 0) {
+        for (uint32_t s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], nc / 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (p.table_in_smem) stage_table<TT>(p, s_tab);  // ends with __syncthreads
+    else __syncthreads();
+
+    const size_t half_stage = (size_t)(g.stage_bytes >> 1);
+    auto fld = [&](uint32_t stage, int f) -> E* {
+        return reinterpret_cast<E*>(ring + (size_t)stage * g.stage_bytes + (size_t)f * half_stage);
+    };
+
+    // ------------------------------------------------------------ producer
+    // Each item loads planes i0-1 .. i0+ni (ni + 2 ring positions).
+    if (t >= nc) {
+        if (t != nc) return;
+        const uint32_t plane_tx = (uint32_t)(2 * rows * n2 * (int)sizeof(E));
+        RingPos w{0, 0};
+        uint32_t issued = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
+            const int ic = item / g.nJB;
+            const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+            const int npl = min(g.CI, n0 - i0) + 2;
+            for (int q = 0; q < npl; ++q) {
+                // stage w.stage last held position issued - NS, released in phase w.phase ^ 1
+                if (issued >= NS && !mbar_wait(&empty[w.stage], w.phase ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(&full[w.stage], plane_tx);
+                int iw = i0 - 1 + q;
+                iw = iw < 0 ? iw + n0 : (iw >= n0 ? iw - n0 : iw);
+                for (int rr = 0; rr < rows; ++rr) {
+                    int jr = j0 - 1 + rr;
+                    jr = jr < 0 ? jr + n1 : (jr >= n1 ? jr - n1 : jr);
+                    for (int kb = 0; kb < n2; kb += g.BK) {
+                        tma_row(fld(w.stage, 0) + rr * pitch + kb, &tm_phi, kb, jr, iw, &full[w.stage]);
+                        tma_row(fld(w.stage, 1) + rr * pitch + kb, &tm_pi, kb, jr, iw, &full[w.stage]);
+                    }
+                }
+                ++issued;
+                w.next(NS);
+            }
+        }
+        if (!ok) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+        // keep the CTA alive until the last copies issued have landed (bounded):
+        // walk back over the last min(NS, issued) positions
+        RingPos d = w;
+        for (uint32_t k = 0; k < NS && k < issued; ++k) {
+            d.stage = d.stage == 0 ? NS - 1 : d.stage - 1;
+            if (d.stage == NS - 1) d.phase ^= 1u;
+            (void)mbar_wait(&full[d.stage], d.phase);
+        }
+        return;
+    }
+
+    // ----------------------------------------------------------- consumers
+    const int lane = t & 31;
+    const int r = 1 + t / tpr;               // own tile row (1..TJ)
+    const int c = 2 * (t - (r - 1) * tpr);   // first column of pair A
+    const int half = n2 >> 1;
+    const int kmA = c == 0 ? n2 - 1 : c - 1;                  // left of pair A
+    const int kpA = c + 2;                                    // right of pair A
+    const int kmB = half + c - 1;                             // left of pair B
+    const int kpB = half + c + 2 == n2 ? 0 : half + c + 2;    // right of pair B
+    const float tminf = (float)p.tmin, dinvf = (float)p.dinv;
+    E* const phi_out = static_cast<E*>(p.phi_out);
+    E* const pi_out = static_cast<E*>(p.pi_out);
+    const int orow = r * pitch, urow = (r - 1) * pitch, drow = (r + 1) * pitch;
+
+    RingPos pm{0, 0};  // ring position of plane i-1 for the current iteration
+    for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
+        const int ic = item / g.nJB;
+        const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+        const int ni = min(g.CI, n0 - i0);
+        const int jw = j0 + r - 1;
+        RingPos pc = pm, pp;
+        pc.next(NS);
+        pp = pc;
+        pp.next(NS);
+        if (!mbar_wait(&full[pm.stage], pm.phase) || !mbar_wait(&full[pc.stage], pc.phase)) {
+            if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+            return;
+        }
+        for (int q = 0; q < ni; ++q) {
+            if (!mbar_wait(&full[pp.stage], pp.phase)) {
+                if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+                return;
+            }
+            const int i = i0 + q;
+            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {   // pair A (h = 0), pair B (h = 1)
+                const int col = h ? half + c : c;
+                const int kl_ = h ? kmB : kmA;
+                const int kr_ = h ? kpB : kpA;
+                E ce[2][2], ip[2][2], im[2][2], jp[2][2], jm[2][2], kl[2], kr[2];
+#pragma unroll
+                for (int f = 0; f < 2; ++f) {
+                    const E* sc = fld(pc.stage, f);
+                    ld_pair_s(sc + orow + col, ce[f][0], ce[f][1]);
+                    ld_pair_s(sc + urow + col, jm[f][0], jm[f][1]);
+                    ld_pair_s(sc + drow + col, jp[f][0], jp[f][1]);
+                    kl[f] = sc[orow + kl_];
+                    kr[f] = sc[orow + kr_];
+                    ld_pair_s(fld(pm.stage, f) + orow + col, im[f][0], im[f][1]);
+                    ld_pair_s(fld(pp.stage, f) + orow + col, ip[f][0], ip[f][1]);
+                }
+                if (h == 1) {  // this warp is done with plane i-1
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[pm.stage]);
+                }
+                E op[2], ov[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    // stencil order: centre, ip, im, jp, jm, kp, km (R:1913-1920)
+                    const E ph[7] = {ce[0][u], ip[0][u], im[0][u], jp[0][u], jm[0][u],
+                                     u ? kr[0] : ce[0][1], u ? ce[0][0] : kl[0]};
+                    const E pv[7] = {ce[1][u], ip[1][u], im[1][u], jp[1][u], jm[1][u],
+                                     u ? kr[1] : ce[1][1], u ? ce[1][0] : kl[1]};
+                    uint64_t site;
+                    if constexpr (WIDE) site = (uint64_t)(rowoff + col + u);
+                    else site = (uint32_t)rowoff + (uint32_t)(col + u);
+                    site_update<S>(p, s_tab, tminf, dinvf, ph, pv, site, op[u], ov[u]);
+                }
+                st_pair_g(phi_out + rowoff + col, op[0], op[1]);
+                st_pair_g(pi_out + rowoff + col, ov[0], ov[1]);
+            }
+            pm = pc;
+            pc = pp;
+            pp.next(NS);
+        }
+        // planes i0+ni-1 and i0+ni were read for the last time
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(&empty[pm.stage]);
+            mbar_arrive(&empty[pc.stage]);
+        }
+        pm = pp;  // the next item starts at the following ring position
+    }
+}
+
+// ------------------------------------------------------------------ host ---
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeFn encode_fn() {
+    static EncodeFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeFn>(f);
+    }
+    return fn;
+}
+
+static bool make_map(CUtensorMap* tm, const void* base, int n0, int n1, int n2, int BK) {
+    EncodeFn enc = encode_fn();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)n2, (cuuint64_t)n1, (cuuint64_t)n0};
+    const cuuint64_t strides[2] = {(cuuint64_t)n2 * 8, (cuuint64_t)n2 * 8 * n1};
+    const cuuint32_t box[3] = {(cuuint32_t)BK, 1, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides, box,
+               es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
+// Tile shape; 0 = choose automatically.  Set by tipt_set_march_tiles().
+static int g_force_tj = 0, g_force_ci = 0, g_force_stages = 0;
+
+// TMA box width.  A tensor copy's shared-memory destination must be 128-byte
+// aligned: rows sit at multiples of the (128-byte) pitch, and a row split into
+// several boxes needs box widths of a multiple of 16 elements (128 bytes).
+static int pick_bk(int n2) {
+    if (n2 <= 256) return n2;
+    for (int bk = 256; bk >= 16; bk -= 16)
+        if (n2 % bk == 0) return bk;
+    return 0;
+}
+
+static int round128(int x) { return (x + 127) & ~127; }
+
+constexpr int kSmemPerSm = 228 * 1024;   // B200 shared memory per SM
+constexpr int kSmemPerCta = 227 * 1024;  // largest opt-in allocation per CTA
+constexpr int kSmemReserve = 1024;       // per-CTA reservation of the runtime
+constexpr int kWarpsPerSm = 18;          // at kMarchRegs registers per thread
+
+static int64_t smem_need(const MarchGeom& g) {
+    return 128 + (int64_t)g.tab_bytes + 128 + (int64_t)g.S * g.stage_bytes;  // + alignment slack
+}
+
+// CTAs per SM for a geometry (shared memory and register-file bound).
+static int ctas_per_sm(const MarchGeom& g, int tpr) {
+    const int64_t need = smem_need(g) + kSmemReserve;
+    int by_smem = (int)(kSmemPerSm / need);
+    const int warps = g.TJ * tpr / 32 + 1;
+    int by_warps = kWarpsPerSm / warps;
+    return by_smem < by_warps ? by_smem : by_warps;
+}
+
+static bool geometry(const RealStageParams& p, int64_t smem_table, MarchGeom& g, int64_t& smem) {
+    const int n1 = p.n1, n2 = p.n2;
+    if (n2 % 4 != 0 || n2 < 8 || n2 > 2048) return false;
+    g.BK = pick_bk(n2);
+    if (!g.BK) return false;
+    g.pitch = (n2 + 15) & ~15;
+    const int tpr = n2 / 4;
+    g.tab_bytes = round128((int)smem_table);
+    g.CI = g_force_ci > 0 ? g_force_ci : 64;
+    if (g.CI > p.n0) g.CI = p.n0;
+    // Candidates: TJ with TJ*tpr consumers a multiple of 32 in [32, 512], ring
+    // depth S in [3, 5].  Score = consumer warps per SM x TJ/(TJ+2) (the share
+    // of loaded rows that are not halo), deeper rings preferred on ties.
+    double best = -1.0;
+    MarchGeom pick{};
+    for (int tj = 1; tj <= 64; ++tj) {
+        if (g_force_tj > 0 && tj != g_force_tj) continue;
+        if (n1 % tj || (tj * tpr) % 32 || tj * tpr > 512) continue;
+        for (int st = 3; st <= 5; ++st) {
+            if (g_force_stages > 0 && st != g_force_stages) continue;
+            MarchGeom c = g;
+            c.TJ = tj;
+            c.S = st;
+            c.stage_bytes = 2 * round128((tj + 2) * c.pitch * 8);
+            if (smem_need(c) > kSmemPerCta) continue;
+            const int cps = ctas_per_sm(c, tpr);
+            if (cps < 1) continue;
+            const double score = cps * (tj * tpr / 32) * (double)tj / (tj + 2) + 0.01 * st;
+            if (score > best) {
+                best = score;
+                pick = c;
+            }
+        }
+    }
+    if (best < 0) return false;
+    g = pick;
+    // every TMA destination (ring + stage*stage_bytes + f*stage_bytes/2 +
+    // (rr*pitch + kb)*8) must be 128-byte aligned
+    if ((g.pitch * 8) % 128 || (g.BK * 8) % 128 && g.BK != n2 || g.stage_bytes % 256 ||
+        g.tab_bytes % 128)
+        return false;
+    g.nJB = n1 / g.TJ;
+    g.nIC = (p.n0 + g.CI - 1) / g.CI;
+    g.items = g.nJB * g.nIC;
+    smem = smem_need(g);
+    return true;
+}
+
+bool march_supported(int storage, const RealStageParams& p) {
+    if (storage != TIPT_F32C && storage != TIPT_F64) return false;
+    if (!encode_fn()) return false;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p.phi) | reinterpret_cast<uintptr_t>(p.pi) |
+                        reinterpret_cast<uintptr_t>(p.phi_out) |
+                        reinterpret_cast<uintptr_t>(p.pi_out);
+    if (a % 16) return false;
+    MarchGeom g;
+    int64_t smem;
+    int64_t tb = p.table_in_smem ? (int64_t)p.npts * (storage == TIPT_F32C ? 4 : 8) : 0;
+    return geometry(p, tb, g, smem);
+}
+
+template <int S, bool WIDE>
+static int launch_march_t(const RealStageParams& p, const MarchGeom& g, int64_t smem,
+                          cudaStream_t st) {
+    CUtensorMap tphi, tpi;
+    if (!make_map(&tphi, p.phi, p.n0, p.n1, p.n2, g.BK) ||
+        !make_map(&tpi, p.pi, p.n0, p.n1, p.n2, g.BK))
+        return fail(TIPT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    auto kern = rk2_stage_march<S, WIDE>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return fail_cuda(e, "rk2_stage_march attributes");
+    const int threads = g.TJ * (p.n2 / 4) + 32;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, (size_t)smem);
+    if (e != cudaSuccess || per_sm < 1)
+        return fail(TIPT_ERR_UNSUPPORTED, "rk2_stage_march does not fit an SM (%d threads, %lld "
+                    "bytes of shared memory)", threads, (long long)smem);
+    int grid = num_sms() * per_sm;
+    if (grid > g.items) grid = g.items;
+    kern<<<grid, threads, (size_t)smem, st>>>(tphi, tpi, p, g);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "rk2_stage_march launch");
+}
+
+int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cudaStream_t st) {
+    MarchGeom g;
+    int64_t smem;
+    if (!geometry(p, smem_table, g, smem))
+        return fail(TIPT_ERR_UNSUPPORTED, "marching kernel geometry");
+    const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
+    if (storage == TIPT_F32C)
+        return wide ? launch_march_t<TIPT_F32C, true>(p, g, smem, st)
+                    : launch_march_t<TIPT_F32C, false>(p, g, smem, st);
+    if (storage == TIPT_F64)
+        return wide ? launch_march_t<TIPT_F64, true>(p, g, smem, st)
+                    : launch_march_t<TIPT_F64, false>(p, g, smem, st);
+    return fail(TIPT_ERR_STORAGE, "marching kernel takes F32C or F64");
 }
 
 }  // namespace tipt
+
+using namespace tipt;
+
+// Tile shape of the marching kernel: rows per tile, planes per i-chunk and
+// ring stages (0 = automatic).  Used by the autotuner; performance only.
+extern "C" int tipt_set_march_tiles(int rows, int planes, int stages) {
+    if (rows < 0 || planes < 0 || stages < 0 || (stages > 0 && stages < 3) || stages > 5)
+        return fail(TIPT_ERR_ARG, "bad tile shape");
+    g_force_tj = rows;
+    g_force_ci = planes;
+    g_force_stages = stages;
+    return TIPT_OK;
+}
+
+// Reads (and with clear != 0 resets) the device status word that bounded
+// device-side waits set on expiry.  Synchronises the device.
+extern "C" int tipt_device_status(int* status, int clear) {
+    if (!status) return fail(TIPT_ERR_ARG, "status is NULL");
+    cudaError_t e = cudaMemcpyFromSymbol(status, g_device_status, sizeof(int));
+    if (e != cudaSuccess) return fail_cuda(e, "read device status");
+    if (clear) {
+        const int zero = 0;
+        e = cudaMemcpyToSymbol(g_device_status, &zero, sizeof(int));
+        if (e != cudaSuccess) return fail_cuda(e, "clear device status");
+    }
+    return TIPT_OK;
+}

@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p) {
             }
             float2 a, b;
             update_f32c(p, reinterpret_cast<const float*>(s_tab), tminf, dinvf, ph, pv,
-                        site_noise<double>(p, (uint64_t)s), a, b);
+                        site_kick_f32c(p, (uint64_t)s), a, b);
             static_cast<float2*>(p.phi_out)[s] = a;
             static_cast<float2*>(p.pi_out)[s] = b;
         }
@@ -117,28 +117,37 @@ static int launch_generic(RealStageParams p, int64_t smem, cudaStream_t st) {
 // global memory (L1/L2 resident), longer 2-D tables are rejected.
 constexpr int64_t kMaxTableSmem = 96 * 1024;
 
+// Kernel choice: 0 automatic, 1 generic kernel only, 2 marching kernel only.
+static int g_kernel_policy = 0;
+
+// A lattice whose contiguous extent is 1 (the reference's 2-D form nz = 1) is
+// relabelled so the contiguous axis is the longest non-trivial one: (nx, ny, 1)
+// -> (1, nx, ny) and (nx, 1, 1) -> (1, 1, nx).  Linear site indices, hence the
+// noise keys, are unchanged; the neighbour set of every site is the same.
+static void canonical_shape(RealStageParams& p) {
+    if (p.n2 != 1) return;
+    if (p.n1 > 1) {
+        p.n2 = p.n1;
+        p.n1 = p.n0;
+        p.n0 = 1;
+    } else {
+        p.n2 = p.n0;
+        p.n0 = 1;
+    }
+}
+
 int launch_real_stage(int storage, RealStageParams p, cudaStream_t st) {
+    canonical_shape(p);
     const int64_t tb = table_smem_bytes(storage, p);
     p.table_in_smem = (tb > 0 && tb <= kMaxTableSmem) ? 1 : 0;
     if (p.vkind == TIPT_VP_TABLE2D && !p.table_in_smem)
         return fail(TIPT_ERR_UNSUPPORTED, "2-D V' table row of %d points exceeds %lld bytes of "
                     "shared memory", p.npts, (long long)kMaxTableSmem);
     const int64_t smem = p.table_in_smem ? tb : 0;
-    if (march_supported(storage, p)) return launch_march(storage, p, smem, st);
-    switch (storage) {
-        case TIPT_F64: return launch_generic<TIPT_F64>(p, smem, st);
-        case TIPT_F32: return launch_generic<TIPT_F32>(p, smem, st);
-        case TIPT_F32C: return launch_generic<TIPT_F32C>(p, smem, st);
-    }
-    return fail(TIPT_ERR_STORAGE, "unknown storage %d", storage);
-}
-
-int launch_real_stage_generic_only(int storage, RealStageParams p, cudaStream_t st) {
-    const int64_t tb = table_smem_bytes(storage, p);
-    p.table_in_smem = (tb > 0 && tb <= kMaxTableSmem) ? 1 : 0;
-    if (p.vkind == TIPT_VP_TABLE2D && !p.table_in_smem)
-        return fail(TIPT_ERR_UNSUPPORTED, "2-D V' table too large for shared memory");
-    const int64_t smem = p.table_in_smem ? tb : 0;
+    const bool march = g_kernel_policy != 1 && march_supported(storage, p);
+    if (g_kernel_policy == 2 && !march)
+        return fail(TIPT_ERR_UNSUPPORTED, "marching kernel does not cover this shape/storage");
+    if (march) return launch_march(storage, p, smem, st);
     switch (storage) {
         case TIPT_F64: return launch_generic<TIPT_F64>(p, smem, st);
         case TIPT_F32: return launch_generic<TIPT_F32>(p, smem, st);
@@ -148,3 +157,12 @@ int launch_real_stage_generic_only(int storage, RealStageParams p, cudaStream_t 
 }
 
 }  // namespace tipt
+
+// Selects the real-field stage kernel: 0 automatic (the marching kernel where it
+// applies), 1 the generic kernel, 2 the marching kernel or an error.  Results are
+// bitwise identical between the two kernels; this exists for tests and tuning.
+extern "C" int tipt_set_kernel_policy(int policy) {
+    if (policy < 0 || policy > 2) return tipt::fail(TIPT_ERR_ARG, "policy must be 0, 1 or 2");
+    tipt::g_kernel_policy = policy;
+    return TIPT_OK;
+}

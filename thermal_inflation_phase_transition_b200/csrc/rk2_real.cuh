@@ -89,27 +89,36 @@ __device__ __forceinline__ float vprime_f(const RealStageParams& p, const float*
 // Noise increment for one site (FP64): array value * nfac, or ns_eff * z.
 template <typename NT>
 __device__ __forceinline__ double site_noise(const RealStageParams& p, uint64_t site) {
-    if (p.noise) return p.nfac * (double)static_cast<const NT*>(p.noise)[site];
+    if (p.noise) return __dmul_rn(p.nfac, (double)static_cast<const NT*>(p.noise)[site]);
     if (p.ns_eff == 0.0) return 0.0;
-    return p.ns_eff * gauss_cos(noise_key(site, p.step, p.mul, p.seed));
+    return __dmul_rn(p.ns_eff, gauss_cos(noise_key(site, p.step, p.mul, p.seed)));
 }
 
 // --------------------------------------------------------------- F64 ----
-// Stencil order ip, im, jp, jm, kp, km as R:1913-1920.
+// Stencil order ip, im, jp, jm, kp, km as R:1913-1920.  Every operation is an
+// explicit round-to-nearest intrinsic, so each kernel that calls this produces
+// the same bits (no compiler-chosen contraction).
+__device__ __forceinline__ double sum6_d(const double v[7]) {
+    return __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(v[1], v[2]), v[3]), v[4]), v[5]), v[6]);
+}
+__device__ __forceinline__ double force_d(const RealStageParams& p, double lap, double pv, double dv) {
+    // inv_a2*lap - eta*pi - V'/mu^2
+    return __dsub_rn(__dsub_rn(__dmul_rn(p.inv_a2, lap), __dmul_rn(p.eta, pv)), __dmul_rn(dv, p.inv_mu2));
+}
 __device__ __forceinline__ void update_f64(const RealStageParams& p, const double* s_tab,
                                            const double ph[7], const double pv[7], double noise,
                                            double& phi_new, double& pi_new) {
     const double c = ph[0];
-    double lap = (ph[1] + ph[2] + ph[3] + ph[4] + ph[5] + ph[6] - 6.0 * c) * p.inv_dx2;
+    const double lap = __dmul_rn(__fma_rn(-6.0, c, sum6_d(ph)), p.inv_dx2);
     double pt[7];
 #pragma unroll
-    for (int q = 0; q < 7; ++q) pt[q] = ph[q] + p.h1 * pv[q];
-    double lap2 = (pt[1] + pt[2] + pt[3] + pt[4] + pt[5] + pt[6] - 6.0 * pt[0]) * p.inv_dx2;
-    double k1 = p.inv_a2 * lap - p.eta * pv[0] - vprime_d(p, s_tab, c) * p.inv_mu2;
-    double pit = pv[0] + p.h1 * k1;
-    double k2 = p.inv_a2 * lap2 - p.eta * pit - vprime_d(p, s_tab, pt[0]) * p.inv_mu2;
-    phi_new = c + p.h2 * pit;
-    pi_new = pv[0] + (p.h2 * k2 + noise);
+    for (int q = 0; q < 7; ++q) pt[q] = __fma_rn(p.h1, pv[q], ph[q]);
+    const double lap2 = __dmul_rn(__fma_rn(-6.0, pt[0], sum6_d(pt)), p.inv_dx2);
+    const double k1 = force_d(p, lap, pv[0], vprime_d(p, s_tab, c));
+    const double pit = __fma_rn(p.h1, k1, pv[0]);
+    const double k2 = force_d(p, lap2, pit, vprime_d(p, s_tab, pt[0]));
+    phi_new = __fma_rn(p.h2, pit, c);
+    pi_new = __dadd_rn(pv[0], __fma_rn(p.h2, k2, noise));
 }
 
 // --------------------------------------------------------------- F32 ----
@@ -136,39 +145,62 @@ __device__ __forceinline__ void update_f32(const RealStageParams& p, const doubl
 }
 
 // -------------------------------------------------------------- F32C ----
-// float2 {hi, lo} storage.  Forces in FP32 from hi/lo differences (the
-// Laplacian of a smooth field is a difference of nearly equal values, so
-// hi - hi is exact and the lo parts carry the rest); the state updates
-// phi + h2*pi~ and pi + h2*k + noise are accumulated in FP64 and split back,
-// so increments far below ulp_fp32(phi) are kept.
+// float2 {hi, lo} storage, FP32 arithmetic only.  Forces from hi/lo
+// differences (the Laplacian of a smooth field is a difference of nearly
+// equal values: hi - hi is exact and the lo parts carry the rest); the state
+// updates phi + h2*pi~ and pi + h2*k + kick are float-float (TwoSum), so
+// increments far below ulp_fp32(phi) are kept.  `kick` is the noise
+// increment (FP32 Box-Muller of the exact hash bits, or an array value).
+// All operations are explicit round-to-nearest intrinsics (bitwise identical
+// results in every kernel that calls this).
+__device__ __forceinline__ float lap_ff(const float2 v[7], float inv_dx2) {
+    float dh = __fsub_rn(v[1].x, v[0].x);
+    float dl = v[1].y;
+#pragma unroll
+    for (int q = 2; q < 7; ++q) {
+        dh = __fadd_rn(dh, __fsub_rn(v[q].x, v[0].x));
+        dl = __fadd_rn(dl, v[q].y);
+    }
+    dl = __fmaf_rn(-6.0f, v[0].y, dl);
+    return __fmul_rn(__fadd_rn(dh, dl), inv_dx2);
+}
+__device__ __forceinline__ float force_f(float inv_a2, float eta, float inv_mu2, float lap, float pv,
+                                         float dv) {
+    return __fsub_rn(__fsub_rn(__fmul_rn(inv_a2, lap), __fmul_rn(eta, pv)), __fmul_rn(dv, inv_mu2));
+}
 __device__ __forceinline__ void update_f32c(const RealStageParams& p, const float* s_tab,
                                             float tminf, float dinvf, const float2 ph[7],
-                                            const float2 pv[7], double noise, float2& phi_new,
+                                            const float2 pv[7], float kick, float2& phi_new,
                                             float2& pi_new) {
     const float h1 = (float)p.h1;
-    float dph = 0.f, dpl = 0.f, dvh = 0.f, dvl = 0.f;
-#pragma unroll
-    for (int q = 1; q < 7; ++q) {
-        dph += ph[q].x - ph[0].x;
-        dpl += ph[q].y - ph[0].y;
-        dvh += pv[q].x - pv[0].x;
-        dvl += pv[q].y - pv[0].y;
-    }
+    const float h2h = (float)p.h2;
+    const float h2l = (float)(p.h2 - (double)h2h);
     const float inv_dx2 = (float)p.inv_dx2;
-    float lap = (dph + dpl) * inv_dx2;
-    float lapv = (dvh + dvl) * inv_dx2;
-    float lap2 = lap + h1 * lapv;  // Laplacian of phi~ = phi + h1 pi
-    float phc = ph[0].x + ph[0].y;
-    float pvc = pv[0].x + pv[0].y;
     const float inv_a2 = (float)p.inv_a2, eta = (float)p.eta, inv_mu2 = (float)p.inv_mu2;
-    float k1 = inv_a2 * lap - eta * pvc - vprime_f(p, s_tab, phc, tminf, dinvf) * inv_mu2;
-    float pit = pvc + h1 * k1;
-    float pht = ph[0].x + (ph[0].y + h1 * pvc);
-    float k2 = inv_a2 * lap2 - eta * pit - vprime_f(p, s_tab, pht, tminf, dinvf) * inv_mu2;
-    double pi_d = join_f32c(pv[0]);
-    double pit_d = pi_d + p.h1 * (double)k1;
-    phi_new = split_f32c(join_f32c(ph[0]) + p.h2 * pit_d);
-    pi_new = split_f32c(pi_d + ((double)(p.h2 * (double)k2) + noise));
+    const float lap = lap_ff(ph, inv_dx2);
+    const float lap2 = __fmaf_rn(h1, lap_ff(pv, inv_dx2), lap);  // Laplacian of phi + h1 pi
+    const float phc = __fadd_rn(ph[0].x, ph[0].y);
+    const float pvc = __fadd_rn(pv[0].x, pv[0].y);
+    const float k1 = force_f(inv_a2, eta, inv_mu2, lap, pvc, vprime_f(p, s_tab, phc, tminf, dinvf));
+    // pi~ = pi + h1 k1 as {t_hi, t_lo}
+    float t_hi, t_e;
+    two_sum(pv[0].x, __fmul_rn(h1, k1), t_hi, t_e);
+    const float t_lo = __fadd_rn(pv[0].y, t_e);
+    const float pit = __fadd_rn(t_hi, t_lo);
+    const float pht = __fadd_rn(ph[0].x, __fmaf_rn(h1, pvc, ph[0].y));
+    const float k2 = force_f(inv_a2, eta, inv_mu2, lap2, pit, vprime_f(p, s_tab, pht, tminf, dinvf));
+    // phi + h2 pi~ with the product's rounding error kept
+    const float d_hi = __fmul_rn(h2h, t_hi);
+    const float d_lo = __fadd_rn(__fmaf_rn(h2h, t_hi, -d_hi), __fmaf_rn(h2h, t_lo, __fmul_rn(h2l, t_hi)));
+    phi_new = ff_add(ph[0], d_hi, d_lo);
+    pi_new = ff_add(pv[0], __fmaf_rn(h2h, k2, kick), 0.0f);
+}
+
+// Noise increment for one F32C site: array value * nfac, or ns * z (FP32 z).
+__device__ __forceinline__ float site_kick_f32c(const RealStageParams& p, uint64_t site) {
+    if (p.noise) return (float)(p.nfac * static_cast<const double*>(p.noise)[site]);
+    if (p.ns_eff == 0.0) return 0.0f;
+    return __fmul_rn((float)p.ns_eff, gauss_cos_f(noise_key(site, p.step, p.mul, p.seed)));
 }
 
 }  // namespace tipt

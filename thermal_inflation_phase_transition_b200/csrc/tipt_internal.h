@@ -28,6 +28,5 @@ int check_state(int storage, const void* phi, const void* pi, void* phi_out, voi
 
 struct RealStageParams;
 int launch_real_stage(int storage, RealStageParams p, cudaStream_t st);
-int launch_real_stage_generic_only(int storage, RealStageParams p, cudaStream_t st);
 
 }  // namespace tipt

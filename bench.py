@@ -275,7 +275,7 @@ def main():
     def make_state():
         if args.storage == "f32c":
             a = RF.to_f32c(phi64)
-            b = torch.zeros(shape + (2,), dtype=torch.float32, device=dev)
+            b = torch.zeros((2,) + shape, dtype=torch.float32, device=dev)
         elif args.storage == "f64":
             a = phi64.clone()
             b = torch.zeros(shape, dtype=torch.float64, device=dev)
@@ -378,7 +378,7 @@ def run_e2e(args, shape, seed, RF, observables, torch, dev, world):
     N = n ** 3
     rng = np.random.default_rng(99)
     if args.storage == "f32c":
-        host_shape = shape + (2,)
+        host_shape = (2,) + shape
         hdt = torch.float32
     else:
         host_shape = shape
@@ -388,7 +388,7 @@ def run_e2e(args, shape, seed, RF, observables, torch, dev, world):
     h_phi.copy_(torch.from_numpy(rng.normal(0, 0.01, host_shape).astype(
         np.float32 if hdt == torch.float32 else np.float64)))
     if args.storage == "f32c":
-        h_phi[..., 1].zero_()
+        h_phi[1].zero_()
     h_obs = torch.empty(10, dtype=torch.float64).pin_memory()
     d_phi = torch.empty(host_shape, dtype=hdt, device=dev)
     d_pi = torch.empty_like(d_phi)

@@ -112,7 +112,7 @@ def test_march_f64_vs_oracle():
 def test_fp32_box_muller_accuracy():
     """F32C kicks: FP32 Box-Muller of the exact hash bits vs the FP64 z."""
     shape = (64, 64, 64)
-    zero = torch.zeros(shape + (2,), dtype=torch.float32, device=DEV)
+    zero = torch.zeros((2,) + shape, dtype=torch.float32, device=DEV)
     phi, pi = zero.clone(), zero.clone()
     po, vo = torch.empty_like(phi), torch.empty_like(pi)
     # V' = 0, dt = 0: pi' = kick = ns * z exactly

@@ -9,19 +9,20 @@ from . import _lib as L
 
 
 def storage_of(t: torch.Tensor) -> int:
-    """float64 (nx,ny,nz) -> F64; float32 (nx,ny,nz) -> F32; float32 (nx,ny,nz,2) -> F32C."""
+    """float64 (nx,ny,nz) -> F64; float32 (nx,ny,nz) -> F32; float32 (2,nx,ny,nz) -> F32C
+    (compensated pair: plane 0 = hi, plane 1 = lo, value hi + lo)."""
     if t.dtype == torch.float64 and t.dim() == 3:
         return L.TIPT_F64
     if t.dtype == torch.float32 and t.dim() == 3:
         return L.TIPT_F32
-    if t.dtype == torch.float32 and t.dim() == 4 and t.shape[-1] == 2:
+    if t.dtype == torch.float32 and t.dim() == 4 and t.shape[0] == 2:
         return L.TIPT_F32C
     raise TypeError(f"unsupported field tensor: dtype={t.dtype}, shape={tuple(t.shape)} "
-                    "(want float64/float32 (nx,ny,nz) or float32 (nx,ny,nz,2) hi/lo pairs)")
+                    "(want float64/float32 (nx,ny,nz) or float32 (2,nx,ny,nz) hi/lo planes)")
 
 
 def dims_of(t: torch.Tensor) -> tuple[int, int, int]:
-    return tuple(int(x) for x in t.shape[:3])
+    return tuple(int(x) for x in (t.shape[1:] if t.dim() == 4 else t.shape))
 
 
 def need_cuda(*ts, names=None):

@@ -45,7 +45,9 @@ int check_storage(int s) {
     return TIPT_OK;
 }
 
+// Bytes per site (F32C: a hi and a lo float) and required pointer alignment.
 int elem_bytes(int s) { return s == TIPT_F32 ? 4 : 8; }
+int elem_align(int s) { return s == TIPT_F64 ? 8 : 4; }
 
 int check_ptr(const void* p, int align, const char* name) {
     if (!p) return fail(TIPT_ERR_ARG, "%s is NULL", name);
@@ -115,9 +117,9 @@ int check_state(int storage, const void* phi, const void* pi, void* phi_out,
                        void* pi_out, int64_t nx, int64_t ny, int64_t nz) {
     int rc;
     if ((rc = check_storage(storage)) || (rc = check_dims(nx, ny, nz))) return rc;
-    const int eb = elem_bytes(storage);
-    if ((rc = check_ptr(phi, eb, "phi")) || (rc = check_ptr(pi, eb, "pi")) ||
-        (rc = check_ptr(phi_out, eb, "phi_out")) || (rc = check_ptr(pi_out, eb, "pi_out")))
+    const int eb = elem_bytes(storage), ea = elem_align(storage);
+    if ((rc = check_ptr(phi, ea, "phi")) || (rc = check_ptr(pi, ea, "pi")) ||
+        (rc = check_ptr(phi_out, ea, "phi_out")) || (rc = check_ptr(pi_out, ea, "pi_out")))
         return rc;
     const int64_t bytes = nx * ny * nz * eb;
     const void* ins[2] = {phi, pi};

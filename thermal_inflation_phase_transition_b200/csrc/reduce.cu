@@ -71,11 +71,15 @@ __device__ __forceinline__ ObsAcc block_reduce(ObsAcc a) {
     return a;
 }
 
+// Site value in FP64; F32C is planar (hi plane, then lo plane N sites later).
 template <int S>
-__device__ __forceinline__ double load_val(const void* p, int64_t s) {
+__device__ __forceinline__ double load_val(const void* p, int64_t s, int64_t N) {
     if constexpr (S == TIPT_F64) return __ldg(static_cast<const double*>(p) + s);
     else if constexpr (S == TIPT_F32) return (double)__ldg(static_cast<const float*>(p) + s);
-    else return join_f32c(__ldg(static_cast<const float2*>(p) + s));
+    else {
+        const float* f = static_cast<const float*>(p);
+        return (double)__ldg(f + s) + (double)__ldg(f + N + s);
+    }
 }
 
 struct ObsParams {
@@ -101,12 +105,12 @@ __global__ void __launch_bounds__(kRedThreads) obs_partial_kernel(ObsParams p) {
         const int64_t r = s / p.n2;
         const int j = (int)(r % p.n1);
         const int i = (int)(r / p.n1);
-        const double ph = load_val<S>(p.phi, s);
-        const double pv = p.pi ? load_val<S>(p.pi, s) : 0.0;
+        const double ph = load_val<S>(p.phi, s, N);
+        const double pv = p.pi ? load_val<S>(p.pi, s, N) : 0.0;
         // forward differences, R:2303-2308
-        const double fx = load_val<S>(p.phi, s + ((i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12)) - ph;
-        const double fy = load_val<S>(p.phi, s + ((j + 1 < p.n1) ? (int64_t)p.n2 : -(int64_t)(p.n1 - 1) * p.n2)) - ph;
-        const double fz = load_val<S>(p.phi, s + ((k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1))) - ph;
+        const double fx = load_val<S>(p.phi, s + ((i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12), N) - ph;
+        const double fy = load_val<S>(p.phi, s + ((j + 1 < p.n1) ? (int64_t)p.n2 : -(int64_t)(p.n1 - 1) * p.n2), N) - ph;
+        const double fz = load_val<S>(p.phi, s + ((k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1)), N) - ph;
         a.kin += 0.5 * pv * pv;
         a.grad += 0.5 * p.inv_a2 * (fx * fx + fy * fy + fz * fz) * p.inv_dx2;
         const double ph2 = ph * ph;
@@ -224,7 +228,7 @@ extern "C" int tipt_observables(int storage, const void* phi, const void* pi, in
                                 void* workspace, int64_t workspace_bytes, void* stream) {
     int rc;
     if ((rc = check_storage(storage)) || (rc = check_dims(nx, ny, nz))) return rc;
-    const int eb = elem_bytes(storage);
+    const int eb = elem_align(storage);
     if ((rc = check_ptr(phi, eb, "phi")) || (rc = check_ptr(out, 8, "out")) ||
         (rc = check_ptr(workspace, 8, "workspace")))
         return rc;

@@ -98,8 +98,8 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
             s + ((j > 0) ? -(int64_t)p.n2 : (int64_t)(p.n1 - 1) * p.n2),
             s + ((k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1)),
             s + ((k > 0) ? -1 : (int64_t)(p.n2 - 1))};
-        double n1, n2;
         if constexpr (S == TIPT_F64) {
+            double n1, n2;
             double a[4][7];
 #pragma unroll
             for (int f = 0; f < 4; ++f)
@@ -127,6 +127,7 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
             static_cast<double*>(p.o[2])[s] = a[2][0] + (p.h2 * k2a + n1);
             static_cast<double*>(p.o[3])[s] = a[3][0] + (p.h2 * k2b + n2);
         } else if constexpr (S == TIPT_F32) {
+            double n1, n2;
             // float32 storage, FP64 arithmetic after the float32 neighbour sums,
             // float32-rounded midpoint state (as the reference's float32 mode)
             float a[4][7];
@@ -161,58 +162,87 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
             static_cast<float*>(p.o[2])[s] = __double2float_rn((double)a[2][0] + (p.h2 * k2a + n1));
             static_cast<float*>(p.o[3])[s] = __double2float_rn((double)a[3][0] + (p.h2 * k2b + n2));
         } else {
-            float2 a[4][7];
+            // planar {hi, lo} fields; FP32 forces, float-float state updates
+            float hi[4][7], lo[4][7];
 #pragma unroll
             for (int f = 0; f < 4; ++f)
 #pragma unroll
-                for (int q = 0; q < 7; ++q) a[f][q] = __ldg(static_cast<const float2*>(p.f[f]) + idx[q]);
+                for (int q = 0; q < 7; ++q) {
+                    const float* src = static_cast<const float*>(p.f[f]);
+                    hi[f][q] = __ldg(src + idx[q]);
+                    lo[f][q] = __ldg(src + N + idx[q]);
+                }
             const float h1 = (float)p.h1, inv_dx2 = (float)p.inv_dx2;
-            float lap[4];
+            const float h2h = (float)p.h2, h2l = (float)(p.h2 - (double)h2h);
+            const float inv_a2 = (float)p.inv_a2, eta = (float)p.eta, inv_mu2 = (float)p.inv_mu2;
+            float lap[4], c[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                float dh = 0.f, dl = 0.f;
-#pragma unroll
-                for (int q = 1; q < 7; ++q) {
-                    dh += a[f][q].x - a[f][0].x;
-                    dl += a[f][q].y - a[f][0].y;
-                }
-                lap[f] = (dh + dl) * inv_dx2;
+                float dh, dl;
+                stencil_sums(hi[f], lo[f], dh, dl);
+                lap[f] = __fmul_rn(__fadd_rn(dh, dl), inv_dx2);
+                c[f] = __fadd_rn(hi[f][0], lo[f][0]);
             }
-            float c[4];
-#pragma unroll
-            for (int f = 0; f < 4; ++f) c[f] = a[f][0].x + a[f][0].y;
             const float* ftab = reinterpret_cast<const float*>(s_tab);
-            const float inv_a2 = (float)p.inv_a2, eta = (float)p.eta, inv_mu2 = (float)p.inv_mu2;
+            // The Z_N force of the reference form (C:2152-2158) grows like 1/rho
+            // near the origin and amplifies FP32 rounding, so with Z_N active the
+            // force is evaluated in FP64 from the full hi + lo values (q1d, q2d).
+            const bool zn = p.zn_active > 0.5 && p.zn_n > 0.5;
+            auto cforce = [&](float q1, float q2, double q1d, double q2d, float& d1, float& d2) {
+                if (!zn && (p.table_in_smem || p.vkind == TIPT_VP_POLY)) {
+                    complex_force<float>(p, ftab, (float)p.tmin, (float)p.dinv, q1, q2, d1, d2);
+                } else {
+                    double e1, e2;
+                    complex_force<double>(p, p.table, p.tmin, p.dinv, q1d, q2d, e1, e2);
+                    d1 = (float)e1;
+                    d2 = (float)e2;
+                }
+            };
             float d1, d2;
-            if (p.table_in_smem || p.vkind == TIPT_VP_POLY) {
-                complex_force<float>(p, ftab, (float)p.tmin, (float)p.dinv, c[0], c[1], d1, d2);
-            } else {
-                double e1, e2;
-                complex_force<double>(p, p.table, p.tmin, p.dinv, c[0], c[1], e1, e2);
-                d1 = (float)e1;
-                d2 = (float)e2;
+            cforce(c[0], c[1], (double)hi[0][0] + (double)lo[0][0],
+                   (double)hi[1][0] + (double)lo[1][0], d1, d2);
+            const float k1[2] = {force_v<float>(inv_a2, eta, inv_mu2, lap[0], c[2], d1),
+                                 force_v<float>(inv_a2, eta, inv_mu2, lap[1], c[3], d2)};
+            float t_hi[2], t_lo[2], pit[2], q[2];
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                float e;
+                two_sum(hi[2 + a][0], __fmul_rn(h1, k1[a]), t_hi[a], e);
+                t_lo[a] = __fadd_rn(lo[2 + a][0], e);
+                pit[a] = __fadd_rn(t_hi[a], t_lo[a]);
+                q[a] = __fadd_rn(hi[a][0], __fmaf_rn(h1, c[2 + a], lo[a][0]));
             }
-            float k1a = inv_a2 * lap[0] - eta * c[2] - d1 * inv_mu2;
-            float k1b = inv_a2 * lap[1] - eta * c[3] - d2 * inv_mu2;
-            float pta = c[2] + h1 * k1a, ptb = c[3] + h1 * k1b;
-            float q1 = a[0][0].x + (a[0][0].y + h1 * c[2]);
-            float q2 = a[1][0].x + (a[1][0].y + h1 * c[3]);
-            if (p.table_in_smem || p.vkind == TIPT_VP_POLY) {
-                complex_force<float>(p, ftab, (float)p.tmin, (float)p.dinv, q1, q2, d1, d2);
-            } else {
-                double e1, e2;
-                complex_force<double>(p, p.table, p.tmin, p.dinv, q1, q2, e1, e2);
-                d1 = (float)e1;
-                d2 = (float)e2;
+            cforce(q[0], q[1],
+                   (double)hi[0][0] + ((double)lo[0][0] + (double)h1 * ((double)hi[2][0] + (double)lo[2][0])),
+                   (double)hi[1][0] + ((double)lo[1][0] + (double)h1 * ((double)hi[3][0] + (double)lo[3][0])),
+                   d1, d2);
+            const float k2[2] = {force_v<float>(inv_a2, eta, inv_mu2, __fmaf_rn(h1, lap[2], lap[0]), pit[0], d1),
+                                 force_v<float>(inv_a2, eta, inv_mu2, __fmaf_rn(h1, lap[3], lap[1]), pit[1], d2)};
+            float kick[2] = {0.0f, 0.0f};
+            if (p.noise1) {
+                kick[0] = (float)(p.nfac * static_cast<const double*>(p.noise1)[s]);
+                kick[1] = (float)(p.nfac * static_cast<const double*>(p.noise2)[s]);
+            } else if (p.ns_eff != 0.0) {
+                float z1, z2;
+                gauss_pair_f(noise_key((uint64_t)s, p.step, p.mul, p.seed), z1, z2);
+                kick[0] = __fmul_rn((float)p.ns_eff, z1);
+                kick[1] = __fmul_rn((float)p.ns_eff, z2);
             }
-            float k2a = inv_a2 * (lap[0] + h1 * lap[2]) - eta * pta - d1 * inv_mu2;
-            float k2b = inv_a2 * (lap[1] + h1 * lap[3]) - eta * ptb - d2 * inv_mu2;
-            complex_noise<double>(p, (uint64_t)s, n1, n2);
-            const double pia = join_f32c(a[2][0]), pib = join_f32c(a[3][0]);
-            static_cast<float2*>(p.o[0])[s] = split_f32c(join_f32c(a[0][0]) + p.h2 * (pia + p.h1 * (double)k1a));
-            static_cast<float2*>(p.o[1])[s] = split_f32c(join_f32c(a[1][0]) + p.h2 * (pib + p.h1 * (double)k1b));
-            static_cast<float2*>(p.o[2])[s] = split_f32c(pia + ((double)(p.h2 * (double)k2a) + n1));
-            static_cast<float2*>(p.o[3])[s] = split_f32c(pib + ((double)(p.h2 * (double)k2b) + n2));
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const float d_hi = __fmul_rn(h2h, t_hi[a]);
+                const float d_lo = __fadd_rn(__fmaf_rn(h2h, t_hi[a], -d_hi),
+                                             __fmaf_rn(h2h, t_lo[a], __fmul_rn(h2l, t_hi[a])));
+                float nh, nl;
+                ff_add(hi[a][0], lo[a][0], d_hi, d_lo, nh, nl);
+                float* po = static_cast<float*>(p.o[a]);
+                po[s] = nh;
+                po[N + s] = nl;
+                ff_add(hi[2 + a][0], lo[2 + a][0], __fmaf_rn(h2h, k2[a], kick[a]), 0.0f, nh, nl);
+                float* vo = static_cast<float*>(p.o[2 + a]);
+                vo[s] = nh;
+                vo[N + s] = nl;
+            }
         }
     }
 }

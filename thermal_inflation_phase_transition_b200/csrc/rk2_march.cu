@@ -96,11 +96,6 @@ struct MarchGeom {
 template <int S>
 struct MarchElem;
 template <>
-struct MarchElem<TIPT_F32C> {
-    using E = float2;
-    using TT = float;
-};
-template <>
 struct MarchElem<TIPT_F64> {
     using E = double;
     using TT = double;
@@ -129,17 +124,11 @@ __device__ __forceinline__ void ld_pair_g(const E* p, E& a, E& b) {
 
 template <int S>
 __device__ __forceinline__ void site_update(const RealStageParams& p, const void* s_tab,
-                                            float tminf, float dinvf,
-                                            const typename MarchElem<S>::E ph[7],
+                                            float, float, const typename MarchElem<S>::E ph[7],
                                             const typename MarchElem<S>::E pv[7], uint64_t site,
                                             typename MarchElem<S>::E& a,
                                             typename MarchElem<S>::E& b) {
-    if constexpr (S == TIPT_F32C)
-        update_f32c(p, static_cast<const float*>(s_tab), tminf, dinvf, ph, pv,
-                    site_kick_f32c(p, site), a, b);
-    else
-        update_f64(p, static_cast<const double*>(s_tab), ph, pv, site_noise<double>(p, site), a,
-                   b);
+    update_f64(p, static_cast<const double*>(s_tab), ph, pv, site_noise<double>(p, site), a, b);
 }
 
 // Launch bounds of the two block-size classes: up to 256 consumer threads
@@ -328,6 +317,199 @@ __global__ void __maxnreg__(kMarchRegs)
     }
 }
 
+// Planar compensated-FP32 marching kernel.  Same ring, roles and work items as
+// rk2_stage_march; a field is two FP32 planes (hi, then lo N sites later), so
+// the TMA map spans 2*n0 planes and a ring stage holds [phi, pi][hi, lo]
+// tiles.  A consumer thread owns four consecutive sites of its row (one
+// 16-byte vector per plane and neighbour) and evaluates them as two site
+// pairs in the lanes of the packed FP32x2 instructions; the stencil sums run
+// in the order of the generic kernel, so results are bitwise identical.
+template <bool WIDE>
+__global__ void __maxnreg__(kMarchRegs)
+    rk2_stage_march_f32c(const __grid_constant__ CUtensorMap tm_phi,
+                         const __grid_constant__ CUtensorMap tm_pi, RealStageParams p,
+                         MarchGeom g) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    float* s_tab = reinterpret_cast<float*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + g.tab_bytes);
+    uint64_t* empty = full + 8;
+    unsigned char* ring = smem + g.tab_bytes + 128;
+
+    const int n0 = p.n0, n1 = p.n1, n2 = p.n2;
+    const int pitch = g.pitch;
+    const int TJ = g.TJ;
+    const uint32_t NS = (uint32_t)g.S;
+    const int rows = TJ + 2;
+    const int tpr = n2 >> 2;
+    const int nc = TJ * tpr;
+    const int t = threadIdx.x;
+
+    if (t == 0) {
+        for (uint32_t s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], nc / 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (p.table_in_smem) stage_table<float>(p, s_tab);  // ends with __syncthreads
+    else __syncthreads();
+
+    const size_t plane_blk = (size_t)(g.stage_bytes >> 2);  // one [rows][pitch] block
+    // stage -> field f (0 phi, 1 pi) -> component c (0 hi, 1 lo)
+    auto blk = [&](uint32_t stage, int f, int c) -> float* {
+        return reinterpret_cast<float*>(ring + (size_t)stage * g.stage_bytes +
+                                        (size_t)(2 * f + c) * plane_blk);
+    };
+
+    // ------------------------------------------------------------ producer
+    if (t >= nc) {
+        if (t != nc) return;
+        const uint32_t plane_tx = (uint32_t)(4 * rows * n2 * 4);
+        RingPos w{0, 0};
+        uint32_t issued = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
+            const int ic = item / g.nJB;
+            const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+            const int npl = min(g.CI, n0 - i0) + 2;
+            for (int q = 0; q < npl; ++q) {
+                if (issued >= NS && !mbar_wait(&empty[w.stage], w.phase ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(&full[w.stage], plane_tx);
+                int iw = i0 - 1 + q;
+                iw = iw < 0 ? iw + n0 : (iw >= n0 ? iw - n0 : iw);
+                for (int rr = 0; rr < rows; ++rr) {
+                    int jr = j0 - 1 + rr;
+                    jr = jr < 0 ? jr + n1 : (jr >= n1 ? jr - n1 : jr);
+                    for (int kb = 0; kb < n2; kb += g.BK) {
+                        const int o = rr * pitch + kb;
+                        // plane iw = hi, plane n0 + iw = lo
+                        tma_row(blk(w.stage, 0, 0) + o, &tm_phi, kb, jr, iw, &full[w.stage]);
+                        tma_row(blk(w.stage, 0, 1) + o, &tm_phi, kb, jr, n0 + iw, &full[w.stage]);
+                        tma_row(blk(w.stage, 1, 0) + o, &tm_pi, kb, jr, iw, &full[w.stage]);
+                        tma_row(blk(w.stage, 1, 1) + o, &tm_pi, kb, jr, n0 + iw, &full[w.stage]);
+                    }
+                }
+                ++issued;
+                w.next(NS);
+            }
+        }
+        if (!ok) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+        RingPos d = w;
+        for (uint32_t k = 0; k < NS && k < issued; ++k) {
+            d.stage = d.stage == 0 ? NS - 1 : d.stage - 1;
+            if (d.stage == NS - 1) d.phase ^= 1u;
+            (void)mbar_wait(&full[d.stage], d.phase);
+        }
+        return;
+    }
+
+    // ----------------------------------------------------------- consumers
+    const int lane = t & 31;
+    const int r = 1 + t / tpr;                 // own tile row (1..TJ)
+    const int k0 = 4 * (t - (r - 1) * tpr);    // first of the four own columns
+    const int kml = k0 == 0 ? n2 - 1 : k0 - 1;
+    const int kpr = k0 + 4 == n2 ? 0 : k0 + 4;
+    const float tminf = (float)p.tmin, dinvf = (float)p.dinv;
+    float* const phi_out = static_cast<float*>(p.phi_out);
+    float* const pi_out = static_cast<float*>(p.pi_out);
+    const int64_t N = (int64_t)n0 * n1 * n2;
+    const int orow = r * pitch, urow = (r - 1) * pitch, drow = (r + 1) * pitch;
+
+    RingPos pm{0, 0};
+    for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
+        const int ic = item / g.nJB;
+        const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+        const int ni = min(g.CI, n0 - i0);
+        const int jw = j0 + r - 1;
+        RingPos pc = pm, pp;
+        pc.next(NS);
+        pp = pc;
+        pp.next(NS);
+        if (!mbar_wait(&full[pm.stage], pm.phase) || !mbar_wait(&full[pc.stage], pc.phase)) {
+            if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+            return;
+        }
+        for (int q = 0; q < ni; ++q) {
+            if (!mbar_wait(&full[pp.stage], pp.phase)) {
+                if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+                return;
+            }
+            const int i = i0 + q;
+            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2 + k0;
+            F32CIn<float2> in[2];
+#pragma unroll
+            for (int f = 0; f < 2; ++f) {
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const float* sc = blk(pc.stage, f, c);
+                    const float4 ce = *reinterpret_cast<const float4*>(sc + orow + k0);
+                    const float4 jm = *reinterpret_cast<const float4*>(sc + urow + k0);
+                    const float4 jp = *reinterpret_cast<const float4*>(sc + drow + k0);
+                    const float4 im = *reinterpret_cast<const float4*>(blk(pm.stage, f, c) + orow + k0);
+                    const float4 ip = *reinterpret_cast<const float4*>(blk(pp.stage, f, c) + orow + k0);
+                    const float kl = sc[orow + kml], kr = sc[orow + kpr];
+                    // site pairs (0,1) and (2,3): centre and the six neighbours
+                    const float2 cc[2] = {make_float2(ce.x, ce.y), make_float2(ce.z, ce.w)};
+                    const float2 nb[2][6] = {
+                        {make_float2(ip.x, ip.y), make_float2(im.x, im.y), make_float2(jp.x, jp.y),
+                         make_float2(jm.x, jm.y), make_float2(ce.y, ce.z), make_float2(kl, ce.x)},
+                        {make_float2(ip.z, ip.w), make_float2(im.z, im.w), make_float2(jp.z, jp.w),
+                         make_float2(jm.z, jm.w), make_float2(ce.w, kr), make_float2(ce.y, ce.z)}};
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        float2 acc;
+                        if (c == 0) {  // dh = sum (hi_n - hi_c)
+                            acc = v_sub(nb[h][0], cc[h]);
+#pragma unroll
+                            for (int n = 1; n < 6; ++n) acc = v_add(acc, v_sub(nb[h][n], cc[h]));
+                        } else {       // dl = fma(-6, lo_c, sum lo_n)
+                            acc = nb[h][0];
+#pragma unroll
+                            for (int n = 1; n < 6; ++n) acc = v_add(acc, nb[h][n]);
+                            acc = v_fma(vs<float2>(-6.0f), cc[h], acc);
+                        }
+                        if (f == 0) {
+                            if (c == 0) { in[h].dh_phi = acc; in[h].phh = cc[h]; }
+                            else { in[h].dl_phi = acc; in[h].phl = cc[h]; }
+                        } else {
+                            if (c == 0) { in[h].dh_pi = acc; in[h].pih = cc[h]; }
+                            else { in[h].dl_pi = acc; in[h].pil = cc[h]; }
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[pm.stage]);  // plane i-1 is no longer read
+            float2 o[2][4];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint64_t site;
+                if constexpr (WIDE) site = (uint64_t)(rowoff + 2 * h);
+                else site = (uint32_t)rowoff + (uint32_t)(2 * h);
+                update_f32c<float2>(p, s_tab, tminf, dinvf, in[h], site_kick_f32c2(p, site),
+                                    o[h][0], o[h][1], o[h][2], o[h][3]);
+            }
+            *reinterpret_cast<float4*>(phi_out + rowoff) = make_float4(o[0][0].x, o[0][0].y, o[1][0].x, o[1][0].y);
+            *reinterpret_cast<float4*>(phi_out + N + rowoff) = make_float4(o[0][1].x, o[0][1].y, o[1][1].x, o[1][1].y);
+            *reinterpret_cast<float4*>(pi_out + rowoff) = make_float4(o[0][2].x, o[0][2].y, o[1][2].x, o[1][2].y);
+            *reinterpret_cast<float4*>(pi_out + N + rowoff) = make_float4(o[0][3].x, o[0][3].y, o[1][3].x, o[1][3].y);
+            pm = pc;
+            pc = pp;
+            pp.next(NS);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(&empty[pm.stage]);
+            mbar_arrive(&empty[pc.stage]);
+        }
+        pm = pp;
+    }
+}
+
 // ------------------------------------------------------------------ host ---
 using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                               const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -349,28 +531,33 @@ static EncodeFn encode_fn() {
     return fn;
 }
 
-static bool make_map(CUtensorMap* tm, const void* base, int n0, int n1, int n2, int BK) {
+// 3-D map of one field: (n2, n1, planes) with elements of `es` bytes (FP64
+// fields: planes = n0; planar FP32 pairs: planes = 2*n0, hi then lo).
+static bool make_map(CUtensorMap* tm, const void* base, int planes, int n1, int n2, int es,
+                     int BK) {
     EncodeFn enc = encode_fn();
     if (!enc) return false;
-    const cuuint64_t dims[3] = {(cuuint64_t)n2, (cuuint64_t)n1, (cuuint64_t)n0};
-    const cuuint64_t strides[2] = {(cuuint64_t)n2 * 8, (cuuint64_t)n2 * 8 * n1};
+    const cuuint64_t dims[3] = {(cuuint64_t)n2, (cuuint64_t)n1, (cuuint64_t)planes};
+    const cuuint64_t strides[2] = {(cuuint64_t)n2 * es, (cuuint64_t)n2 * es * n1};
     const cuuint32_t box[3] = {(cuuint32_t)BK, 1, 1};
-    const cuuint32_t es[3] = {1, 1, 1};
-    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides, box,
-               es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
-           CUDA_SUCCESS;
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(tm, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+               const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // Tile shape; 0 = choose automatically.  Set by tipt_set_march_tiles().
 static int g_force_tj = 0, g_force_ci = 0, g_force_stages = 0;
 
-// TMA box width.  A tensor copy's shared-memory destination must be 128-byte
-// aligned: rows sit at multiples of the (128-byte) pitch, and a row split into
-// several boxes needs box widths of a multiple of 16 elements (128 bytes).
-static int pick_bk(int n2) {
+// TMA box width (elements of `es` bytes).  A tensor copy's shared-memory
+// destination must be 128-byte aligned: rows sit at multiples of the
+// 128-byte pitch, and a row split into several boxes needs box widths of a
+// multiple of 128 bytes.
+static int pick_bk(int n2, int es) {
     if (n2 <= 256) return n2;
-    for (int bk = 256; bk >= 16; bk -= 16)
+    const int step = 128 / es;
+    for (int bk = 256; bk >= step; bk -= step)
         if (n2 % bk == 0) return bk;
     return 0;
 }
@@ -395,12 +582,20 @@ static int ctas_per_sm(const MarchGeom& g, int tpr) {
     return by_smem < by_warps ? by_smem : by_warps;
 }
 
-static bool geometry(const RealStageParams& p, int64_t smem_table, MarchGeom& g, int64_t& smem) {
+// Shared-memory ring layout of a storage: FP64 -> one 8-byte plane per field;
+// F32C -> two 4-byte planes (hi, lo) per field.
+static int layout_es(int storage) { return storage == TIPT_F64 ? 8 : 4; }
+static int layout_planes(int storage) { return storage == TIPT_F64 ? 1 : 2; }
+
+static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, MarchGeom& g,
+                     int64_t& smem) {
     const int n1 = p.n1, n2 = p.n2;
+    const int es = layout_es(storage), np = layout_planes(storage);
     if (n2 % 4 != 0 || n2 < 8 || n2 > 2048) return false;
-    g.BK = pick_bk(n2);
+    g.BK = pick_bk(n2, es);
     if (!g.BK) return false;
-    g.pitch = (n2 + 15) & ~15;
+    const int per128 = 128 / es;
+    g.pitch = (n2 + per128 - 1) / per128 * per128;
     const int tpr = n2 / 4;
     g.tab_bytes = round128((int)smem_table);
     g.CI = g_force_ci > 0 ? g_force_ci : 64;
@@ -418,7 +613,7 @@ static bool geometry(const RealStageParams& p, int64_t smem_table, MarchGeom& g,
             MarchGeom c = g;
             c.TJ = tj;
             c.S = st;
-            c.stage_bytes = 2 * round128((tj + 2) * c.pitch * 8);
+            c.stage_bytes = 2 * np * round128((tj + 2) * c.pitch * es);
             if (smem_need(c) > kSmemPerCta) continue;
             const int cps = ctas_per_sm(c, tpr);
             if (cps < 1) continue;
@@ -433,8 +628,8 @@ static bool geometry(const RealStageParams& p, int64_t smem_table, MarchGeom& g,
     g = pick;
     // every TMA destination (ring + stage*stage_bytes + f*stage_bytes/2 +
     // (rr*pitch + kb)*8) must be 128-byte aligned
-    if ((g.pitch * 8) % 128 || (g.BK * 8) % 128 && g.BK != n2 || g.stage_bytes % 256 ||
-        g.tab_bytes % 128)
+    if ((g.pitch * es) % 128 || ((g.BK * es) % 128 && g.BK != n2) || (g.BK * es) % 16 ||
+        g.stage_bytes % (256 * np) || g.tab_bytes % 128)
         return false;
     g.nJB = n1 / g.TJ;
     g.nIC = (p.n0 + g.CI - 1) / g.CI;
@@ -453,48 +648,49 @@ bool march_supported(int storage, const RealStageParams& p) {
     MarchGeom g;
     int64_t smem;
     int64_t tb = p.table_in_smem ? (int64_t)p.npts * (storage == TIPT_F32C ? 4 : 8) : 0;
-    return geometry(p, tb, g, smem);
+    return geometry(storage, p, tb, g, smem);
 }
 
-template <int S, bool WIDE>
-static int launch_march_t(const RealStageParams& p, const MarchGeom& g, int64_t smem,
+template <typename Kern>
+static int launch_march_k(Kern kern, const CUtensorMap& tphi, const CUtensorMap& tpi,
+                          const RealStageParams& p, const MarchGeom& g, int64_t smem,
                           cudaStream_t st) {
-    CUtensorMap tphi, tpi;
-    if (!make_map(&tphi, p.phi, p.n0, p.n1, p.n2, g.BK) ||
-        !make_map(&tpi, p.pi, p.n0, p.n1, p.n2, g.BK))
-        return fail(TIPT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    auto kern = rk2_stage_march<S, WIDE>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return fail_cuda(e, "rk2_stage_march attributes");
+    if (e != cudaSuccess) return fail_cuda(e, "marching kernel attributes");
     const int threads = g.TJ * (p.n2 / 4) + 32;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, (size_t)smem);
     if (e != cudaSuccess || per_sm < 1)
-        return fail(TIPT_ERR_UNSUPPORTED, "rk2_stage_march does not fit an SM (%d threads, %lld "
+        return fail(TIPT_ERR_UNSUPPORTED, "marching kernel does not fit an SM (%d threads, %lld "
                     "bytes of shared memory)", threads, (long long)smem);
     int grid = num_sms() * per_sm;
     if (grid > g.items) grid = g.items;
     kern<<<grid, threads, (size_t)smem, st>>>(tphi, tpi, p, g);
     e = cudaGetLastError();
-    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "rk2_stage_march launch");
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "marching kernel launch");
 }
 
 int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cudaStream_t st) {
     MarchGeom g;
     int64_t smem;
-    if (!geometry(p, smem_table, g, smem))
+    if (!geometry(storage, p, smem_table, g, smem))
         return fail(TIPT_ERR_UNSUPPORTED, "marching kernel geometry");
     const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
+    const int es = layout_es(storage), planes = layout_planes(storage) * p.n0;
+    CUtensorMap tphi, tpi;
+    if (!make_map(&tphi, p.phi, planes, p.n1, p.n2, es, g.BK) ||
+        !make_map(&tpi, p.pi, planes, p.n1, p.n2, es, g.BK))
+        return fail(TIPT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     if (storage == TIPT_F32C)
-        return wide ? launch_march_t<TIPT_F32C, true>(p, g, smem, st)
-                    : launch_march_t<TIPT_F32C, false>(p, g, smem, st);
+        return wide ? launch_march_k(rk2_stage_march_f32c<true>, tphi, tpi, p, g, smem, st)
+                    : launch_march_k(rk2_stage_march_f32c<false>, tphi, tpi, p, g, smem, st);
     if (storage == TIPT_F64)
-        return wide ? launch_march_t<TIPT_F64, true>(p, g, smem, st)
-                    : launch_march_t<TIPT_F64, false>(p, g, smem, st);
+        return wide ? launch_march_k(rk2_stage_march<TIPT_F64, true>, tphi, tpi, p, g, smem, st)
+                    : launch_march_k(rk2_stage_march<TIPT_F64, false>, tphi, tpi, p, g, smem, st);
     return fail(TIPT_ERR_STORAGE, "marching kernel takes F32C or F64");
 }
 

@@ -62,19 +62,33 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p) {
             static_cast<float*>(p.phi_out)[s] = a;
             static_cast<float*>(p.pi_out)[s] = b;
         } else {
-            const float2* phi = static_cast<const float2*>(p.phi);
-            const float2* pi = static_cast<const float2*>(p.pi);
-            float2 ph[7], pv[7];
+            // planar {hi, lo}: hi plane at [0, N), lo plane at [N, 2N)
+            const float* phi = static_cast<const float*>(p.phi);
+            const float* pi = static_cast<const float*>(p.pi);
+            float hh[7], hl[7], vh[7], vl[7];
 #pragma unroll
             for (int q = 0; q < 7; ++q) {
-                ph[q] = __ldg(phi + idx[q]);
-                pv[q] = __ldg(pi + idx[q]);
+                hh[q] = __ldg(phi + idx[q]);
+                hl[q] = __ldg(phi + N + idx[q]);
+                vh[q] = __ldg(pi + idx[q]);
+                vl[q] = __ldg(pi + N + idx[q]);
             }
-            float2 a, b;
-            update_f32c(p, reinterpret_cast<const float*>(s_tab), tminf, dinvf, ph, pv,
-                        site_kick_f32c(p, (uint64_t)s), a, b);
-            static_cast<float2*>(p.phi_out)[s] = a;
-            static_cast<float2*>(p.pi_out)[s] = b;
+            F32CIn<float> x;
+            stencil_sums(hh, hl, x.dh_phi, x.dl_phi);
+            stencil_sums(vh, vl, x.dh_pi, x.dl_pi);
+            x.phh = hh[0];
+            x.phl = hl[0];
+            x.pih = vh[0];
+            x.pil = vl[0];
+            float a, b, c, d;
+            update_f32c<float>(p, reinterpret_cast<const float*>(s_tab), tminf, dinvf, x,
+                               site_kick_f32c(p, (uint64_t)s), a, b, c, d);
+            float* po = static_cast<float*>(p.phi_out);
+            float* vo = static_cast<float*>(p.pi_out);
+            po[s] = a;
+            po[N + s] = b;
+            vo[s] = c;
+            vo[N + s] = d;
         }
     }
 }

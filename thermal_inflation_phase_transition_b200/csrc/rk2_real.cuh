@@ -77,13 +77,47 @@ __device__ __forceinline__ double vprime_d(const RealStageParams& p, const doubl
     return lerp_table<double>(t, p.tmin, p.dinv, p.npts - 2, x);
 }
 
-// V'(x) in FP32 from a float row staged in shared memory (F32C storage).
-__device__ __forceinline__ float vprime_f(const RealStageParams& p, const float* s_tab, float x,
-                                          float tmin, float dinv) {
-    if (p.vkind == TIPT_VP_POLY)
-        return poly_vprime<float>((float)p.c1, (float)p.c2, (float)p.c3, x);
-    if (p.table_in_smem) return lerp_table<float>(s_tab, tmin, dinv, p.npts - 2, x);
-    return (float)lerp_table<double>(p.table, p.tmin, p.dinv, p.npts - 2, (double)x);
+// V'(x) in FP32 (F32C storage) for a lane vector: the polynomial, the float
+// row staged in shared memory, or (long 1-D tables) the FP64 table in global
+// memory.  Lane by lane the same operations as lerp_table<float>.
+__device__ __forceinline__ float vlane(float v, int) { return v; }
+__device__ __forceinline__ float vlane(float2 v, int l) { return l ? v.y : v.x; }
+__device__ __forceinline__ void vset(float& v, int, float x) { v = x; }
+__device__ __forceinline__ void vset(float2& v, int l, float x) {
+    if (l) v.y = x;
+    else v.x = x;
+}
+
+template <typename V>
+__device__ __forceinline__ V vprime_v(const RealStageParams& p, const float* s_tab, V x, float tmin,
+                                      float dinv) {
+    constexpr int NL = sizeof(V) / sizeof(float);
+    if (p.vkind == TIPT_VP_POLY) {
+        const V d = v_fma(v_mul(v_mul(vs<V>((float)p.c3), x), x), x, v_mul(vs<V>((float)p.c1), x));
+        return p.c2 != 0.0 ? v_fma(v_mul(vs<V>((float)p.c2), x), x, d) : d;
+    }
+    if (!p.table_in_smem) {
+        V r;
+#pragma unroll
+        for (int l = 0; l < NL; ++l)
+            vset(r, l, (float)lerp_table<double>(p.table, p.tmin, p.dinv, p.npts - 2,
+                                                 (double)vlane(x, l)));
+        return r;
+    }
+    const V fidx = v_mul(v_sub(x, vs<V>(tmin)), vs<V>(dinv));
+    const float last = (float)(p.npts - 2);
+    V fi, a, b;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        float c = vlane(fidx, l);
+        c = c > 0.0f ? c : 0.0f;
+        c = c < last ? c : last;
+        const int idx = (int)c;
+        vset(fi, l, (float)idx);
+        vset(a, l, s_tab[idx]);
+        vset(b, l, s_tab[idx + 1]);
+    }
+    return v_fma(v_sub(fidx, fi), v_sub(b, a), a);
 }
 
 // Noise increment for one site (FP64): array value * nfac, or ns_eff * z.
@@ -145,55 +179,70 @@ __device__ __forceinline__ void update_f32(const RealStageParams& p, const doubl
 }
 
 // -------------------------------------------------------------- F32C ----
-// float2 {hi, lo} storage, FP32 arithmetic only.  Forces from hi/lo
-// differences (the Laplacian of a smooth field is a difference of nearly
-// equal values: hi - hi is exact and the lo parts carry the rest); the state
-// updates phi + h2*pi~ and pi + h2*k + kick are float-float (TwoSum), so
-// increments far below ulp_fp32(phi) are kept.  `kick` is the noise
-// increment (FP32 Box-Muller of the exact hash bits, or an array value).
-// All operations are explicit round-to-nearest intrinsics (bitwise identical
-// results in every kernel that calls this).
-__device__ __forceinline__ float lap_ff(const float2 v[7], float inv_dx2) {
-    float dh = __fsub_rn(v[1].x, v[0].x);
-    float dl = v[1].y;
+// Planar {hi, lo} storage (a field is two FP32 planes, value hi + lo), FP32
+// arithmetic only, written for lane vectors (one site, or two sites in the
+// lanes of the packed FP32x2 instructions).  Forces from hi/lo differences
+// (the Laplacian of a smooth field is a difference of nearly equal values:
+// hi - hi is exact and the lo parts carry the rest); the state updates
+// phi + h2*pi~ and pi + h2*k + kick are float-float (TwoSum), so increments far
+// below ulp_fp32(phi) are kept.  `kick` is the noise increment.
+//
+// Stencil inputs, summed by the caller in the order ip, im, jp, jm, kp, km:
+//   dh = sum (hi_n - hi_c),  dl = fma(-6, lo_c, sum lo_n)
+template <typename V>
+struct F32CIn {
+    V dh_phi, dl_phi, dh_pi, dl_pi;  // stencil sums of phi and pi
+    V phh, phl, pih, pil;            // centre values
+};
+
+template <typename V>
+__device__ __forceinline__ V force_v(V inv_a2, V eta, V inv_mu2, V lap, V pv, V dv) {
+    return v_sub(v_sub(v_mul(inv_a2, lap), v_mul(eta, pv)), v_mul(dv, inv_mu2));
+}
+
+template <typename V>
+__device__ __forceinline__ void update_f32c(const RealStageParams& p, const float* s_tab,
+                                            float tminf, float dinvf, const F32CIn<V>& x, V kick,
+                                            V& phh, V& phl, V& pih, V& pil) {
+    const V h1 = vs<V>((float)p.h1);
+    const float h2f = (float)p.h2;
+    const V h2h = vs<V>(h2f);
+    const V h2l = vs<V>((float)(p.h2 - (double)h2f));
+    const V inv_dx2 = vs<V>((float)p.inv_dx2);
+    const V inv_a2 = vs<V>((float)p.inv_a2), eta = vs<V>((float)p.eta),
+            inv_mu2 = vs<V>((float)p.inv_mu2);
+    const V lap = v_mul(v_add(x.dh_phi, x.dl_phi), inv_dx2);
+    const V lapv = v_mul(v_add(x.dh_pi, x.dl_pi), inv_dx2);
+    const V lap2 = v_fma(h1, lapv, lap);  // Laplacian of phi + h1 pi
+    const V phc = v_add(x.phh, x.phl);
+    const V pvc = v_add(x.pih, x.pil);
+    const V k1 = force_v(inv_a2, eta, inv_mu2, lap, pvc, vprime_v<V>(p, s_tab, phc, tminf, dinvf));
+    // pi~ = pi + h1 k1 as {t_hi, t_lo}
+    V t_hi, t_e;
+    two_sum(x.pih, v_mul(h1, k1), t_hi, t_e);
+    const V t_lo = v_add(x.pil, t_e);
+    const V pit = v_add(t_hi, t_lo);
+    const V pht = v_add(x.phh, v_fma(h1, pvc, x.phl));
+    const V k2 = force_v(inv_a2, eta, inv_mu2, lap2, pit, vprime_v<V>(p, s_tab, pht, tminf, dinvf));
+    // phi + h2 pi~ with the product's rounding error kept
+    const V d_hi = v_mul(h2h, t_hi);
+    const V d_lo = v_add(v_fma(h2h, t_hi, v_neg(d_hi)), v_fma(h2h, t_lo, v_mul(h2l, t_hi)));
+    ff_add(x.phh, x.phl, d_hi, d_lo, phh, phl);
+    ff_add(x.pih, x.pil, v_fma(h2h, k2, kick), vs<V>(0.0f), pih, pil);
+}
+
+// Stencil sums of one planar field for one site from the seven values in
+// stencil order (centre, ip, im, jp, jm, kp, km).
+__device__ __forceinline__ void stencil_sums(const float hi[7], const float lo[7], float& dh,
+                                             float& dl) {
+    dh = __fsub_rn(hi[1], hi[0]);
+    dl = lo[1];
 #pragma unroll
     for (int q = 2; q < 7; ++q) {
-        dh = __fadd_rn(dh, __fsub_rn(v[q].x, v[0].x));
-        dl = __fadd_rn(dl, v[q].y);
+        dh = __fadd_rn(dh, __fsub_rn(hi[q], hi[0]));
+        dl = __fadd_rn(dl, lo[q]);
     }
-    dl = __fmaf_rn(-6.0f, v[0].y, dl);
-    return __fmul_rn(__fadd_rn(dh, dl), inv_dx2);
-}
-__device__ __forceinline__ float force_f(float inv_a2, float eta, float inv_mu2, float lap, float pv,
-                                         float dv) {
-    return __fsub_rn(__fsub_rn(__fmul_rn(inv_a2, lap), __fmul_rn(eta, pv)), __fmul_rn(dv, inv_mu2));
-}
-__device__ __forceinline__ void update_f32c(const RealStageParams& p, const float* s_tab,
-                                            float tminf, float dinvf, const float2 ph[7],
-                                            const float2 pv[7], float kick, float2& phi_new,
-                                            float2& pi_new) {
-    const float h1 = (float)p.h1;
-    const float h2h = (float)p.h2;
-    const float h2l = (float)(p.h2 - (double)h2h);
-    const float inv_dx2 = (float)p.inv_dx2;
-    const float inv_a2 = (float)p.inv_a2, eta = (float)p.eta, inv_mu2 = (float)p.inv_mu2;
-    const float lap = lap_ff(ph, inv_dx2);
-    const float lap2 = __fmaf_rn(h1, lap_ff(pv, inv_dx2), lap);  // Laplacian of phi + h1 pi
-    const float phc = __fadd_rn(ph[0].x, ph[0].y);
-    const float pvc = __fadd_rn(pv[0].x, pv[0].y);
-    const float k1 = force_f(inv_a2, eta, inv_mu2, lap, pvc, vprime_f(p, s_tab, phc, tminf, dinvf));
-    // pi~ = pi + h1 k1 as {t_hi, t_lo}
-    float t_hi, t_e;
-    two_sum(pv[0].x, __fmul_rn(h1, k1), t_hi, t_e);
-    const float t_lo = __fadd_rn(pv[0].y, t_e);
-    const float pit = __fadd_rn(t_hi, t_lo);
-    const float pht = __fadd_rn(ph[0].x, __fmaf_rn(h1, pvc, ph[0].y));
-    const float k2 = force_f(inv_a2, eta, inv_mu2, lap2, pit, vprime_f(p, s_tab, pht, tminf, dinvf));
-    // phi + h2 pi~ with the product's rounding error kept
-    const float d_hi = __fmul_rn(h2h, t_hi);
-    const float d_lo = __fadd_rn(__fmaf_rn(h2h, t_hi, -d_hi), __fmaf_rn(h2h, t_lo, __fmul_rn(h2l, t_hi)));
-    phi_new = ff_add(ph[0], d_hi, d_lo);
-    pi_new = ff_add(pv[0], __fmaf_rn(h2h, k2, kick), 0.0f);
+    dl = __fmaf_rn(-6.0f, lo[0], dl);
 }
 
 // Noise increment for one F32C site: array value * nfac, or ns * z (FP32 z).
@@ -201,6 +250,17 @@ __device__ __forceinline__ float site_kick_f32c(const RealStageParams& p, uint64
     if (p.noise) return (float)(p.nfac * static_cast<const double*>(p.noise)[site]);
     if (p.ns_eff == 0.0) return 0.0f;
     return __fmul_rn((float)p.ns_eff, gauss_cos_f(noise_key(site, p.step, p.mul, p.seed)));
+}
+// The same for two consecutive sites (s, s + 1) in the lanes of a float2.
+__device__ __forceinline__ float2 site_kick_f32c2(const RealStageParams& p, uint64_t s) {
+    if (p.noise) {
+        const double* n = static_cast<const double*>(p.noise);
+        return make_float2((float)(p.nfac * n[s]), (float)(p.nfac * n[s + 1]));
+    }
+    if (p.ns_eff == 0.0) return make_float2(0.0f, 0.0f);
+    const float2 z = gauss_cos_f2(noise_key(s, p.step, p.mul, p.seed),
+                                  noise_key(s + 1, p.step, p.mul, p.seed));
+    return v_mul(vs<float2>((float)p.ns_eff), z);
 }
 
 }  // namespace tipt

@@ -57,71 +57,126 @@ __device__ __forceinline__ void gauss_pair(uint64_t key, double& z1, double& z2)
     z2 = r * s;
 }
 
+// ------------------------------------------------ FP32 lane vectors ----
+// The compensated-FP32 arithmetic is written once for a "lane vector" V: a
+// float (one site) or a float2 (two sites in the two lanes of Blackwell's
+// packed FP32x2 instructions).  The packed intrinsics round each component
+// exactly as the scalar ones, so both forms give identical bits.
+__device__ __forceinline__ float v_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float v_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float v_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float v_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float v_splat(float x, float) { return x; }
+
+__device__ __forceinline__ float2 v_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b as fma(b, -1, a): exact product, one rounding -- bitwise a - b
+__device__ __forceinline__ float2 v_sub(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ float2 v_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 v_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 v_splat(float x, float2) { return make_float2(x, x); }
+
+template <typename V>
+__device__ __forceinline__ V vs(float x) { return v_splat(x, V{}); }
+
 // FP32 Box-Muller for the compensated-FP32 storage.  The hash is the same
-// integer computation; only the Gaussian transform runs in FP32, from the exact
-// 53-bit integers m1, m2 (u = m * 2^-53), with argument reductions done exactly
-// in integer arithmetic and short series on the reduced ranges:
-//  * log(u1): u1 = 2^(e-53) (1 + g) with 1 + g in [3/4, 3/2) and g formed by an
-//    exact integer subtraction; log(1 + g) = 2 atanh(s), s = g / (2 + g),
-//    |s| <= 1/5, summed as 2 s (1 + s^2/3 + s^4/5 + ... + s^10/11) (the atanh
-//    series; truncation < 4e-10 relative).  The reference's clamp
-//    u1 >= 1e-12 is m1 <= 9007.
-//  * cos/sin(2 pi u2): 2 u2 = m2 * 2^-52; the nearest quarter turn is taken from
-//    the integer (exact), the remainder x lies in [-pi/4, pi/4] and the Taylor
-//    series of sin (to x^9) and cos (to x^10) are truncated below 3e-9.
+// integer computation; only the Gaussian transform runs in FP32, from the
+// 53-bit integers m1, m2 (u = m * 2^-53) held as 32-bit halves (hi < 2^21):
+//  * log(u1): for u1 >= 1/2 the distance d = 1 - u1 is formed from the halves
+//    (exact to 2^-45 absolute) and log(u1) = log(1 + g) with g = -d; for
+//    u1 < 1/2 the FP32 value of u1 is split into exponent k and mantissa
+//    1 + g in [3/4, 3/2).  log(1 + g) = 2 atanh(s), s = g / (2 + g), summed as
+//    2 s (1 + s^2/3 + ... + s^14/15) (the atanh series; |s| <= 1/3, truncation
+//    below 2e-8).  The reference's clamp u1 >= 1e-12 is m1 <= 9007.
+//  * cos/sin(2 pi u2): 2 u2 = m2 * 2^-52; the nearest quarter turn q is read
+//    from the high half (exact), the remainder x lies in [-pi/4, pi/4] and the
+//    Taylor series of sin (to x^9) and cos (to x^10) are truncated below 3e-9.
 //  * sqrt via rsqrt and one Newton step.
-// z agrees with the FP64 reference value to a few FP32 ulps.
-__device__ __forceinline__ void hash_bits(uint64_t x, uint64_t& m1, uint64_t& m2) {
+// The absolute error of z against the FP64 reference value is a few 1e-7.
+__device__ __forceinline__ void hash_words(uint64_t x, uint32_t& h1, uint32_t& l1, uint32_t& h2,
+                                           uint32_t& l2) {
     x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
     x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
     x = x ^ (x >> 31);
-    m1 = x >> 11;
+    const uint64_t m1 = x >> 11;
     x = (x * 0x2545F4914F6CDD1Dull) ^ 0x9E3779B97F4A7C15ull;
     x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
     x = x ^ (x >> 31);
-    m2 = x >> 11;
+    const uint64_t m2 = x >> 11;
+    h1 = (uint32_t)(m1 >> 32);
+    l1 = (uint32_t)m1;
+    h2 = (uint32_t)(m2 >> 32);
+    l2 = (uint32_t)m2;
 }
 
 constexpr float kLn2Hi = 0.693147182464599609375f;   // ln 2 rounded to FP32
 constexpr float kLn2Lo = -1.904654299957768e-09f;    // ln 2 - kLn2Hi
 constexpr float kLog1em12 = -27.631021115928547f;    // log(1e-12)
 
-__device__ __forceinline__ float log_u1_f(uint64_t m1) {
-    if (m1 <= 9007ull) return kLog1em12;
-    const int e = 63 - __clzll((long long)m1);            // m1 in [2^e, 2^(e+1))
-    const int ep = ((m1 >> (e - 1)) & 1ull) ? e + 1 : e;   // m1 / 2^ep in [3/4, 3/2)
-    const long long gi = (long long)m1 - (1ll << ep);      // exact
-    const float g = __fmul_rn(__ll2float_rn(gi), __int_as_float((127 - ep) << 23));
-    const float s = __fdividef(g, __fadd_rn(2.0f, g));
-    const float w = __fmul_rn(s, s);
-    float poly = __fmaf_rn(w, 1.0f / 11.0f, 1.0f / 9.0f);
-    poly = __fmaf_rn(w, poly, 1.0f / 7.0f);
-    poly = __fmaf_rn(w, poly, 1.0f / 5.0f);
-    poly = __fmaf_rn(w, poly, 1.0f / 3.0f);
-    poly = __fmul_rn(w, poly);                             // s^2/3 + ... + s^10/11
-    const float two_s = __fadd_rn(s, s);
-    const float l1p = __fmaf_rn(two_s, poly, two_s);       // 2 s (1 + poly)
-    const float k = (float)(ep - 53);
-    return __fmaf_rn(k, kLn2Hi, __fmaf_rn(k, kLn2Lo, l1p));
+// Integer half of the log reduction for one lane: g (log1p argument) and k
+// (power of two), plus the clamp flag.
+__device__ __forceinline__ void log_u1_reduce(uint32_t h, uint32_t l, float& g, float& k,
+                                              bool& clamp) {
+    clamp = (h == 0u) && (l <= 9007u);
+    if (h >= (1u << 20)) {
+        // u1 >= 1/2: g = -(1 - u1) = -((2^21 - h) 2^-21 - l 2^-53)
+        g = __fmaf_rn(-(float)((1u << 21) - h), 0x1p-21f, __fmul_rn((float)l, 0x1p-53f));
+        k = 0.0f;
+    } else {
+        const float u = __fmaf_rn((float)h, 0x1p-21f, __fmul_rn((float)l, 0x1p-53f));
+        const uint32_t b = __float_as_uint(u);
+        // mantissa in [3/4, 3/2): shift the exponent when the mantissa is >= 3/2
+        const uint32_t up = (b & 0x00400000u) ? 1u : 0u;
+        const int e = (int)((b >> 23) & 0xffu) - 127 + (int)up;
+        g = __fsub_rn(__uint_as_float((b & 0x007fffffu) | ((127u - up) << 23)), 1.0f);
+        k = (float)e;
+    }
 }
 
-__device__ __forceinline__ void cossin_2pi_f(uint64_t m2, float& c, float& s) {
-    // 2 u2 = m2 * 2^-52 = q/2 + r * 2^-52: q quarter turns (the multiple of
-    // 2^51 nearest m2) plus a remainder |r| <= 2^50, i.e. |x| <= pi/4
-    const uint32_t q = (uint32_t)((m2 + (1ull << 50)) >> 51);        // 0..4
-    const long long r = (long long)m2 - ((long long)q << 51);
-    const float x = __fmul_rn(__ll2float_rn(r), 6.97573699e-16f);    // pi * 2^-52
-    const float x2 = __fmul_rn(x, x);
-    float sp = __fmaf_rn(x2, 2.75573192e-6f, -1.98412698e-4f);       // 1/9!, -1/7!
-    sp = __fmaf_rn(x2, sp, 8.33333333e-3f);                          // 1/5!
-    sp = __fmaf_rn(x2, sp, -1.66666667e-1f);                         // -1/3!
-    const float sn = __fmaf_rn(__fmul_rn(x2, x), sp, x);
-    float cp = __fmaf_rn(x2, -2.75573192e-7f, 2.48015873e-5f);       // -1/10!, 1/8!
-    cp = __fmaf_rn(x2, cp, -1.38888889e-3f);                         // -1/6!
-    cp = __fmaf_rn(x2, cp, 4.16666667e-2f);                          // 1/4!
-    cp = __fmaf_rn(x2, cp, -0.5f);
-    const float cs = __fmaf_rn(x2, cp, 1.0f);
-    // rotate by q quarter turns
+template <typename V>
+__device__ __forceinline__ V log_u1_series(V g, V k) {
+    const V s = [&] {
+        if constexpr (sizeof(V) == 4) return __fdividef(g, __fadd_rn(2.0f, g));
+        else return make_float2(__fdividef(g.x, __fadd_rn(2.0f, g.x)), __fdividef(g.y, __fadd_rn(2.0f, g.y)));
+    }();
+    const V w = v_mul(s, s);
+    V poly = v_fma(w, vs<V>(1.0f / 15.0f), vs<V>(1.0f / 13.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 11.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 9.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 7.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 5.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 3.0f));
+    poly = v_mul(w, poly);
+    const V two_s = v_add(s, s);
+    const V l1p = v_fma(two_s, poly, two_s);
+    return v_fma(k, vs<V>(kLn2Hi), v_fma(k, vs<V>(kLn2Lo), l1p));
+}
+
+// Integer half of the angle reduction: quarter turns q and the remainder x.
+__device__ __forceinline__ void angle_reduce(uint32_t h, uint32_t l, uint32_t& q, float& x) {
+    q = (h + (1u << 18)) >> 19;                        // nearest multiple of 2^51 in m2
+    const int rh = (int)h - (int)(q << 19);            // |rh| <= 2^18, exact in FP32
+    // x = pi * 2^-52 * (rh 2^32 + l)
+    x = __fmaf_rn((float)rh, 2.99605662e-6f /* pi 2^-20 */, __fmul_rn((float)l, 6.97573699e-16f));
+}
+
+template <typename V>
+__device__ __forceinline__ void sincos_series(V x, V& sn, V& cs) {
+    const V x2 = v_mul(x, x);
+    V sp = v_fma(x2, vs<V>(2.75573192e-6f), vs<V>(-1.98412698e-4f));   // 1/9!, -1/7!
+    sp = v_fma(x2, sp, vs<V>(8.33333333e-3f));                           // 1/5!
+    sp = v_fma(x2, sp, vs<V>(-1.66666667e-1f));                          // -1/3!
+    sn = v_fma(v_mul(x2, x), sp, x);
+    V cp = v_fma(x2, vs<V>(-2.75573192e-7f), vs<V>(2.48015873e-5f));   // -1/10!, 1/8!
+    cp = v_fma(x2, cp, vs<V>(-1.38888889e-3f));                          // -1/6!
+    cp = v_fma(x2, cp, vs<V>(4.16666667e-2f));                           // 1/4!
+    cp = v_fma(x2, cp, vs<V>(-0.5f));
+    cs = v_fma(x2, cp, vs<V>(1.0f));
+}
+
+// rotate (cos x, sin x) by q quarter turns -> (cos, sin) of the full angle
+__device__ __forceinline__ void quarter_turn(uint32_t q, float sn, float cs, float& c, float& s) {
     const uint32_t qq = q & 3u;
     const float a = (qq & 1u) ? sn : cs;
     const float b = (qq & 1u) ? cs : sn;
@@ -129,47 +184,92 @@ __device__ __forceinline__ void cossin_2pi_f(uint64_t m2, float& c, float& s) {
     s = (qq >= 2u) ? -b : b;
 }
 
-__device__ __forceinline__ float bm_radius_f(uint64_t m1) {
-    const float v = __fmul_rn(-2.0f, log_u1_f(m1));   // > 0
-    const float y = rsqrtf(v);
-    const float r = __fmul_rn(v, y);
-    return __fmaf_rn(__fmul_rn(0.5f, y), __fmaf_rn(-r, r, v), r);  // one Newton step
+template <typename V>
+__device__ __forceinline__ V radius_from_log(V lg) {
+    const V v = v_mul(vs<V>(-2.0f), lg);   // > 0
+    V y;
+    if constexpr (sizeof(V) == 4) y = rsqrtf(v);
+    else y = make_float2(rsqrtf(v.x), rsqrtf(v.y));
+    const V r = v_mul(v, y);
+    return v_fma(v_mul(vs<V>(0.5f), y), v_fma(v_mul(vs<V>(-1.0f), r), r, v), r);  // Newton
 }
 
+// z (cos branch) for one key, FP32.
 __device__ __forceinline__ float gauss_cos_f(uint64_t key) {
-    uint64_t m1, m2;
-    hash_bits(key, m1, m2);
-    float c, s;
-    cossin_2pi_f(m2, c, s);
-    return __fmul_rn(bm_radius_f(m1), c);
+    uint32_t h1, l1, h2, l2, q;
+    hash_words(key, h1, l1, h2, l2);
+    float g, k, x, sn, cs, c, s;
+    bool clamp;
+    log_u1_reduce(h1, l1, g, k, clamp);
+    float lg = log_u1_series<float>(g, k);
+    lg = clamp ? kLog1em12 : lg;
+    angle_reduce(h2, l2, q, x);
+    sincos_series<float>(x, sn, cs);
+    quarter_turn(q, sn, cs, c, s);
+    return __fmul_rn(radius_from_log<float>(lg), c);
 }
 
+// z for two keys in the two lanes of a float2 (bitwise the same as two calls
+// of gauss_cos_f).
+__device__ __forceinline__ float2 gauss_cos_f2(uint64_t key0, uint64_t key1) {
+    uint32_t h1a, l1a, h2a, l2a, h1b, l1b, h2b, l2b, qa, qb;
+    hash_words(key0, h1a, l1a, h2a, l2a);
+    hash_words(key1, h1b, l1b, h2b, l2b);
+    float ga, ka, gb, kb, xa, xb;
+    bool ca, cb;
+    log_u1_reduce(h1a, l1a, ga, ka, ca);
+    log_u1_reduce(h1b, l1b, gb, kb, cb);
+    float2 lg = log_u1_series<float2>(make_float2(ga, gb), make_float2(ka, kb));
+    lg.x = ca ? kLog1em12 : lg.x;
+    lg.y = cb ? kLog1em12 : lg.y;
+    angle_reduce(h2a, l2a, qa, xa);
+    angle_reduce(h2b, l2b, qb, xb);
+    float2 sn, cs;
+    sincos_series<float2>(make_float2(xa, xb), sn, cs);
+    float2 c, s;
+    quarter_turn(qa, sn.x, cs.x, c.x, s.x);
+    quarter_turn(qb, sn.y, cs.y, c.y, s.y);
+    return v_mul(radius_from_log<float2>(lg), c);
+}
+
+// (z1, z2) = r (cos, sin) for one key (complex field, one pair per site).
 __device__ __forceinline__ void gauss_pair_f(uint64_t key, float& z1, float& z2) {
-    uint64_t m1, m2;
-    hash_bits(key, m1, m2);
-    float c, s;
-    cossin_2pi_f(m2, c, s);
-    const float r = bm_radius_f(m1);
+    uint32_t h1, l1, h2, l2, q;
+    hash_words(key, h1, l1, h2, l2);
+    float g, k, x, sn, cs, c, s;
+    bool clamp;
+    log_u1_reduce(h1, l1, g, k, clamp);
+    float lg = log_u1_series<float>(g, k);
+    lg = clamp ? kLog1em12 : lg;
+    angle_reduce(h2, l2, q, x);
+    sincos_series<float>(x, sn, cs);
+    quarter_turn(q, sn, cs, c, s);
+    const float r = radius_from_log<float>(lg);
     z1 = __fmul_rn(r, c);
     z2 = __fmul_rn(r, s);
 }
 
 // ------------------------------------------------------- float-float ----
-// Error-free sum (Knuth TwoSum); the _rn intrinsics keep the compiler from
-// contracting or reordering the operations.
-__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
-    s = __fadd_rn(a, b);
-    const float bb = __fsub_rn(s, a);
-    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+// Error-free sum (Knuth TwoSum) and a renormalised float-float add, in lane
+// vectors; every operation is an explicit round-to-nearest intrinsic.
+__device__ __forceinline__ float v_neg(float a) { return -a; }
+__device__ __forceinline__ float2 v_neg(float2 a) { return make_float2(-a.x, -a.y); }
+
+template <typename V>
+__device__ __forceinline__ void two_sum(V a, V b, V& s, V& e) {
+    s = v_add(a, b);
+    const V bb = v_sub(s, a);
+    e = v_add(v_sub(a, v_sub(s, bb)), v_sub(b, bb));
 }
 
-// {hi, lo} + (dhi + dlo), renormalised.
-__device__ __forceinline__ float2 ff_add(float2 a, float dhi, float dlo) {
-    float s, e;
-    two_sum(a.x, dhi, s, e);
-    const float t = __fadd_rn(__fadd_rn(a.y, dlo), e);
-    const float hi = __fadd_rn(s, t);
-    return make_float2(hi, __fsub_rn(t, __fsub_rn(hi, s)));
+// (hi, lo) + (dhi + dlo), renormalised.
+template <typename V>
+__device__ __forceinline__ void ff_add(V ahi, V alo, V dhi, V dlo, V& hi, V& lo) {
+    V s, e;
+    two_sum(ahi, dhi, s, e);
+    const V t = v_add(v_add(alo, dlo), e);
+    hi = v_add(s, t);
+    lo = v_sub(t, v_sub(hi, s));
 }
 
 // ----------------------------------------------------------- V' source ----
@@ -202,15 +302,5 @@ __device__ __forceinline__ R poly_vprime(R c1, R c2, R c3, R x) {
     const R d = rn_fma(rn_mul(rn_mul(c3, x), x), x, rn_mul(c1, x));
     return c2 != R(0) ? rn_fma(rn_mul(c2, x), x, d) : d;
 }
-
-// ------------------------------------------------------------ storages ----
-// F64: double.  F32: float with the reference's mixed arithmetic.  F32C:
-// float2 {hi, lo} with value hi + lo (a 48-bit significand in 8 bytes).
-__device__ __forceinline__ float2 split_f32c(double v) {
-    float hi = __double2float_rn(v);
-    float lo = __double2float_rn(v - (double)hi);
-    return make_float2(hi, lo);
-}
-__device__ __forceinline__ double join_f32c(float2 v) { return (double)v.x + (double)v.y; }
 
 }  // namespace tipt

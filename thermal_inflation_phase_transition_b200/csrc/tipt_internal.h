@@ -20,6 +20,7 @@ int num_sms();
 int check_dims(int64_t nx, int64_t ny, int64_t nz);
 int check_storage(int s);
 int elem_bytes(int s);
+int elem_align(int s);
 int check_ptr(const void* p, int align, const char* name);
 bool overlap(const void* a, const void* b, int64_t n);
 int check_vsource(const tipt_vsource* vp, const char* name);

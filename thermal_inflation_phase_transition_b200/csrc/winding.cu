@@ -22,11 +22,15 @@ __device__ __forceinline__ int plaquette(double a, double b, double c, double e)
     return -(wrap_count(b - a) + wrap_count(c - b) + wrap_count(e - c) + wrap_count(a - e));
 }
 
+// Site value in FP64; F32C is planar (hi plane, then lo plane N sites later).
 template <int S>
-__device__ __forceinline__ double load_field(const void* p, int64_t s) {
+__device__ __forceinline__ double load_field(const void* p, int64_t s, int64_t N) {
     if constexpr (S == TIPT_F64) return __ldg(static_cast<const double*>(p) + s);
     else if constexpr (S == TIPT_F32) return (double)__ldg(static_cast<const float*>(p) + s);
-    else return join_f32c(__ldg(static_cast<const float2*>(p) + s));
+    else {
+        const float* f = static_cast<const float*>(p);
+        return (double)__ldg(f + s) + (double)__ldg(f + N + s);
+    }
 }
 
 struct WindParams {
@@ -61,7 +65,7 @@ __global__ void __launch_bounds__(256) winding_kernel(WindParams p) {
             const int64_t oi = (i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12;
             const int64_t oj = (j + 1 < p.n1) ? (int64_t)p.n2 : -(int64_t)(p.n1 - 1) * p.n2;
             const int64_t ok = (k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1);
-            auto th = [&](int64_t q) { return atan2(load_field<S>(p.phi2, q), load_field<S>(p.phi1, q)); };
+            auto th = [&](int64_t q) { return atan2(load_field<S>(p.phi2, q, N), load_field<S>(p.phi1, q, N)); };
             const double t00 = th(s), t10 = th(s + oi), t11 = th(s + oi + oj), t01 = th(s + oj);
             const double t1k = th(s + oi + ok), t0k = th(s + ok), tj1k = th(s + oj + ok);
             wxy = plaquette(t00, t10, t11, t01);   // (i,j)->(i+1,j)->(i+1,j+1)->(i,j+1)
@@ -128,7 +132,7 @@ extern "C" int tipt_compute_winding_number(int storage, const void* phi1, const 
                                            int64_t* counts, void* stream) {
     int rc;
     if ((rc = check_storage(storage)) || (rc = check_dims(nx, ny, nz))) return rc;
-    const int eb = elem_bytes(storage);
+    const int eb = elem_align(storage);
     if ((rc = check_ptr(phi1, eb, "phi1")) || (rc = check_ptr(phi2, eb, "phi2")) ||
         (rc = check_ptr(counts, 8, "counts")))
         return rc;

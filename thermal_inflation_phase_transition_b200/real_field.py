@@ -2,7 +2,7 @@
 
 Reference: simulation/latticeSimeRescale_numba.py (R).  Fields are CUDA tensors:
 float64 (nx,ny,nz) [FP64], float32 (nx,ny,nz) [the reference's FP32 storage],
-or float32 (nx,ny,nz,2) hi/lo pairs [FP32-compensated].  Calls are enqueued on
+or float32 (2,nx,ny,nz) hi/lo planes [FP32-compensated, value hi + lo].  Calls are enqueued on
 the current CUDA stream and do not synchronise.
 
 Extensions over the reference signatures are keyword-only:
@@ -149,12 +149,12 @@ def compute_energy_densities(phi, pi, dx, inv_a2, lam_val, mphi_val, mu):
 
 # ------------------------------------------------------------ state helpers
 def to_f32c(x: torch.Tensor) -> torch.Tensor:
-    """float64 field -> float32 (…,2) hi/lo pairs (exact to 48 bits)."""
+    """float64 field -> float32 (2, ...) hi/lo planes (exact to 48 bits)."""
     hi = x.to(torch.float32)
     lo = (x - hi.to(torch.float64)).to(torch.float32)
-    return torch.stack([hi, lo], dim=-1).contiguous()
+    return torch.stack([hi, lo], dim=0).contiguous()
 
 
 def from_f32c(x: torch.Tensor) -> torch.Tensor:
-    """float32 (…,2) hi/lo pairs -> float64 field."""
-    return x[..., 0].to(torch.float64) + x[..., 1].to(torch.float64)
+    """float32 (2, ...) hi/lo planes -> float64 field."""
+    return x[0].to(torch.float64) + x[1].to(torch.float64)

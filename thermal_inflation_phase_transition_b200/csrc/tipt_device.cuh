@@ -36,7 +36,11 @@ __device__ __forceinline__ void hash_pair(uint64_t x, double& u1, double& u2) {
 // extension that leaves the reference key unchanged at seed = 0.
 __device__ __forceinline__ uint64_t noise_key(uint64_t site, uint64_t step, uint64_t mul,
                                               uint64_t seed) {
-    return ((site * mul) ^ step) + seed * kSeedStride;
+    // the pass multipliers are 32-bit; a 32-bit site then needs one wide multiply
+    const uint64_t sm = (site >> 32) == 0 && (mul >> 32) == 0
+                            ? (uint64_t)(uint32_t)site * (uint64_t)(uint32_t)mul
+                            : site * mul;
+    return (sm ^ step) + seed * kSeedStride;
 }
 
 // R:2519-2521 Box-Muller radius and angle, FP64 (the reference's precision).
@@ -115,42 +119,46 @@ constexpr float kLn2Lo = -1.904654299957768e-09f;    // ln 2 - kLn2Hi
 constexpr float kLog1em12 = -27.631021115928547f;    // log(1e-12)
 
 // Integer half of the log reduction for one lane: g (log1p argument) and k
-// (power of two), plus the clamp flag.
+// (power of two), plus the clamp flag.  Both reductions are formed and one is
+// selected, so lanes of a warp do not diverge.
 __device__ __forceinline__ void log_u1_reduce(uint32_t h, uint32_t l, float& g, float& k,
                                               bool& clamp) {
     clamp = (h == 0u) && (l <= 9007u);
-    if (h >= (1u << 20)) {
-        // u1 >= 1/2: g = -(1 - u1) = -((2^21 - h) 2^-21 - l 2^-53)
-        g = __fmaf_rn(-(float)((1u << 21) - h), 0x1p-21f, __fmul_rn((float)l, 0x1p-53f));
-        k = 0.0f;
-    } else {
-        const float u = __fmaf_rn((float)h, 0x1p-21f, __fmul_rn((float)l, 0x1p-53f));
-        const uint32_t b = __float_as_uint(u);
-        // mantissa in [3/4, 3/2): shift the exponent when the mantissa is >= 3/2
-        const uint32_t up = (b & 0x00400000u) ? 1u : 0u;
-        const int e = (int)((b >> 23) & 0xffu) - 127 + (int)up;
-        g = __fsub_rn(__uint_as_float((b & 0x007fffffu) | ((127u - up) << 23)), 1.0f);
-        k = (float)e;
-    }
+    const float lo = __fmul_rn((float)l, 0x1p-53f);
+    // u1 >= 1/2: g = -(1 - u1) = -((2^21 - h) 2^-21 - l 2^-53)
+    const float g_hi = __fmaf_rn(-(float)((1u << 21) - h), 0x1p-21f, lo);
+    // u1 < 1/2: mantissa of the FP32 value of u1 in [3/4, 3/2), exponent e
+    const float u = __fmaf_rn((float)h, 0x1p-21f, lo);
+    const uint32_t b = __float_as_uint(u);
+    const uint32_t up = (b >> 22) & 1u;
+    const int e = (int)((b >> 23) & 0xffu) - 127 + (int)up;
+    const float g_lo = __fsub_rn(__uint_as_float((b & 0x007fffffu) | ((127u - up) << 23)), 1.0f);
+    const bool big = h >= (1u << 20);
+    g = big ? g_hi : g_lo;
+    k = big ? 0.0f : (float)e;
 }
 
+__device__ __forceinline__ float log_u1_series1(float g, float k) {
+    const float s = __fdividef(g, __fadd_rn(2.0f, g));
+    const float w = __fmul_rn(s, s);
+    float poly = __fmaf_rn(w, 1.0f / 15.0f, 1.0f / 13.0f);
+    poly = __fmaf_rn(w, poly, 1.0f / 11.0f);
+    poly = __fmaf_rn(w, poly, 1.0f / 9.0f);
+    poly = __fmaf_rn(w, poly, 1.0f / 7.0f);
+    poly = __fmaf_rn(w, poly, 1.0f / 5.0f);
+    poly = __fmaf_rn(w, poly, 1.0f / 3.0f);
+    poly = __fmul_rn(w, poly);
+    const float two_s = __fadd_rn(s, s);
+    const float l1p = __fmaf_rn(two_s, poly, two_s);
+    return __fmaf_rn(k, kLn2Hi, __fmaf_rn(k, kLn2Lo, l1p));
+}
+
+// Series in lane vectors: evaluated lane by lane with immediate coefficients
+// (bitwise the same for both lane widths).
 template <typename V>
 __device__ __forceinline__ V log_u1_series(V g, V k) {
-    const V s = [&] {
-        if constexpr (sizeof(V) == 4) return __fdividef(g, __fadd_rn(2.0f, g));
-        else return make_float2(__fdividef(g.x, __fadd_rn(2.0f, g.x)), __fdividef(g.y, __fadd_rn(2.0f, g.y)));
-    }();
-    const V w = v_mul(s, s);
-    V poly = v_fma(w, vs<V>(1.0f / 15.0f), vs<V>(1.0f / 13.0f));
-    poly = v_fma(w, poly, vs<V>(1.0f / 11.0f));
-    poly = v_fma(w, poly, vs<V>(1.0f / 9.0f));
-    poly = v_fma(w, poly, vs<V>(1.0f / 7.0f));
-    poly = v_fma(w, poly, vs<V>(1.0f / 5.0f));
-    poly = v_fma(w, poly, vs<V>(1.0f / 3.0f));
-    poly = v_mul(w, poly);
-    const V two_s = v_add(s, s);
-    const V l1p = v_fma(two_s, poly, two_s);
-    return v_fma(k, vs<V>(kLn2Hi), v_fma(k, vs<V>(kLn2Lo), l1p));
+    if constexpr (sizeof(V) == 4) return log_u1_series1(g, k);
+    else return make_float2(log_u1_series1(g.x, k.x), log_u1_series1(g.y, k.y));
 }
 
 // Integer half of the angle reduction: quarter turns q and the remainder x.
@@ -161,18 +169,27 @@ __device__ __forceinline__ void angle_reduce(uint32_t h, uint32_t l, uint32_t& q
     x = __fmaf_rn((float)rh, 2.99605662e-6f /* pi 2^-20 */, __fmul_rn((float)l, 6.97573699e-16f));
 }
 
+__device__ __forceinline__ void sincos_series1(float x, float& sn, float& cs) {
+    const float x2 = __fmul_rn(x, x);
+    float sp = __fmaf_rn(x2, 2.75573192e-6f, -1.98412698e-4f);   // 1/9!, -1/7!
+    sp = __fmaf_rn(x2, sp, 8.33333333e-3f);                      // 1/5!
+    sp = __fmaf_rn(x2, sp, -1.66666667e-1f);                     // -1/3!
+    sn = __fmaf_rn(__fmul_rn(x2, x), sp, x);
+    float cp = __fmaf_rn(x2, -2.75573192e-7f, 2.48015873e-5f);   // -1/10!, 1/8!
+    cp = __fmaf_rn(x2, cp, -1.38888889e-3f);                     // -1/6!
+    cp = __fmaf_rn(x2, cp, 4.16666667e-2f);                      // 1/4!
+    cp = __fmaf_rn(x2, cp, -0.5f);
+    cs = __fmaf_rn(x2, cp, 1.0f);
+}
+
 template <typename V>
 __device__ __forceinline__ void sincos_series(V x, V& sn, V& cs) {
-    const V x2 = v_mul(x, x);
-    V sp = v_fma(x2, vs<V>(2.75573192e-6f), vs<V>(-1.98412698e-4f));   // 1/9!, -1/7!
-    sp = v_fma(x2, sp, vs<V>(8.33333333e-3f));                           // 1/5!
-    sp = v_fma(x2, sp, vs<V>(-1.66666667e-1f));                          // -1/3!
-    sn = v_fma(v_mul(x2, x), sp, x);
-    V cp = v_fma(x2, vs<V>(-2.75573192e-7f), vs<V>(2.48015873e-5f));   // -1/10!, 1/8!
-    cp = v_fma(x2, cp, vs<V>(-1.38888889e-3f));                          // -1/6!
-    cp = v_fma(x2, cp, vs<V>(4.16666667e-2f));                           // 1/4!
-    cp = v_fma(x2, cp, vs<V>(-0.5f));
-    cs = v_fma(x2, cp, vs<V>(1.0f));
+    if constexpr (sizeof(V) == 4) {
+        sincos_series1(x, sn, cs);
+    } else {
+        sincos_series1(x.x, sn.x, cs.x);
+        sincos_series1(x.y, sn.y, cs.y);
+    }
 }
 
 // rotate (cos x, sin x) by q quarter turns -> (cos, sin) of the full angle
@@ -184,14 +201,17 @@ __device__ __forceinline__ void quarter_turn(uint32_t q, float sn, float cs, flo
     s = (qq >= 2u) ? -b : b;
 }
 
+__device__ __forceinline__ float radius_from_log1(float lg) {
+    const float v = __fmul_rn(-2.0f, lg);   // > 0
+    const float y = rsqrtf(v);
+    const float r = __fmul_rn(v, y);
+    return __fmaf_rn(__fmul_rn(0.5f, y), __fmaf_rn(-r, r, v), r);  // one Newton step
+}
+
 template <typename V>
 __device__ __forceinline__ V radius_from_log(V lg) {
-    const V v = v_mul(vs<V>(-2.0f), lg);   // > 0
-    V y;
-    if constexpr (sizeof(V) == 4) y = rsqrtf(v);
-    else y = make_float2(rsqrtf(v.x), rsqrtf(v.y));
-    const V r = v_mul(v, y);
-    return v_fma(v_mul(vs<V>(0.5f), y), v_fma(v_mul(vs<V>(-1.0f), r), r, v), r);  // Newton
+    if constexpr (sizeof(V) == 4) return radius_from_log1(lg);
+    else return make_float2(radius_from_log1(lg.x), radius_from_log1(lg.y));
 }
 
 // z (cos branch) for one key, FP32.

@@ -132,6 +132,21 @@ int tipt_rk2_fused_table(int storage, const void* phi, const void* pi, void* phi
                          int64_t nz, const tipt_step_params* sp, const tipt_vsource* vp_T,
                          const tipt_vsource* vp_Tm, const void* noise, void* stream);
 
+/* Allocation-free form of tipt_rk2_fused_table, for callers that cannot
+ * allocate device memory (code running inside another library's CUDA-graph
+ * capture, hosts without a device allocator, real-time loops).  No counterpart
+ * in the reference.  The intermediate state lives in an 8 MiB device array
+ * inside the library (held by every GPU that loads it until exit); lattices
+ * whose intermediate phi and pi exceed it (about 512K sites for F64 / F32C,
+ * 1M for F32) are rejected with TIPT_ERR_UNSUPPORTED.  All calls share the
+ * array: calls that overlap on the GPU race.  The first call on each device
+ * looks up the array's device address and should precede any stream capture.
+ * Allocates nothing. */
+int tipt_rk2_fused_table_noalloc(int storage, const void* phi, const void* pi, void* phi_out,
+                                 void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                                 const tipt_step_params* sp, const tipt_vsource* vp_T,
+                                 const tipt_vsource* vp_Tm, const void* noise, void* stream);
+
 /* --------------------------------------------------------- complex field */
 
 /* Complex rk2_step_table (C:2067-2215): the real step for Phi = phi1 + i phi2

@@ -121,6 +121,23 @@ int tipt_rk2_step_table(int storage, const void* phi, const void* pi, void* phi_
                         const tipt_step_params* sp, const tipt_vsource* vp, const void* noise,
                         void* stream);
 
+/* rk2_step_table with the per-step scalars read on the device, for step loops
+ * captured once into a CUDA graph and replayed (the reference's host loop
+ * R:3619-3768 recomputes them each step on the host).  The step index is
+ * s = *counter + offset; the V' 2-D table is blended at T = sched[2s], the
+ * inline hash noise has amplitude sched[2s+1] and hash step
+ * sp->noise_step + s.  sched is a device array of sched_len (T, ns) pairs
+ * (steps beyond it reuse the last pair); counter is a device uint64 that the
+ * caller advances with tipt_counter_add. */
+int tipt_rk2_step_table_sched(int storage, const void* phi, const void* pi, void* phi_out,
+                              void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                              const tipt_step_params* sp, const tipt_vsource* vp,
+                              const double* sched, int64_t sched_len, const uint64_t* counter,
+                              int64_t offset, void* stream);
+
+/* *counter += k on the stream (one-thread kernel; graph-capturable). */
+int tipt_counter_add(uint64_t* counter, int64_t k, void* stream);
+
 /* rk2_fused_table (R:1708-1872): two dt/2 midpoint halves, the first with
  * vp_T, the second with vp_Tm; array noise adds 0.5*noise in each half
  * (R:1806, R:1872).  With noise == NULL the halves use the inline hash of

@@ -55,6 +55,9 @@ _SIGS = {
     "tipt_rk2_fused_table": [_i, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
                              C.POINTER(StepParams), C.POINTER(VSource), C.POINTER(VSource), _p,
                              _p],
+    "tipt_rk2_step_table_sched": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
+                                  C.POINTER(VSource), _p, _i64, _p, _i64, _p],
+    "tipt_counter_add": [_p, _i64, _p],
     "tipt_rk2_fused_table_noalloc": [_i, _p, _p, _p, _p, _i64, _i64, _i64,
                                      C.POINTER(StepParams), C.POINTER(VSource),
                                      C.POINTER(VSource), _p, _p],

@@ -195,6 +195,43 @@ int tipt_rk2_step_table(int storage, const void* phi, const void* pi, void* phi_
     return launch_real_stage(storage, p, (cudaStream_t)stream);
 }
 
+int tipt_rk2_step_table_sched(int storage, const void* phi, const void* pi, void* phi_out,
+                              void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                              const tipt_step_params* sp, const tipt_vsource* vp,
+                              const double* sched, int64_t sched_len, const uint64_t* counter,
+                              int64_t offset, void* stream) {
+    int rc;
+    if ((rc = check_state(storage, phi, pi, phi_out, pi_out, nx, ny, nz))) return rc;
+    if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
+    if ((rc = check_vsource(vp, "vp"))) return rc;
+    if ((rc = check_ptr(sched, 8, "sched")) || (rc = check_ptr(counter, 8, "counter"))) return rc;
+    if (sched_len < 1 || offset < 0) return fail(TIPT_ERR_ARG, "bad schedule length or offset");
+    RealStageParams p = stage_params(phi, pi, phi_out, pi_out, nx, ny, nz, sp, vp);
+    p.h1 = 0.5 * sp->dt;
+    p.h2 = sp->dt;
+    p.noise = nullptr;
+    p.nfac = 1.0;
+    p.ns_eff = 0.0;
+    p.mul = kPass2Mul;
+    p.sched = sched;
+    p.ctr = reinterpret_cast<const unsigned long long*>(counter);
+    p.offset = offset;
+    p.sched_len = sched_len;
+    p.ns_mult = 1.0;
+    return launch_real_stage(storage, p, (cudaStream_t)stream);
+}
+
+__global__ void counter_add_kernel(unsigned long long* c, long long k) { *c += (unsigned long long)k; }
+
+int tipt_counter_add(uint64_t* counter, int64_t k, void* stream) {
+    int rc;
+    if ((rc = check_ptr(counter, 8, "counter"))) return rc;
+    counter_add_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<unsigned long long*>(counter), (long long)k);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "counter_add launch");
+}
+
 int tipt_rk2_fused_table(int storage, const void* phi, const void* pi, void* phi_out,
                          void* pi_out, void* mid_phi, void* mid_pi, int64_t nx, int64_t ny,
                          int64_t nz, const tipt_step_params* sp, const tipt_vsource* vp_T,

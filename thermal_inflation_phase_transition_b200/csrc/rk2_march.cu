@@ -150,7 +150,9 @@ constexpr int kMarchRegs = 96;
 template <int S, bool WIDE>
 __global__ void __maxnreg__(kMarchRegs)
     rk2_stage_march(const __grid_constant__ CUtensorMap tm_phi,
-                    const __grid_constant__ CUtensorMap tm_pi, RealStageParams p, MarchGeom g) {
+                    const __grid_constant__ CUtensorMap tm_pi, RealStageParams p_in, MarchGeom g) {
+    RealStageParams p = p_in;
+    resolve_schedule(p);
     using E = typename MarchElem<S>::E;
     using TT = typename MarchElem<S>::TT;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -327,8 +329,10 @@ __global__ void __maxnreg__(kMarchRegs)
 template <bool WIDE>
 __global__ void __maxnreg__(kMarchRegs)
     rk2_stage_march_f32c(const __grid_constant__ CUtensorMap tm_phi,
-                         const __grid_constant__ CUtensorMap tm_pi, RealStageParams p,
+                         const __grid_constant__ CUtensorMap tm_pi, RealStageParams p_in,
                          MarchGeom g) {
+    RealStageParams p = p_in;
+    resolve_schedule(p);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     float* s_tab = reinterpret_cast<float*>(smem);

@@ -11,7 +11,9 @@
 namespace tipt {
 
 template <int S>
-__global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p) {
+__global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
+    RealStageParams p = p_in;
+    resolve_schedule(p);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using TT = typename std::conditional<S == TIPT_F32C, float, double>::type;
     TT* s_tab = reinterpret_cast<TT*>(smem_raw);

@@ -34,7 +34,25 @@ struct RealStageParams {
     double T_min, T_dinv, T;
     double c1, c2, c3;
     int table_in_smem;   // 1: stage (and blend) the row into dynamic smem
+    // Device-resident schedule (for graph-captured step loops): when sched is
+    // set, the step is s = *ctr + offset, T = sched[2s], the noise amplitude
+    // is ns_mult * sched[2s+1] and the hash step is step + s.
+    const double* sched;
+    const unsigned long long* ctr;
+    long long offset;
+    long long sched_len;  // steps beyond the schedule reuse its last entry
+    double ns_mult;
 };
+
+// Resolve the per-step scalars of a scheduled launch (no-op otherwise).
+__device__ __forceinline__ void resolve_schedule(RealStageParams& p) {
+    if (!p.sched) return;
+    const unsigned long long s = *p.ctr + (unsigned long long)p.offset;
+    const unsigned long long e = s < (unsigned long long)p.sched_len ? s : p.sched_len - 1;
+    p.T = p.sched[2 * e];
+    p.ns_eff = p.ns_mult * p.sched[2 * e + 1];
+    p.step += s;
+}
 
 // Row-blend weight of a 2-D table (same trunc/clamp/unclamped-weight rule
 // along T as along phi).

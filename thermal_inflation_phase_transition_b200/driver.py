@@ -1,0 +1,223 @@
+"""Host step driver: the reference's per-step loop (R:3619-3880) on the GPU.
+
+The reference recomputes T(t), the noise amplitude and the table on the host
+every step and calls one numba kernel.  Here the per-step scalars for the whole
+run are computed once in FP64 on the host (``schedule``), uploaded, and read by
+the kernels through a device step counter, so a chunk of K steps (each step a
+fused midpoint launch, optionally followed by the observables reduction) is
+captured once into a CUDA graph and replayed; the graph ends by advancing the
+counter.  No host synchronisation happens inside a chunk.
+
+    sim = Simulation((256, 256, 1), storage="f64", table=Table1D(...),
+                     schedule=constant_temperature(1.02, 2000, dt=0.05))
+    history = sim.run(2000)          # (2000, 10) observables, FP64, on the host
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from ._common import ptr, step_params, stream_handle, table_source
+from .observables import OBS_INDEX, OBS_NAMES, workspace_bytes
+from .real_field import to_f32c
+
+__all__ = ["Table1D", "Table2D", "Simulation", "constant_temperature", "linear_cooling",
+           "toy_vprime", "OBS_NAMES", "OBS_INDEX"]
+
+
+def toy_vprime(phi, T, D=0.1, E=0.05, lam=0.1, T0=1.0):
+    """V'(phi) of V = D(T^2-T0^2) phi^2 - E T phi^3 + (lam/4) phi^4."""
+    phi = np.asarray(phi, np.float64)
+    return 2.0 * D * (T * T - T0 * T0) * phi - 3.0 * E * T * phi * phi + lam * phi ** 3
+
+
+@dataclass
+class Table1D:
+    """Uniform V' table at one temperature (R:840-849 build_vprime_table)."""
+    values: np.ndarray
+    tmin: float
+    dinv: float
+
+    @classmethod
+    def build(cls, fn, T, lo, hi, n):
+        x = np.linspace(lo, hi, n, dtype=np.float64)
+        return cls(np.ascontiguousarray(fn(x, T), np.float64), float(lo),
+                   1.0 / ((hi - lo) / (n - 1)))
+
+
+@dataclass
+class Table2D:
+    """V'(phi, T) on a uniform (T, phi) grid, rows blended at the step's T."""
+    values: np.ndarray  # [nT][nphi]
+    tmin: float
+    dinv: float
+    T_min: float
+    T_dinv: float
+
+    @classmethod
+    def build(cls, fn, lo, hi, n_phi, T_lo, T_hi, n_T):
+        x = np.linspace(lo, hi, n_phi, dtype=np.float64)
+        Ts = np.linspace(T_lo, T_hi, n_T, dtype=np.float64)
+        v = np.stack([fn(x, T) for T in Ts]).astype(np.float64)
+        return cls(np.ascontiguousarray(v), float(lo), 1.0 / ((hi - lo) / (n_phi - 1)),
+                   float(T_lo), 1.0 / ((T_hi - T_lo) / (n_T - 1)))
+
+
+def noise_amplitude(T, eta, dt, dx_phys=1.0, mu=1.0, a=1.0):
+    """ns = sqrt(2 eta T dt a^-3 / (mu^2 dx_phys^3))  (R:3714-3718)."""
+    return math.sqrt(max(2.0 * eta * T * dt / (a ** 3) / (mu * mu * dx_phys ** 3), 0.0))
+
+
+def constant_temperature(T, n_steps, *, dt, eta=1.0, dx_phys=1.0, mu=1.0, noise=True):
+    """(n_steps, 2) schedule of (T, ns) at fixed T (the reference's --no_hubble run)."""
+    ns = noise_amplitude(T, eta, dt, dx_phys, mu) if noise else 0.0
+    return np.tile(np.array([[T, ns]], np.float64), (n_steps, 1))
+
+
+def linear_cooling(T_start, T_end, n_cool, n_steps, *, dt, eta=1.0, dx_phys=1.0, mu=1.0,
+                   noise=True):
+    """T(t) = max(T_start - rate t, 0) with rate = (T_start - T_end)/(n_cool dt)
+    (the temperature(t) form of R:2828-2829), t = n dt."""
+    rate = (T_start - T_end) / (n_cool * dt)
+    n = np.arange(n_steps, dtype=np.float64)
+    T = np.maximum(T_start - rate * (n * dt), 0.0)
+    ns = np.array([noise_amplitude(t, eta, dt, dx_phys, mu) if noise else 0.0 for t in T])
+    return np.ascontiguousarray(np.stack([T, ns], axis=1), np.float64)
+
+
+class Simulation:
+    """A real scalar field on a periodic lattice, stepped by graph-captured chunks.
+
+    storage: "f64", "f32" (the reference's float32 mode) or "f32c" (compensated).
+    phi0/pi0: initial fields (numpy, FP64); default phi ~ N(0, init_sigma^2), pi = 0.
+    """
+
+    def __init__(self, shape, *, storage="f32c", dt=0.05, dx=1.0, eta=1.0, mu=1.0, inv_a2=1.0,
+                 table, schedule, seed=0, phi0=None, pi0=None, init_sigma=0.01, init_seed=0,
+                 obs_threshold=1.0, graph_steps=50, device="cuda"):
+        self.shape = tuple(int(x) for x in shape)
+        self.storage = storage
+        self.dev = torch.device(device)
+        self.dt, self.dx, self.eta, self.mu, self.inv_a2 = dt, dx, eta, mu, inv_a2
+        self.seed = seed
+        self.thr = obs_threshold
+        self.graph_steps = max(2, graph_steps + (graph_steps & 1))  # even: state ends in buffer 0
+        self.schedule = np.ascontiguousarray(schedule, np.float64)
+        if self.schedule.ndim != 2 or self.schedule.shape[1] != 2:
+            raise ValueError("schedule must be (n_steps, 2): (T, ns) per step")
+        self._sched = torch.from_numpy(self.schedule).to(self.dev)
+        self._table = torch.from_numpy(np.asarray(table.values)).to(self.dev)
+        if isinstance(table, Table2D):
+            self._vs = table_source(self._table, table.tmin, table.dinv, table.values.shape[1],
+                                    float(self.schedule[0, 0]), table.T_min, table.T_dinv)
+        else:
+            self._vs = table_source(self._table, table.tmin, table.dinv, table.values.shape[0])
+        if phi0 is None:
+            phi0 = np.random.default_rng(init_seed).normal(0.0, init_sigma, self.shape)
+        if pi0 is None:
+            pi0 = np.zeros(self.shape)
+        self.phi = [self._to_storage(phi0), None]
+        self.pi = [self._to_storage(pi0), None]
+        self.phi[1] = torch.empty_like(self.phi[0])
+        self.pi[1] = torch.empty_like(self.pi[0])
+        self._counter = torch.zeros(1, dtype=torch.int64, device=self.dev)
+        self._ws = torch.empty(workspace_bytes(self.shape) // 8 + 1, dtype=torch.float64,
+                               device=self.dev)
+        self._sp = step_params(dt, dx, eta, mu, inv_a2, 0.0, 0, seed)
+        self.steps_done = 0
+        self._graphs = {}
+
+    # ------------------------------------------------------------- state
+    def _to_storage(self, a):
+        t = torch.from_numpy(np.ascontiguousarray(a, np.float64)).to(self.dev)
+        if self.storage == "f64":
+            return t
+        if self.storage == "f32":
+            return t.to(torch.float32).contiguous()
+        if self.storage == "f32c":
+            return to_f32c(t)
+        raise ValueError(f"unknown storage {self.storage}")
+
+    def fields(self):
+        """Current (phi, pi) as FP64 CUDA tensors."""
+        def f64(t):
+            if self.storage == "f32c":
+                return t[0].double() + t[1].double()
+            return t.double()
+        return f64(self.phi[0]), f64(self.pi[0])
+
+    # ------------------------------------------------------------ stepping
+    def _st(self):
+        return {"f64": L.TIPT_F64, "f32": L.TIPT_F32, "f32c": L.TIPT_F32C}[self.storage]
+
+    def _launch_chunk(self, K, obs):
+        """Enqueue K steps (+ observables into obs[q]) and the counter advance."""
+        lib = L.lib()
+        st = stream_handle()
+        nx, ny, nz = self.shape
+        for q in range(K):
+            a, b = q & 1, (q + 1) & 1
+            rc = lib.tipt_rk2_step_table_sched(
+                self._st(), ptr(self.phi[a]), ptr(self.pi[a]), ptr(self.phi[b]), ptr(self.pi[b]),
+                nx, ny, nz, self._sp, self._vs, ptr(self._sched), self.schedule.shape[0],
+                ptr(self._counter), q, st)
+            L.check(rc, "tipt_rk2_step_table_sched")
+            if obs is not None:
+                rc = lib.tipt_observables(self._st(), ptr(self.phi[b]), ptr(self.pi[b]), nx, ny,
+                                          nz, float(self.dx), float(self.inv_a2), 0.0, 0.0,
+                                          float(self.mu), float(self.thr), ptr(obs[q]),
+                                          ptr(self._ws), self._ws.numel() * 8, st)
+                L.check(rc, "tipt_observables")
+        L.check(lib.tipt_counter_add(ptr(self._counter), K, st), "tipt_counter_add")
+
+    def _graph(self, K, observe):
+        # a graph bakes the buffer pointers: an odd eager remainder exchanges the
+        # two buffers, so the graph is keyed by which buffer holds the state
+        key = (K, observe, self.phi[0].data_ptr())
+        if key not in self._graphs:
+            obs = torch.zeros((K, 10), dtype=torch.float64, device=self.dev) if observe else None
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                self._launch_chunk(K, obs)
+            torch.cuda.current_stream().wait_stream(s)
+            self._graphs[key] = (g, obs)
+        return self._graphs[key]
+
+    def run(self, n_steps, *, observe=True, use_graphs=True):
+        """Advance n_steps; returns the per-step observables (n_steps, 10) on the host
+        (None if observe=False).  Steps beyond the schedule reuse its last (T, ns)."""
+        K = self.graph_steps
+        out = []
+        done = 0
+        while done < n_steps:
+            k = min(K, n_steps - done)
+            if use_graphs and k == K:
+                g, obs = self._graph(K, observe)
+                g.replay()
+                if observe:
+                    out.append(obs.clone())
+            else:
+                # remainder (or graphs off): eager launches in pairs keep the
+                # state in buffer 0; an odd final step is followed by a swap
+                obs = torch.zeros((k, 10), dtype=torch.float64, device=self.dev) if observe else None
+                self._launch_chunk(k, obs)
+                if k & 1:
+                    self.phi.reverse()
+                    self.pi.reverse()
+                if observe:
+                    out.append(obs)
+            done += k
+        self.steps_done += n_steps
+        if not observe:
+            return None
+        return torch.cat(out).cpu().numpy()
+
+    def synchronize(self):
+        torch.cuda.synchronize(self.dev)

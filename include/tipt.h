@@ -195,6 +195,50 @@ int tipt_compute_winding_number(int storage, const void* phi1, const void* phi2,
                                 uint32_t* pierced, int64_t pierced_cap, int64_t* counts,
                                 void* stream);
 
+/* -------------------------------------------------------------- ensemble */
+
+/* One replica of a batched ensemble (no reference counterpart: the reference
+ * runs one lattice per invocation).  Replicas are slices of one packed state
+ * buffer (planar hi/lo for TIPT_F32C over all n_total sites).  A 2-D lattice
+ * is given as (1, nx, ny). */
+typedef struct {
+    int32_t n0, n1, n2;  /* extents; n2 contiguous */
+    uint32_t m1, m2;     /* ceil(2^32 / n1), ceil(2^32 / n2); 0 for an extent of 1 */
+    int32_t pad_;
+    int64_t offset;      /* first site of the replica in the packed buffers */
+    double c1, c2, c3;   /* V'(phi) = c1 phi + c2 phi^2 + c3 phi^3 */
+    double noise_scale;  /* ns: kick ns*z per step (R:3714-3718) */
+    uint64_t seed;       /* hash noise seed of the replica */
+} tipt_replica;
+
+/* A work-list entry: sites [begin, begin + count) of one replica. */
+typedef struct {
+    int32_t replica;
+    int32_t count;
+    int64_t begin;
+} tipt_chunk;
+
+/* One midpoint RK2 step (the rk2_step_table arithmetic, R:1875-1966, with a
+ * polynomial V' and inline hash noise) of every active replica, as one
+ * persistent launch over the chunk work-list; replicas with active[r] == 0 are
+ * skipped.  sp supplies dt, dx, eta_eff, mu, inv_a2; the hash step is
+ * sp->noise_step, plus *counter + offset when counter (a device uint64) is
+ * given (graph-captured loops). */
+int tipt_ensemble_step(int storage, const void* phi, const void* pi, void* phi_out, void* pi_out,
+                       int64_t n_total, const tipt_replica* replicas, const tipt_chunk* chunks,
+                       int32_t n_chunks, const int32_t* active, const tipt_step_params* sp,
+                       const uint64_t* counter, int64_t offset, void* stream);
+
+/* Per replica (one block each, fixed order): frac_out[r] = fraction of sites
+ * with phi > thr.  An active replica whose fraction exceeds stop_frac gets
+ * first_step[r] = step (+ *counter + offset), active[r] = 0, and *n_active is
+ * decremented. */
+int tipt_ensemble_observe(int storage, const void* phi, int64_t n_total,
+                          const tipt_replica* replicas, int32_t n_replicas, int32_t* active,
+                          int32_t* n_active, double thr, double stop_frac, uint64_t step,
+                          const uint64_t* counter, int64_t offset, int64_t* first_step,
+                          double* frac_out, void* stream);
+
 /* ----------------------------------------------------------- observables */
 
 /* compute_energy_densities (R:2270-2319) plus the host loop's per-step

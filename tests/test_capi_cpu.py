@@ -103,3 +103,12 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(L, "LIB_PATH", str(tmp_path / "libtipt.so"))
     with pytest.raises(RuntimeError, match="no CPU"):
         L.lib()
+
+
+def test_gamma_mle_censoring():
+    from thermal_inflation_phase_transition_b200.ensemble import gamma_mle
+    # 3 events at steps 9, 19, 99 and one censored at 100 steps, volume 8, dt 0.5
+    g, rel, n = gamma_mle([9, 19, 99, -1], 100, 8.0, 0.5)
+    assert n == 3
+    assert abs(g - 3 / (8.0 * 0.5 * (10 + 20 + 100 + 100))) < 1e-15
+    assert abs(rel - 1 / 3 ** 0.5) < 1e-15

@@ -36,6 +36,17 @@ class StepParams(C.Structure):
                 ("noise_step", C.c_uint64), ("noise_seed", C.c_uint64)]
 
 
+class Replica(C.Structure):
+    _fields_ = [("n0", C.c_int32), ("n1", C.c_int32), ("n2", C.c_int32), ("m1", C.c_uint32),
+                ("m2", C.c_uint32), ("pad_", C.c_int32), ("offset", C.c_int64),
+                ("c1", C.c_double), ("c2", C.c_double), ("c3", C.c_double),
+                ("noise_scale", C.c_double), ("seed", C.c_uint64)]
+
+
+class Chunk(C.Structure):
+    _fields_ = [("replica", C.c_int32), ("count", C.c_int32), ("begin", C.c_int64)]
+
+
 class ComplexTerms(C.Structure):
     _fields_ = [("zn_n", C.c_double), ("zn_dv", C.c_double), ("zn_active", C.c_double),
                 ("eps4", C.c_double)]
@@ -58,6 +69,10 @@ _SIGS = {
     "tipt_rk2_step_table_sched": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
                                   C.POINTER(VSource), _p, _i64, _p, _i64, _p],
     "tipt_counter_add": [_p, _i64, _p],
+    "tipt_ensemble_step": [_i, _p, _p, _p, _p, _i64, _p, _p, C.c_int32, _p,
+                           C.POINTER(StepParams), _p, _i64, _p],
+    "tipt_ensemble_observe": [_i, _p, _i64, _p, C.c_int32, _p, _p, _d, _d, _u64, _p, _i64, _p,
+                              _p, _p],
     "tipt_rk2_fused_table_noalloc": [_i, _p, _p, _p, _p, _i64, _i64, _i64,
                                      C.POINTER(StepParams), C.POINTER(VSource),
                                      C.POINTER(VSource), _p, _p],

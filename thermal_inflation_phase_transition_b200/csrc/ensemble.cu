@@ -1,0 +1,241 @@
+// Batched ensemble of independent real-field replicas with uneven lattice
+// sizes, seeds and potentials, advanced by one persistent launch per step.
+//
+// The reference runs one replica per CLI invocation (one numba call per
+// step).  Here every replica's state is a slice of one packed buffer (planar
+// for the compensated storage: hi plane of all replicas, then the lo plane);
+// a work-list of chunks (replica, site range) covers the active replicas and
+// persistent CTAs walk it, so a step of 1792 small replicas is one launch
+// instead of 1792.  Each site runs the same midpoint arithmetic as the
+// single-lattice kernels, with the replica's own extents, noise seed and
+// amplitude, and polynomial V'(phi) = c1 phi + c2 phi^2 + c3 phi^3 (the
+// potential family's derivative: c1 = 2D(T^2-T0^2), c2 = -3ET, c3 = lam).
+// Results are bitwise those of stepping the replica alone with the generic
+// kernel.
+//
+// tipt_ensemble_observe reduces, per replica and in a fixed order, the
+// fraction of sites with phi > thr; the first time it exceeds the stop
+// fraction the step is recorded as the replica's first-passage step and the
+// replica is retired (its chunks are skipped from then on).
+#include <cstring>
+
+#include "rk2_real.cuh"
+#include "tipt_internal.h"
+
+namespace tipt {
+
+struct EnsParams {
+    const void* phi;
+    const void* pi;
+    void* phi_out;
+    void* pi_out;
+    int64_t n_total;
+    const tipt_replica* reps;
+    const tipt_chunk* chunks;
+    int n_chunks;
+    const int32_t* active;
+    double h1, h2, inv_dx2, eta, inv_mu2, inv_a2;
+    uint64_t step;                       // hash step = step (+ *ctr + offset)
+    const unsigned long long* ctr;       // device step counter or nullptr
+    long long offset;
+};
+
+// x / d for x < 2^32 / d by a multiply-high with m = ceil(2^32 / d) (exact:
+// x m / 2^32 = x/d + x e / (d 2^32) with e = m d - 2^32 < d); m = 0 means d = 1.
+__device__ __forceinline__ uint32_t fdiv(uint32_t x, uint32_t m) { return m ? __umulhi(x, m) : x; }
+
+template <int S>
+__global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
+    const uint64_t step = e.step + (e.ctr ? *e.ctr + (unsigned long long)e.offset : 0ull);
+    for (int c = blockIdx.x; c < e.n_chunks; c += gridDim.x) {
+        const tipt_chunk ch = e.chunks[c];
+        if (!e.active[ch.replica]) continue;
+        const tipt_replica rp = e.reps[ch.replica];
+        // the replica as a single lattice with a polynomial V' and hash noise
+        RealStageParams p;
+        memset(&p, 0, sizeof(p));
+        p.n0 = rp.n0;
+        p.n1 = rp.n1;
+        p.n2 = rp.n2;
+        p.h1 = e.h1;
+        p.h2 = e.h2;
+        p.inv_dx2 = e.inv_dx2;
+        p.eta = e.eta;
+        p.inv_mu2 = e.inv_mu2;
+        p.inv_a2 = e.inv_a2;
+        p.ns_eff = rp.noise_scale;
+        p.nfac = 1.0;
+        p.step = step;
+        p.mul = kPass2Mul;
+        p.seed = rp.seed;
+        p.vkind = TIPT_VP_POLY;
+        p.c1 = rp.c1;
+        p.c2 = rp.c2;
+        p.c3 = rp.c3;
+        const uint32_t n12 = (uint32_t)rp.n1 * (uint32_t)rp.n2;
+        for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
+            const uint32_t s = (uint32_t)(ch.begin + t);
+            const uint32_t q = fdiv(s, rp.m2);
+            const uint32_t k = s - q * (uint32_t)rp.n2;
+            const uint32_t i = fdiv(q, rp.m1);
+            const uint32_t j = q - i * (uint32_t)rp.n1;
+            const int64_t o_ip = (i + 1 < (uint32_t)rp.n0) ? (int64_t)n12 : -(int64_t)(rp.n0 - 1) * n12;
+            const int64_t o_im = (i > 0) ? -(int64_t)n12 : (int64_t)(rp.n0 - 1) * n12;
+            const int64_t o_jp = (j + 1 < (uint32_t)rp.n1) ? rp.n2 : -(int64_t)(rp.n1 - 1) * rp.n2;
+            const int64_t o_jm = (j > 0) ? -(int64_t)rp.n2 : (int64_t)(rp.n1 - 1) * rp.n2;
+            const int64_t o_kp = (k + 1 < (uint32_t)rp.n2) ? 1 : -(int64_t)(rp.n2 - 1);
+            const int64_t o_km = (k > 0) ? -1 : (int64_t)(rp.n2 - 1);
+            const int64_t g = rp.offset + s;
+            const int64_t idx[7] = {g, g + o_ip, g + o_im, g + o_jp, g + o_jm, g + o_kp, g + o_km};
+            if constexpr (S == TIPT_F64) {
+                const double* phi = static_cast<const double*>(e.phi);
+                const double* pi = static_cast<const double*>(e.pi);
+                double ph[7], pv[7];
+#pragma unroll
+                for (int u = 0; u < 7; ++u) {
+                    ph[u] = __ldg(phi + idx[u]);
+                    pv[u] = __ldg(pi + idx[u]);
+                }
+                double a, b;
+                update_f64(p, nullptr, ph, pv, site_noise<double>(p, (uint64_t)s), a, b);
+                static_cast<double*>(e.phi_out)[g] = a;
+                static_cast<double*>(e.pi_out)[g] = b;
+            } else {
+                const float* phi = static_cast<const float*>(e.phi);
+                const float* pi = static_cast<const float*>(e.pi);
+                const int64_t N = e.n_total;
+                float hh[7], hl[7], vh[7], vl[7];
+#pragma unroll
+                for (int u = 0; u < 7; ++u) {
+                    hh[u] = __ldg(phi + idx[u]);
+                    hl[u] = __ldg(phi + N + idx[u]);
+                    vh[u] = __ldg(pi + idx[u]);
+                    vl[u] = __ldg(pi + N + idx[u]);
+                }
+                F32CIn<float> x;
+                stencil_sums(hh, hl, x.dh_phi, x.dl_phi);
+                stencil_sums(vh, vl, x.dh_pi, x.dl_pi);
+                x.phh = hh[0];
+                x.phl = hl[0];
+                x.pih = vh[0];
+                x.pil = vl[0];
+                float a, b, cc, d;
+                update_f32c<float>(p, nullptr, 0.0f, 0.0f, x, site_kick_f32c(p, (uint64_t)s), a, b,
+                                   cc, d);
+                float* po = static_cast<float*>(e.phi_out);
+                float* vo = static_cast<float*>(e.pi_out);
+                po[g] = a;
+                po[N + g] = b;
+                vo[g] = cc;
+                vo[N + g] = d;
+            }
+        }
+    }
+}
+
+// One block per replica: fraction of sites with phi > thr in a fixed order.
+template <int S>
+__global__ void __launch_bounds__(256) ensemble_observe_kernel(
+    const void* phi, int64_t n_total, const tipt_replica* reps, int32_t* active,
+    int32_t* n_active, double thr, double stop_frac, uint64_t step0,
+    const unsigned long long* ctr, long long offset, int64_t* first_step, double* frac_out) {
+    __shared__ double s_part[256];
+    const uint64_t step = step0 + (ctr ? *ctr + (unsigned long long)offset : 0ull);
+    const int r = blockIdx.x;
+    const tipt_replica rp = reps[r];
+    const int64_t n = (int64_t)rp.n0 * rp.n1 * rp.n2;
+    double cnt = 0.0;
+    for (int64_t s = threadIdx.x; s < n; s += blockDim.x) {
+        const int64_t g = rp.offset + s;
+        double v;
+        if constexpr (S == TIPT_F64) v = static_cast<const double*>(phi)[g];
+        else {
+            const float* f = static_cast<const float*>(phi);
+            v = (double)f[g] + (double)f[n_total + g];
+        }
+        cnt += v > thr ? 1.0 : 0.0;
+    }
+    s_part[threadIdx.x] = cnt;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s_part[threadIdx.x] += s_part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double frac = s_part[0] / (double)n;
+        frac_out[r] = frac;
+        if (active[r] && frac > stop_frac) {
+            first_step[r] = (int64_t)step;
+            active[r] = 0;
+            atomicSub(n_active, 1);
+        }
+    }
+}
+
+}  // namespace tipt
+
+using namespace tipt;
+
+extern "C" int tipt_ensemble_step(int storage, const void* phi, const void* pi, void* phi_out,
+                                  void* pi_out, int64_t n_total, const tipt_replica* replicas,
+                                  const tipt_chunk* chunks, int32_t n_chunks,
+                                  const int32_t* active, const tipt_step_params* sp,
+                                  const uint64_t* counter, int64_t offset, void* stream) {
+    int rc;
+    if (storage != TIPT_F64 && storage != TIPT_F32C)
+        return fail(TIPT_ERR_STORAGE, "the ensemble takes F64 or F32C storage");
+    if ((rc = check_state(storage, phi, pi, phi_out, pi_out, n_total, 1, 1))) return rc;
+    if (!replicas || !chunks || !active || !sp) return fail(TIPT_ERR_ARG, "NULL argument");
+    if (n_chunks < 0) return fail(TIPT_ERR_ARG, "n_chunks < 0");
+    if (n_chunks == 0) return TIPT_OK;
+    EnsParams e;
+    e.phi = phi;
+    e.pi = pi;
+    e.phi_out = phi_out;
+    e.pi_out = pi_out;
+    e.n_total = n_total;
+    e.reps = replicas;
+    e.chunks = chunks;
+    e.n_chunks = n_chunks;
+    e.active = active;
+    e.h1 = 0.5 * sp->dt;
+    e.h2 = sp->dt;
+    e.inv_dx2 = 1.0 / (sp->dx * sp->dx);
+    e.eta = sp->eta_eff;
+    e.inv_mu2 = 1.0 / (sp->mu * sp->mu);
+    e.inv_a2 = sp->inv_a2;
+    e.step = sp->noise_step;
+    e.ctr = reinterpret_cast<const unsigned long long*>(counter);
+    e.offset = offset;
+    int grid = num_sms() * 8;
+    if (grid > n_chunks) grid = n_chunks;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (storage == TIPT_F64) ensemble_stage_kernel<TIPT_F64><<<grid, 256, 0, st>>>(e);
+    else ensemble_stage_kernel<TIPT_F32C><<<grid, 256, 0, st>>>(e);
+    cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? TIPT_OK : fail_cuda(err, "ensemble_stage launch");
+}
+
+extern "C" int tipt_ensemble_observe(int storage, const void* phi, int64_t n_total,
+                                     const tipt_replica* replicas, int32_t n_replicas,
+                                     int32_t* active, int32_t* n_active, double thr,
+                                     double stop_frac, uint64_t step, const uint64_t* counter,
+                                     int64_t offset, int64_t* first_step, double* frac_out,
+                                     void* stream) {
+    if (storage != TIPT_F64 && storage != TIPT_F32C)
+        return fail(TIPT_ERR_STORAGE, "the ensemble takes F64 or F32C storage");
+    if (!phi || !replicas || !active || !n_active || !first_step || !frac_out)
+        return fail(TIPT_ERR_ARG, "NULL argument");
+    if (n_replicas <= 0) return TIPT_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (storage == TIPT_F64)
+        ensemble_observe_kernel<TIPT_F64><<<n_replicas, 256, 0, st>>>(
+            phi, n_total, replicas, active, n_active, thr, stop_frac, step,
+            reinterpret_cast<const unsigned long long*>(counter), offset, first_step, frac_out);
+    else
+        ensemble_observe_kernel<TIPT_F32C><<<n_replicas, 256, 0, st>>>(
+            phi, n_total, replicas, active, n_active, thr, stop_frac, step,
+            reinterpret_cast<const unsigned long long*>(counter), offset, first_step, frac_out);
+    cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? TIPT_OK : fail_cuda(err, "ensemble_observe launch");
+}

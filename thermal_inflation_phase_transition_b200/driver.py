@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from ._common import ptr, step_params, stream_handle, table_source
+from ._common import poly_source, ptr, step_params, stream_handle, table_source
 from .observables import OBS_INDEX, OBS_NAMES, workspace_bytes
 from .real_field import to_f32c
 
@@ -94,12 +94,14 @@ class Simulation:
     """A real scalar field on a periodic lattice, stepped by graph-captured chunks.
 
     storage: "f64", "f32" (the reference's float32 mode) or "f32c" (compensated).
+    table: Table1D / Table2D, or None with vpoly = (c1, c2, c3) for the polynomial
+    V'(phi) = c1 phi + c2 phi^2 + c3 phi^3.
     phi0/pi0: initial fields (numpy, FP64); default phi ~ N(0, init_sigma^2), pi = 0.
     """
 
     def __init__(self, shape, *, storage="f32c", dt=0.05, dx=1.0, eta=1.0, mu=1.0, inv_a2=1.0,
                  table, schedule, seed=0, phi0=None, pi0=None, init_sigma=0.01, init_seed=0,
-                 obs_threshold=1.0, graph_steps=50, device="cuda"):
+                 obs_threshold=1.0, graph_steps=50, vpoly=None, device="cuda"):
         self.shape = tuple(int(x) for x in shape)
         self.storage = storage
         self.dev = torch.device(device)
@@ -111,11 +113,17 @@ class Simulation:
         if self.schedule.ndim != 2 or self.schedule.shape[1] != 2:
             raise ValueError("schedule must be (n_steps, 2): (T, ns) per step")
         self._sched = torch.from_numpy(self.schedule).to(self.dev)
-        self._table = torch.from_numpy(np.asarray(table.values)).to(self.dev)
-        if isinstance(table, Table2D):
+        if table is None:
+            if vpoly is None:
+                raise ValueError("give a table or vpoly")
+            self._table = None
+            self._vs = poly_source(*vpoly)
+        elif isinstance(table, Table2D):
+            self._table = torch.from_numpy(np.asarray(table.values)).to(self.dev)
             self._vs = table_source(self._table, table.tmin, table.dinv, table.values.shape[1],
                                     float(self.schedule[0, 0]), table.T_min, table.T_dinv)
         else:
+            self._table = torch.from_numpy(np.asarray(table.values)).to(self.dev)
             self._vs = table_source(self._table, table.tmin, table.dinv, table.values.shape[0])
         if phi0 is None:
             phi0 = np.random.default_rng(init_seed).normal(0.0, init_sigma, self.shape)
@@ -155,8 +163,9 @@ class Simulation:
     def _st(self):
         return {"f64": L.TIPT_F64, "f32": L.TIPT_F32, "f32c": L.TIPT_F32C}[self.storage]
 
-    def _launch_chunk(self, K, obs):
-        """Enqueue K steps (+ observables into obs[q]) and the counter advance."""
+    def _launch_chunk(self, K, obs, observe_last=False):
+        """Enqueue K steps (+ observables into obs[q], or only after the last step into
+        obs[0] with observe_last) and the counter advance."""
         lib = L.lib()
         st = stream_handle()
         nx, ny, nz = self.shape
@@ -167,11 +176,12 @@ class Simulation:
                 nx, ny, nz, self._sp, self._vs, ptr(self._sched), self.schedule.shape[0],
                 ptr(self._counter), q, st)
             L.check(rc, "tipt_rk2_step_table_sched")
-            if obs is not None:
+            if obs is not None and (not observe_last or q == K - 1):
                 rc = lib.tipt_observables(self._st(), ptr(self.phi[b]), ptr(self.pi[b]), nx, ny,
                                           nz, float(self.dx), float(self.inv_a2), 0.0, 0.0,
-                                          float(self.mu), float(self.thr), ptr(obs[q]),
-                                          ptr(self._ws), self._ws.numel() * 8, st)
+                                          float(self.mu), float(self.thr),
+                                          ptr(obs[0 if observe_last else q]), ptr(self._ws),
+                                          self._ws.numel() * 8, st)
                 L.check(rc, "tipt_observables")
         L.check(lib.tipt_counter_add(ptr(self._counter), K, st), "tipt_counter_add")
 
@@ -218,6 +228,37 @@ class Simulation:
         if not observe:
             return None
         return torch.cat(out).cpu().numpy()
+
+    def run_until(self, stop_frac, max_steps, *, check_every=None):
+        """Step in graph-captured chunks of check_every steps; after each chunk read the
+        fraction of sites with phi > obs_threshold on the host and stop once it exceeds
+        stop_frac.  Returns the 0-based index of that chunk's last step, or -1."""
+        K = self.graph_steps if check_every is None else max(2, check_every & ~1)
+        if K != self.graph_steps:
+            self.graph_steps = K
+            self._graphs = {}
+        k_frac = OBS_INDEX["frac_above"]
+        while self.steps_done + K <= max_steps:
+            obs = self._run_chunk_observe_last(K)
+            self.steps_done += K
+            if float(obs[k_frac]) > stop_frac:
+                return self.steps_done - 1
+        return -1
+
+    def _run_chunk_observe_last(self, K):
+        key = ("last", K, self.phi[0].data_ptr())
+        if key not in self._graphs:
+            obs = torch.zeros((1, 10), dtype=torch.float64, device=self.dev)
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                self._launch_chunk(K, obs, observe_last=True)
+            torch.cuda.current_stream().wait_stream(s)
+            self._graphs[key] = (g, obs)
+        g, obs = self._graphs[key]
+        g.replay()
+        return obs[0].cpu().numpy()
 
     def synchronize(self):
         torch.cuda.synchronize(self.dev)

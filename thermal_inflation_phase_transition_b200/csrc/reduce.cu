@@ -14,7 +14,7 @@ namespace tipt {
 
 constexpr int kObs = 10;          // outputs
 constexpr int kRedThreads = 256;
-constexpr int kMaxRedBlocks = 1024;
+constexpr int kMaxRedBlocks = 1184;
 
 struct ObsAcc {
     double kin, grad, pot, s1, s2, sq, above, nonfinite, mn, mx;
@@ -91,37 +91,55 @@ struct ObsParams {
     double* out;       // [kObs]
 };
 
+// Sites are walked row by row (a row = the n2 sites of fixed (i, j)): warp w
+// of block b takes rows w + 8 b, w + 8 b + 8 G, ... and its lanes stride along
+// the row, so loads are coalesced and the only divisions are one 32-bit
+// division per row.  The assignment depends on the lattice shape alone.
+template <int S>
+__device__ __forceinline__ void obs_site(const ObsParams& p, ObsAcc& a, int64_t s, int64_t ox,
+                                         int64_t oy, int64_t oz, int64_t N) {
+    const double ph = load_val<S>(p.phi, s, N);
+    const double pv = p.pi ? load_val<S>(p.pi, s, N) : 0.0;
+    // forward differences, R:2303-2308
+    const double fx = load_val<S>(p.phi, s + ox, N) - ph;
+    const double fy = load_val<S>(p.phi, s + oy, N) - ph;
+    const double fz = load_val<S>(p.phi, s + oz, N) - ph;
+    a.kin += 0.5 * pv * pv;
+    a.grad += 0.5 * p.inv_a2 * (fx * fx + fy * fy + fz * fz) * p.inv_dx2;
+    const double ph2 = ph * ph;
+    a.pot += (0.25 * p.lam * ph2 * ph2 - 0.5 * p.m2 * ph2) * p.inv_mu2;
+    a.s1 += ph;
+    a.s2 += ph2;
+    a.sq += pv * pv;
+    a.above += ph > p.thr ? 1.0 : 0.0;
+    a.nonfinite += (isfinite(ph) && isfinite(pv)) ? 0.0 : 1.0;
+    a.mn = fmin(a.mn, ph);
+    a.mx = fmax(a.mx, ph);
+}
+
 template <int S>
 __global__ void __launch_bounds__(kRedThreads) obs_partial_kernel(ObsParams p) {
     const int64_t n12 = (int64_t)p.n1 * p.n2;
     const int64_t N = (int64_t)p.n0 * n12;
-    const int64_t per = (N + gridDim.x - 1) / gridDim.x;
-    const int64_t lo = per * blockIdx.x;
-    const int64_t hi = lo + per < N ? lo + per : N;
+    const int64_t rows = (int64_t)p.n0 * p.n1;
+    const int lane = threadIdx.x & 31;
+    const int wpb = kRedThreads / 32;
     ObsAcc a;
     acc_init(a);
-    for (int64_t s = lo + threadIdx.x; s < hi; s += blockDim.x) {
-        const int k = (int)(s % p.n2);
-        const int64_t r = s / p.n2;
-        const int j = (int)(r % p.n1);
-        const int i = (int)(r / p.n1);
-        const double ph = load_val<S>(p.phi, s, N);
-        const double pv = p.pi ? load_val<S>(p.pi, s, N) : 0.0;
-        // forward differences, R:2303-2308
-        const double fx = load_val<S>(p.phi, s + ((i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12), N) - ph;
-        const double fy = load_val<S>(p.phi, s + ((j + 1 < p.n1) ? (int64_t)p.n2 : -(int64_t)(p.n1 - 1) * p.n2), N) - ph;
-        const double fz = load_val<S>(p.phi, s + ((k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1)), N) - ph;
-        a.kin += 0.5 * pv * pv;
-        a.grad += 0.5 * p.inv_a2 * (fx * fx + fy * fy + fz * fz) * p.inv_dx2;
-        const double ph2 = ph * ph;
-        a.pot += (0.25 * p.lam * ph2 * ph2 - 0.5 * p.m2 * ph2) * p.inv_mu2;
-        a.s1 += ph;
-        a.s2 += ph2;
-        a.sq += pv * pv;
-        a.above += ph > p.thr ? 1.0 : 0.0;
-        a.nonfinite += (isfinite(ph) && isfinite(pv)) ? 0.0 : 1.0;
-        a.mn = fmin(a.mn, ph);
-        a.mx = fmax(a.mx, ph);
+    for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < rows;
+         row += (int64_t)gridDim.x * wpb) {
+        const int64_t i = row / p.n1;
+        const int64_t j = row - i * p.n1;
+        const int64_t ox = (i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12;
+        const int64_t oy = (j + 1 < p.n1) ? (int64_t)p.n2 : -(int64_t)(p.n1 - 1) * p.n2;
+        const int64_t base = row * p.n2;
+        int k = lane;
+        // two sites per lane per pass keep more loads in flight
+        for (; k + 32 < p.n2; k += 64) {
+            obs_site<S>(p, a, base + k, ox, oy, 1, N);
+            obs_site<S>(p, a, base + k + 32, ox, oy, (k + 33 < p.n2) ? 1 : -(int64_t)(p.n2 - 1), N);
+        }
+        if (k < p.n2) obs_site<S>(p, a, base + k, ox, oy, (k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1), N);
     }
     a = block_reduce(a);
     if (threadIdx.x == 0) {
@@ -173,14 +191,15 @@ __global__ void __launch_bounds__(kRedThreads) obs_final_kernel(ObsParams p, int
     }
 }
 
-int obs_blocks(int64_t N) {
-    int64_t g = (N + 8191) / 8192;
+// Rows / 8 warps per block, at most kMaxRedBlocks (8 x 148): a function of the shape only.
+int obs_blocks(int64_t rows) {
+    int64_t g = (rows + 7) / 8;
     if (g > kMaxRedBlocks) g = kMaxRedBlocks;
     if (g < 1) g = 1;
     return (int)g;
 }
 
-int64_t obs_workspace_bytes(int64_t N) { return (int64_t)obs_blocks(N) * kObs * 8; }
+int64_t obs_workspace_bytes(int64_t rows) { return (int64_t)obs_blocks(rows) * kObs * 8; }
 
 int launch_observables(int storage, const void* phi, const void* pi, int n0, int n1, int n2,
                        double dx, double inv_a2, double lam, double mphi, double mu, double thr,
@@ -200,7 +219,7 @@ int launch_observables(int storage, const void* phi, const void* pi, int n0, int
     p.partials = partials;
     p.out = out;
     const int64_t N = (int64_t)n0 * n1 * n2;
-    const int G = obs_blocks(N);
+    const int G = obs_blocks((int64_t)n0 * n1);
     switch (storage) {
         case TIPT_F64: obs_partial_kernel<TIPT_F64><<<G, kRedThreads, 0, st>>>(p); break;
         case TIPT_F32: obs_partial_kernel<TIPT_F32><<<G, kRedThreads, 0, st>>>(p); break;
@@ -219,7 +238,7 @@ using namespace tipt;
 
 extern "C" int64_t tipt_observables_workspace_size(int64_t nx, int64_t ny, int64_t nz) {
     if (nx < 1 || ny < 1 || nz < 1) return 0;
-    return obs_workspace_bytes(nx * ny * nz);
+    return obs_workspace_bytes(nz == 1 ? nx : nx * ny);  // rows of the walk
 }
 
 extern "C" int tipt_observables(int storage, const void* phi, const void* pi, int64_t nx,
@@ -233,7 +252,13 @@ extern "C" int tipt_observables(int storage, const void* phi, const void* pi, in
         (rc = check_ptr(workspace, 8, "workspace")))
         return rc;
     if (pi && (rc = check_ptr(pi, eb, "pi"))) return rc;
-    const int64_t need = obs_workspace_bytes(nx * ny * nz);
+    // (nx, ny, 1) is the same C-order memory as (1, nx, ny): walk rows of length ny
+    if (nz == 1) {
+        nz = ny;
+        ny = nx;
+        nx = 1;
+    }
+    const int64_t need = obs_workspace_bytes(nx * ny);
     if (workspace_bytes < need)
         return fail(TIPT_ERR_ARG, "workspace of %lld bytes is smaller than the %lld needed",
                     (long long)workspace_bytes, (long long)need);

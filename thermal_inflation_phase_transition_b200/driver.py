@@ -245,7 +245,11 @@ class Simulation:
                 return self.steps_done - 1
         return -1
 
-    def _run_chunk_observe_last(self, K):
+    def prepare_graphs(self, K):
+        """Capture (without running) the check-interval graph run_until replays."""
+        self._last_graph(K)
+
+    def _last_graph(self, K):
         key = ("last", K, self.phi[0].data_ptr())
         if key not in self._graphs:
             obs = torch.zeros((1, 10), dtype=torch.float64, device=self.dev)
@@ -256,7 +260,10 @@ class Simulation:
                 self._launch_chunk(K, obs, observe_last=True)
             torch.cuda.current_stream().wait_stream(s)
             self._graphs[key] = (g, obs)
-        g, obs = self._graphs[key]
+        return self._graphs[key]
+
+    def _run_chunk_observe_last(self, K):
+        g, obs = self._last_graph(K)
         g.replay()
         return obs[0].cpu().numpy()
 

@@ -220,15 +220,22 @@ def gamma_mle(first_steps, max_steps, volume, dt):
 
 def plain_first_passage(specs, max_steps, *, storage="f32c", dt=0.05, dx=1.0, eta=1.0,
                         thr=1.0, stop_frac=0.5, check_every=10, init_sigma=0.01, init_seed=0,
-                        device="cuda"):
+                        device="cuda", timing=None):
     """The per-replica baseline: each replica alone through the single-lattice driver
     (marching kernel where the shape allows, graph-captured check intervals, a host poll
     per check).  Same arithmetic, noise and initial state as the batched ensemble, so
-    the first-passage steps agree exactly.  Returns first-passage steps (-1 = none)."""
+    the first-passage steps agree exactly.  Returns first-passage steps (-1 = none).
+    ``timing`` (a dict) receives the seconds spent in setup (state upload, first graph
+    capture) and in stepping, separately."""
+    import time
     from .driver import Simulation, constant_temperature
     K = max(2, check_every & ~1)
     out = []
+    if timing is not None:
+        timing.setdefault("setup_s", 0.0)
+        timing.setdefault("run_s", 0.0)
     for sp in specs:
+        t0 = time.perf_counter()
         shape = _canonical(sp.shape)
         n = shape[0] * shape[1] * shape[2]
         phi0 = replica_initial_phi(n, sp.seed, init_seed, init_sigma, device)
@@ -237,5 +244,13 @@ def plain_first_passage(specs, max_steps, *, storage="f32c", dt=0.05, dx=1.0, et
                          schedule=constant_temperature(sp.T, 1, dt=dt, eta=eta, dx_phys=dx),
                          seed=sp.seed, phi0=phi0.reshape(shape).cpu().numpy(),
                          obs_threshold=thr, graph_steps=K, device=device)
+        if timing is not None:
+            sim.prepare_graphs(K)
+            torch.cuda.synchronize(device)
+            t1 = time.perf_counter()
+            timing["setup_s"] += t1 - t0
         out.append(sim.run_until(stop_frac, max_steps, check_every=K))
+        if timing is not None:
+            torch.cuda.synchronize(device)
+            timing["run_s"] += time.perf_counter() - t1
     return np.array(out)

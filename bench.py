@@ -241,7 +241,7 @@ def main():
     ap.add_argument("--storage", choices=["f32c", "f64", "f32"], default="f32c")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["lattice", "ensemble"], default="lattice",
+    ap.add_argument("--workload", choices=["lattice", "ensemble", "surrogate"], default="lattice",
                     help="lattice: the 512^3 site-update headline; ensemble: Gamma estimates "
                          "per GPU-hour of the batched replica engine vs one-at-a-time launches")
     ap.add_argument("--ens-steps", type=int, default=2000)
@@ -251,6 +251,9 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.workload == "ensemble" and args.impl == "tipt":
         run_ensemble_bench(args)
+        return
+    if args.workload == "surrogate" and args.impl == "tipt":
+        run_surrogate_bench(args)
         return
 
     if args.impl == "reference":
@@ -507,6 +510,34 @@ def run_ensemble_bench(args):
         "plain_by_class": by_class,
         "speedup_vs_plain_stepping_only": t_plain_run / t_batched,
         "plain_events_checked_equal": f"{plain_checked}/{sum(min(len(v), args.ens_plain) for v in classes.values())}",
+    }
+    print(json.dumps(line, default=lambda o: o.item() if hasattr(o, "item") else str(o)),
+          flush=True)
+
+
+def run_surrogate_bench(args):
+    """Surrogate-steered scan over T/T0 in [0.97, 1.02], E in [0.03, 0.07], D in [0.05, 0.15],
+    lam in [0.05, 0.2]: 2x10^4 training replicas (128^2 2-D, 48^3, 64^3) from the ensemble
+    engine, training by the library's BF16 kernels, 64 lam* proposals on a 4x4x4 (T, E, D)
+    grid for 64^3, each re-verified by a plain 256-replica ensemble; cost against a dense
+    plain scan of 16 lam values per point."""
+    import torch
+    from thermal_inflation_phase_transition_b200 import scan as SC
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    rep = SC.steered_scan(n_train=20000, n_points=64, n_verify=256, fit_iters=4000, seed=5,
+                          log=lambda m: print(m, file=sys.stderr, flush=True))
+    wall = time.perf_counter() - t0
+    rep.pop("net")
+    v = rep["verify"]
+    line = {
+        "metric": "surrogate Gamma error vs plain 256-replica ensembles; GPU-hours saved vs dense scan",
+        "value": v["median_abs_rel_err"], "unit": "median |Gamma_sur/Gamma_plain - 1|",
+        "n_gpus": 1, "higher_is_better": False, "vs_baseline": None, "dtype": "bf16/fp32",
+        "data": "synthetic",
+        "config": {"workload": "config-5 surrogate-steered scan", "train_replicas": 20000,
+                   "scan_points": 64, "verify_replicas": 256, "scan_lattice": [64, 64, 64]},
+        "report": rep, "wall_s": wall,
     }
     print(json.dumps(line, default=lambda o: o.item() if hasattr(o, "item") else str(o)),
           flush=True)

@@ -230,12 +230,14 @@ int tipt_ensemble_step(int storage, const void* phi, const void* pi, void* phi_o
                        const uint64_t* counter, int64_t offset, void* stream);
 
 /* Per replica (one block each, fixed order): frac_out[r] = fraction of sites
- * with phi > thr.  An active replica whose fraction exceeds stop_frac gets
- * first_step[r] = step (+ *counter + offset), active[r] = 0, and *n_active is
- * decremented. */
+ * with phi > thr.  An active replica whose fraction exceeds stop_frac for the
+ * first time gets first_step[r] = step (+ *counter + offset; first_step starts
+ * at -1); once its fraction exceeds retire_frac (>= stop_frac) it is retired:
+ * active[r] = 0 and *n_active is decremented. */
 int tipt_ensemble_observe(int storage, const void* phi, int64_t n_total,
                           const tipt_replica* replicas, int32_t n_replicas, int32_t* active,
-                          int32_t* n_active, double thr, double stop_frac, uint64_t step,
+                          int32_t* n_active, double thr, double stop_frac, double retire_frac,
+                          uint64_t step,
                           const uint64_t* counter, int64_t offset, int64_t* first_step,
                           double* frac_out, void* stream);
 
@@ -253,6 +255,47 @@ int tipt_observables(int storage, const void* phi, const void* pi, int64_t nx, i
                      int64_t nz, double dx, double inv_a2, double lam, double mphi, double mu,
                      double thr, double* out, void* workspace, int64_t workspace_bytes,
                      void* stream);
+
+/* ------------------------------------------------------------ surrogate network
+ * No reference counterpart (the reference estimates nucleation only by running
+ * lattices).  A 6 -> 128 -> 128 -> 128 -> 17 SiLU network maps normalised
+ * (T/T0, E, D, lam, log volume, dimension) to the log nucleation rate (in
+ * exposure units) and the logits of the converted fraction at 16 fixed times.
+ * Parameters: one FP32 vector of tipt_mlp_param_count() values, per layer
+ * W[in][out] then b[out] with layer widths 16, 128, 128, 128, 32 (inputs 6..15
+ * and outputs 17..31 are padding and stay zero).  Products use BF16 operands
+ * with FP32 accumulation on the tensor cores; results are deterministic. */
+int64_t tipt_mlp_param_count(void);
+
+/* Kernel selection for the network: 0 automatic (tcgen05 tensor-core kernels
+ * with tensor-memory accumulators), 1 the mma.sync kernels, 2 tcgen05.  The two
+ * paths differ only in FP32 accumulation order. */
+int tipt_mlp_set_policy(int policy);
+
+/* Bytes of device workspace tipt_mlp_grad needs for `rows` rows. */
+int64_t tipt_mlp_workspace_size(int64_t rows);
+
+/* y[rows][17] = network(x[rows][6]) (FP32, row-major). */
+int tipt_mlp_forward(const float* params, const float* x, int64_t rows, float* y, void* stream);
+
+/* Gradient of (1/norm) sum_rows loss(row) with respect to params into grad (FP32,
+ * parameter layout); per-row losses into loss_rows when not NULL.  tgt[rows][20]
+ * per row: event (1 if the replica's first passage happened), exposure (volume x
+ * time to first passage or to censoring, in the units of the rate output),
+ * w_gamma, w_curve, then the 16 converted fractions in [0, 1].  loss(row) =
+ * w_gamma (exp(l) exposure - event l) + w_curve/16 sum_k (softplus(o_k) - f_k o_k),
+ * l = y[0] clamped to [-40, 40] inside the exponential, o_k = y[k]. */
+int tipt_mlp_grad(const float* params, const float* x, const float* tgt, int64_t rows,
+                  float norm, float* grad, float* loss_rows, void* workspace,
+                  int64_t workspace_bytes, void* stream);
+
+/* One Adam step over all parameters (bias-corrected with step t = *counter +
+ * offset + 1, or offset + 1 without a counter; decoupled weight decay).  The
+ * learning rate is lr, times lr_schedule[min(t, schedule_len) - 1] when a
+ * device schedule is given (graph-captured training loops). */
+int tipt_mlp_adam(float* params, const float* grad, float* m, float* v, const uint64_t* counter,
+                  int64_t offset, float lr, const float* lr_schedule, int64_t schedule_len,
+                  float beta1, float beta2, float eps, float weight_decay, void* stream);
 
 /* ------------------------------------------------------------ control */
 

@@ -71,8 +71,8 @@ _SIGS = {
     "tipt_counter_add": [_p, _i64, _p],
     "tipt_ensemble_step": [_i, _p, _p, _p, _p, _i64, _p, _p, C.c_int32, _p,
                            C.POINTER(StepParams), _p, _i64, _p],
-    "tipt_ensemble_observe": [_i, _p, _i64, _p, C.c_int32, _p, _p, _d, _d, _u64, _p, _i64, _p,
-                              _p, _p],
+    "tipt_ensemble_observe": [_i, _p, _i64, _p, C.c_int32, _p, _p, _d, _d, _d, _u64, _p, _i64,
+                              _p, _p, _p],
     "tipt_rk2_fused_table_noalloc": [_i, _p, _p, _p, _p, _i64, _i64, _i64,
                                      C.POINTER(StepParams), C.POINTER(VSource),
                                      C.POINTER(VSource), _p, _p],
@@ -83,12 +83,20 @@ _SIGS = {
     "tipt_observables_workspace_size": [_i64, _i64, _i64],
     "tipt_observables": [_i, _p, _p, _i64, _i64, _i64, _d, _d, _d, _d, _d, _d, _p, _p, _i64,
                          _p],
+    "tipt_mlp_param_count": [],
+    "tipt_mlp_set_policy": [_i],
+    "tipt_mlp_workspace_size": [_i64],
+    "tipt_mlp_forward": [_p, _p, _i64, _p, _p],
+    "tipt_mlp_grad": [_p, _p, _p, _i64, C.c_float, _p, _p, _p, _i64, _p],
+    "tipt_mlp_adam": [_p, _p, _p, _p, _p, _i64, C.c_float, _p, _i64, C.c_float, C.c_float,
+                      C.c_float, C.c_float, _p],
     "tipt_set_kernel_policy": [_i],
     "tipt_set_march_tiles": [_i, _i, _i],
     "tipt_device_status": [C.POINTER(C.c_int), _i],
 }
 _RESTYPE = {"tipt_version": C.c_char_p, "tipt_status_string": C.c_char_p,
-            "tipt_last_error": C.c_char_p, "tipt_observables_workspace_size": C.c_int64}
+            "tipt_last_error": C.c_char_p, "tipt_observables_workspace_size": C.c_int64,
+            "tipt_mlp_param_count": C.c_int64, "tipt_mlp_workspace_size": C.c_int64}
 
 _lib = None
 

@@ -1,0 +1,165 @@
+"""Tile-shape autotuner of the marching stage kernel, with a persisted JSON cache.
+
+The marching kernel's tile is (rows per tile, planes per work item, ring
+stages).  The built-in heuristic scores candidates by occupancy and halo share;
+``tune`` instead times every admissible candidate on the device (CUDA events,
+inputs larger than L2 where the lattice is) and keeps the fastest.  Results are
+cached per (GPU name, storage, lattice shape, V' table size) in a JSON file
+(``$TIPT_AUTOTUNE_CACHE``, else ``~/.cache/tipt_b200/autotune.json``);
+``apply`` installs a cached shape, or the heuristic when there is none.
+
+No reference counterpart: the reference's only knob is the CPU tile size
+(R:1969-1970).
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+
+import torch
+
+from . import _lib as L
+from . import real_field as RF
+from ._common import table_source
+
+__all__ = ["cache_path", "cache_key", "candidates", "tune", "apply", "load_cache"]
+
+STAGES = (3, 4, 5)
+PLANES = (8, 16, 32, 64, 128, 256, 512)
+
+
+def cache_path() -> str:
+    p = os.environ.get("TIPT_AUTOTUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "tipt_b200", "autotune.json")
+
+
+def cache_key(shape, storage, table_points, device=None) -> str:
+    dev = torch.device(device or "cuda")
+    name = torch.cuda.get_device_name(dev).replace(" ", "_")
+    cc = "%d.%d" % torch.cuda.get_device_capability(dev)
+    nx, ny, nz = shape
+    return f"{name}|sm{cc}|{storage}|{nx}x{ny}x{nz}|table{int(table_points)}"
+
+
+def load_cache() -> dict:
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _save_cache(c: dict) -> None:
+    p = cache_path()
+    os.makedirs(os.path.dirname(p), exist_ok=True)
+    tmp = p + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(c, f, indent=1, sort_keys=True)
+    os.replace(tmp, p)
+
+
+def candidates(shape):
+    """(rows, planes, stages) the kernel may accept for this lattice (the kernel still
+    rejects those that do not fit shared memory)."""
+    nx, ny, nz = shape
+    n0, n1, n2 = (1, nx, ny) if nz == 1 else (nx, ny, nz)
+    tpr = n2 // 4
+    out = []
+    for tj in range(1, 65):
+        if n1 % tj or (tj * tpr) % 32 or tj * tpr > 512:
+            continue
+        for ci in PLANES:
+            if ci > n0 and ci != PLANES[0]:
+                continue
+            for st in STAGES:
+                out.append((tj, ci, st))
+    return out
+
+
+def _state(shape, storage, device):
+    nx, ny, nz = shape
+    g = torch.Generator(device=device)
+    g.manual_seed(1)
+    if storage == "f32c":
+        phi = torch.zeros((2, nx, ny, nz), dtype=torch.float32, device=device)
+        phi[0] = 0.01 * torch.randn((nx, ny, nz), generator=g, device=device)
+        pi = torch.zeros_like(phi)
+    else:
+        phi = 0.01 * torch.randn((nx, ny, nz), dtype=torch.float64, generator=g, device=device)
+        pi = torch.zeros_like(phi)
+    return [phi, pi, torch.empty_like(phi), torch.empty_like(pi)]
+
+
+def _time(state, table, steps, warmup):
+    """Mean ms per stage launch (ping-pong between the two state pairs)."""
+    bufs = ((state[0], state[1]), (state[2], state[3]))
+    vs = table_source(table, 0.0, (table.numel() - 1) / 3.0, table.numel())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for n in range(warmup + steps):
+        if n == warmup:
+            torch.cuda.synchronize()
+            e0.record()
+        (phi, pi), (po, qo) = bufs[n % 2], bufs[(n + 1) % 2]
+        RF.rk2_step_table_into(phi, pi, po, qo, 0.05, 1.0, 1.0, 1.0, 1.0, vs, noise_scale=0.3,
+                               noise_step=n, seed=1)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def tune(shape, storage="f32c", *, table_points=4096, steps=10, warmup=3, persist=True,
+         device="cuda", log=None):
+    """Time every admissible tile shape; returns {"best": [rows, planes, stages], "ms": t,
+    "default_ms": t0, "tried": n} and stores it in the cache."""
+    if storage not in ("f32c", "f64"):
+        raise ValueError("the marching kernel runs F32C and F64 storage")
+    dev = torch.device(device)
+    state = _state(shape, storage, dev)
+    table = torch.linspace(-0.1, 0.1, table_points, dtype=torch.float64, device=dev)
+    L.set_kernel_policy(2)
+    try:
+        L.set_march_tiles(0, 0, 0)
+        default_ms = _time(state, table, steps, warmup)
+        best, best_ms, tried = None, float("inf"), 0
+        t_start = time.perf_counter()
+        for c in candidates(shape):
+            L.set_march_tiles(*c)
+            try:
+                ms = _time(state, table, steps, warmup)
+            except L.TiptError:
+                continue
+            tried += 1
+            if log:
+                log(f"  rows={c[0]} planes={c[1]} stages={c[2]}: {ms:.4f} ms")
+            if ms < best_ms:
+                best, best_ms = c, ms
+    finally:
+        L.set_march_tiles(0, 0, 0)
+        L.set_kernel_policy(0)
+    if best is None:
+        raise RuntimeError(f"no marching tile shape accepted for {shape} {storage}")
+    res = {"best": list(best), "ms": best_ms, "default_ms": default_ms, "tried": tried,
+           "seconds": time.perf_counter() - t_start}
+    if persist:
+        c = load_cache()
+        c[cache_key(shape, storage, table_points, dev)] = res
+        _save_cache(c)
+    return res
+
+
+def apply(shape, storage="f32c", *, table_points=4096, tune_if_missing=False, device="cuda"):
+    """Install the cached tile shape for this workload (tuning first if asked and absent).
+    Returns the installed (rows, planes, stages), or None for the built-in heuristic."""
+    key = cache_key(shape, storage, table_points, device)
+    entry = load_cache().get(key)
+    if entry is None and tune_if_missing:
+        entry = tune(shape, storage, table_points=table_points, device=device)
+    if entry is None or entry["ms"] >= entry.get("default_ms", float("inf")):
+        L.set_march_tiles(0, 0, 0)
+        return None
+    L.set_march_tiles(*entry["best"])
+    return tuple(entry["best"])

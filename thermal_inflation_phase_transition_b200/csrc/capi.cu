@@ -117,11 +117,20 @@ int check_state(int storage, const void* phi, const void* pi, void* phi_out,
                        void* pi_out, int64_t nx, int64_t ny, int64_t nz) {
     int rc;
     if ((rc = check_storage(storage)) || (rc = check_dims(nx, ny, nz))) return rc;
+    return check_state_sites(storage, phi, pi, phi_out, pi_out, nx * ny * nz);
+}
+
+int check_state_sites(int storage, const void* phi, const void* pi, void* phi_out,
+                      void* pi_out, int64_t sites) {
+    int rc;
+    if ((rc = check_storage(storage))) return rc;
+    if (sites < 1 || (double)sites > 9.0e15)
+        return fail(TIPT_ERR_ARG, "site count %lld out of range", (long long)sites);
     const int eb = elem_bytes(storage), ea = elem_align(storage);
     if ((rc = check_ptr(phi, ea, "phi")) || (rc = check_ptr(pi, ea, "pi")) ||
         (rc = check_ptr(phi_out, ea, "phi_out")) || (rc = check_ptr(pi_out, ea, "pi_out")))
         return rc;
-    const int64_t bytes = nx * ny * nz * eb;
+    const int64_t bytes = sites * eb;
     const void* ins[2] = {phi, pi};
     const void* outs[2] = {phi_out, pi_out};
     for (auto o : outs)

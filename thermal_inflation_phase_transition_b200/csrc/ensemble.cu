@@ -15,8 +15,9 @@
 //
 // tipt_ensemble_observe reduces, per replica and in a fixed order, the
 // fraction of sites with phi > thr; the first time it exceeds the stop
-// fraction the step is recorded as the replica's first-passage step and the
-// replica is retired (its chunks are skipped from then on).
+// fraction the step is recorded as the replica's first-passage step, and once
+// it exceeds the retire fraction (>= the stop fraction) the replica is retired
+// (its chunks are skipped from then on).
 #include <cstring>
 
 #include "rk2_real.cuh"
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
 template <int S>
 __global__ void __launch_bounds__(256) ensemble_observe_kernel(
     const void* phi, int64_t n_total, const tipt_replica* reps, int32_t* active,
-    int32_t* n_active, double thr, double stop_frac, uint64_t step0,
+    int32_t* n_active, double thr, double stop_frac, double retire_frac, uint64_t step0,
     const unsigned long long* ctr, long long offset, int64_t* first_step, double* frac_out) {
     __shared__ double s_part[256];
     const uint64_t step = step0 + (ctr ? *ctr + (unsigned long long)offset : 0ull);
@@ -164,10 +165,12 @@ __global__ void __launch_bounds__(256) ensemble_observe_kernel(
     if (threadIdx.x == 0) {
         const double frac = s_part[0] / (double)n;
         frac_out[r] = frac;
-        if (active[r] && frac > stop_frac) {
-            first_step[r] = (int64_t)step;
-            active[r] = 0;
-            atomicSub(n_active, 1);
+        if (active[r]) {
+            if (frac > stop_frac && first_step[r] < 0) first_step[r] = (int64_t)step;
+            if (frac > retire_frac) {
+                active[r] = 0;
+                atomicSub(n_active, 1);
+            }
         }
     }
 }
@@ -184,7 +187,7 @@ extern "C" int tipt_ensemble_step(int storage, const void* phi, const void* pi, 
     int rc;
     if (storage != TIPT_F64 && storage != TIPT_F32C)
         return fail(TIPT_ERR_STORAGE, "the ensemble takes F64 or F32C storage");
-    if ((rc = check_state(storage, phi, pi, phi_out, pi_out, n_total, 1, 1))) return rc;
+    if ((rc = check_state_sites(storage, phi, pi, phi_out, pi_out, n_total))) return rc;
     if (!replicas || !chunks || !active || !sp) return fail(TIPT_ERR_ARG, "NULL argument");
     if (n_chunks < 0) return fail(TIPT_ERR_ARG, "n_chunks < 0");
     if (n_chunks == 0) return TIPT_OK;
@@ -219,22 +222,25 @@ extern "C" int tipt_ensemble_step(int storage, const void* phi, const void* pi, 
 extern "C" int tipt_ensemble_observe(int storage, const void* phi, int64_t n_total,
                                      const tipt_replica* replicas, int32_t n_replicas,
                                      int32_t* active, int32_t* n_active, double thr,
-                                     double stop_frac, uint64_t step, const uint64_t* counter,
+                                     double stop_frac, double retire_frac, uint64_t step,
+                                     const uint64_t* counter,
                                      int64_t offset, int64_t* first_step, double* frac_out,
                                      void* stream) {
     if (storage != TIPT_F64 && storage != TIPT_F32C)
         return fail(TIPT_ERR_STORAGE, "the ensemble takes F64 or F32C storage");
     if (!phi || !replicas || !active || !n_active || !first_step || !frac_out)
         return fail(TIPT_ERR_ARG, "NULL argument");
+    if (!(retire_frac >= stop_frac))
+        return fail(TIPT_ERR_ARG, "retire_frac must be >= stop_frac");
     if (n_replicas <= 0) return TIPT_OK;
     cudaStream_t st = (cudaStream_t)stream;
     if (storage == TIPT_F64)
         ensemble_observe_kernel<TIPT_F64><<<n_replicas, 256, 0, st>>>(
-            phi, n_total, replicas, active, n_active, thr, stop_frac, step,
+            phi, n_total, replicas, active, n_active, thr, stop_frac, retire_frac, step,
             reinterpret_cast<const unsigned long long*>(counter), offset, first_step, frac_out);
     else
         ensemble_observe_kernel<TIPT_F32C><<<n_replicas, 256, 0, st>>>(
-            phi, n_total, replicas, active, n_active, thr, stop_frac, step,
+            phi, n_total, replicas, active, n_active, thr, stop_frac, retire_frac, step,
             reinterpret_cast<const unsigned long long*>(counter), offset, first_step, frac_out);
     cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? TIPT_OK : fail_cuda(err, "ensemble_observe launch");

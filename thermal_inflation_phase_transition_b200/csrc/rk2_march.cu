@@ -724,5 +724,9 @@ extern "C" int tipt_device_status(int* status, int clear) {
         e = cudaMemcpyToSymbol(g_device_status, &zero, sizeof(int));
         if (e != cudaSuccess) return fail_cuda(e, "clear device status");
     }
+    int mlp = 0;
+    const int rc = mlp_status(&mlp, clear);
+    if (rc) return rc;
+    if (!*status) *status = mlp;
     return TIPT_OK;
 }

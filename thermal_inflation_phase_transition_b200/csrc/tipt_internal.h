@@ -26,6 +26,12 @@ bool overlap(const void* a, const void* b, int64_t n);
 int check_vsource(const tipt_vsource* vp, const char* name);
 int check_state(int storage, const void* phi, const void* pi, void* phi_out, void* pi_out,
                 int64_t nx, int64_t ny, int64_t nz);
+// The same pointer/overlap checks for a packed buffer of `sites` sites (ensembles).
+int check_state_sites(int storage, const void* phi, const void* pi, void* phi_out,
+                      void* pi_out, int64_t sites);
+
+// Status word of the surrogate kernels' bounded waits (TIPT_ERR_TIMEOUT or 0).
+int mlp_status(int* status, int clear);
 
 struct RealStageParams;
 int launch_real_stage(int storage, RealStageParams p, cudaStream_t st);

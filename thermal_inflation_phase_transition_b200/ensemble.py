@@ -5,8 +5,10 @@ reading the converted fraction off its snapshots.  ``Ensemble`` runs many
 replicas with uneven sizes, seeds, temperatures and couplings at once: every
 step is one persistent launch over a chunk work-list (``tipt_ensemble_step``);
 every ``check_every`` steps a per-replica reduction records the converted
-fraction (sites with phi > thr) and retires replicas whose fraction exceeds
-``stop_frac``, recording their first-passage step.  The check interval is
+fraction (sites with phi > thr), records the first-passage step of replicas
+whose fraction exceeds ``stop_frac`` and retires those whose fraction exceeds
+``retire_frac`` (default: ``stop_frac``; a larger value lets the conversion
+curve run on after the first passage).  The check interval is
 captured once into a CUDA graph (device step counter) and replayed.
 
 ``plain_first_passage`` runs the same replicas one at a time (one lattice per
@@ -75,8 +77,8 @@ class Ensemble:
     """Replicas stepped together; see the module docstring."""
 
     def __init__(self, specs, *, storage="f32c", dt=0.05, dx=1.0, eta=1.0, mu=1.0, inv_a2=1.0,
-                 thr=1.0, stop_frac=0.5, init_sigma=0.01, init_seed=0, chunk_sites=8192,
-                 check_every=10, device="cuda"):
+                 thr=1.0, stop_frac=0.5, retire_frac=None, init_sigma=0.01, init_seed=0,
+                 chunk_sites=8192, check_every=10, device="cuda"):
         if storage not in ("f32c", "f64"):
             raise ValueError("ensemble storage is 'f32c' or 'f64'")
         self.specs = list(specs)
@@ -86,6 +88,7 @@ class Ensemble:
         self.dev = torch.device(device)
         self.dt, self.dx, self.eta, self.mu, self.inv_a2 = dt, dx, eta, mu, inv_a2
         self.thr, self.stop_frac, self.check_every = thr, stop_frac, max(2, check_every & ~1)
+        self.retire_frac = stop_frac if retire_frac is None else max(retire_frac, stop_frac)
         reps = (L.Replica * self.R)()
         chunks = []
         off = 0
@@ -146,7 +149,8 @@ class Ensemble:
         # K is even: the state is back in buffer 0; the check records step counter + K - 1
         L.check(lib.tipt_ensemble_observe(
             self.st, ptr(self.phi[0]), self.n_total, ptr(self._reps), self.R, ptr(self.active),
-            ptr(self.n_active), float(self.thr), float(self.stop_frac), 0, ptr(self._counter),
+            ptr(self.n_active), float(self.thr), float(self.stop_frac), float(self.retire_frac),
+            0, ptr(self._counter),
             K - 1, ptr(self.first_step), ptr(self.frac), st), "tipt_ensemble_observe")
         L.check(lib.tipt_counter_add(ptr(self._counter), K, st), "tipt_counter_add")
 

@@ -125,3 +125,86 @@ def test_fp32_box_muller_accuracy():
     assert err.max() < 2e-6 * max(1.0, np.abs(z64).max())
     rel = err / np.maximum(np.abs(z64), 1e-3)
     assert np.median(rel) < 3e-7
+
+
+# ------------------------------------------------------------ complex field --
+from thermal_inflation_phase_transition_b200 import complex_field as CF  # noqa: E402
+
+
+def _cstate(shape, seed):
+    g = torch.Generator(device=DEV)
+    g.manual_seed(seed)
+    f = [0.5 + 0.6 * torch.randn(shape, dtype=torch.float64, device=DEV, generator=g)
+         for _ in range(2)]
+    f += [0.3 * torch.randn(shape, dtype=torch.float64, device=DEV, generator=g) for _ in range(2)]
+    return [RF.to_f32c(a) for a in f]
+
+
+def _crun(policy, shape, steps=3, tiles=(0, 0, 0), poly=False, eps4=1e-3):
+    L.set_kernel_policy(policy)
+    L.set_march_tiles(*tiles)
+    a = _cstate(shape, 5)
+    b = [torch.empty_like(x) for x in a]
+    if poly:
+        vs = poly_source(-0.02, -0.15, 0.1)
+    else:
+        t1, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.01), 0.0, 4.0, 4096)
+        tab = torch.from_numpy(t1).to(DEV)
+        vs = table_source(tab, tmin, dinv, 4096)
+    for n in range(steps):
+        CF.rk2_step_table_into(a, b, 0.05, 1.0, 0.9, 1.0, 1.0, vs, eps4=eps4, noise_scale=0.3,
+                               noise_step=n, seed=2)
+        a, b = b, a
+    torch.cuda.synchronize()
+    return a
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 64), (8, 12, 128), (5, 16, 16), (3, 8, 256),
+                                   (20, 4, 96)])
+def test_complex_march_equals_generic(shape):
+    a = _crun(1, shape)
+    b = _crun(2, shape)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("tiles", [(1, 2, 3), (2, 3, 4), (4, 64, 5), (2, 1, 3)])
+def test_complex_march_tilings_agree(tiles):
+    shape = (9, 16, 64)
+    ref = _crun(1, shape, poly=True, eps4=0.0)
+    got = _crun(2, shape, tiles=tiles, poly=True, eps4=0.0)
+    for x, y in zip(ref, got):
+        assert torch.equal(x, y)
+
+
+def test_complex_march_refuses_zn_when_forced():
+    L.set_kernel_policy(2)
+    a = _cstate((8, 8, 32), 1)
+    b = [torch.empty_like(x) for x in a]
+    vs = poly_source(-0.02, -0.15, 0.1)
+    with pytest.raises(L.TiptError):
+        CF.rk2_step_table_into(a, b, 0.05, 1.0, 0.9, 1.0, 1.0, vs, zn=(4.0, 0.01, 1.0))
+
+
+def test_complex_march_vs_oracle():
+    """Marching F32C complex steps against the FP64 CPU oracle (eps Re Phi^4 on)."""
+    shape = (12, 16, 64)
+    rng = np.random.default_rng(21)
+    f = [rng.normal(0.5, 0.6, shape) for _ in range(2)] + [rng.normal(0, 0.3, shape) for _ in range(2)]
+    tab, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.0), 0.0, 4.0, 4096)
+    ref = [a.copy() for a in f]
+    for n in range(4):
+        O.rk2_step_table_complex(*ref, 0.05, 1.0, 1.0, 1.0, None, None,
+                                 *[np.empty(shape) for _ in range(4)], 1.0, tab, tmin, dinv, 4096,
+                                 eps4=1e-3, noise_scale=0.3, noise_step=n, noise_seed=2)
+    L.set_kernel_policy(2)
+    st = [RF.to_f32c(torch.from_numpy(a).to(DEV)) for a in f]
+    tmp = [torch.empty_like(a) for a in st]
+    for n in range(4):
+        CF.rk2_step_table(*st, 0.05, 1.0, 1.0, 1.0, None, None, *tmp, 1.0,
+                          torch.from_numpy(tab).to(DEV), tmin, dinv, 4096, eps4=1e-3,
+                          noise_scale=0.3, noise_step=n, seed=2)
+    torch.cuda.synchronize()
+    for a, r in zip(st, ref):
+        got = RF.from_f32c(a).cpu().numpy()
+        assert np.abs(got - r).max() <= 5e-6 * np.abs(r).max()

@@ -4,57 +4,11 @@
 // 7-point stencil of (phi1, phi2, pi1, pi2).
 #include <cstring>
 
-#include "rk2_real.cuh"
+#include "rk2_complex.cuh"
+#include "rk2_march.cuh"
 #include "tipt_internal.h"
 
 namespace tipt {
-
-struct ComplexStageParams {
-    const void* f[4];   // phi1, phi2, pi1, pi2
-    void* o[4];
-    int n0, n1, n2;
-    double h1, h2, inv_dx2, eta, inv_mu2, inv_a2;
-    const void* noise1;
-    const void* noise2;
-    double ns_eff, nfac;
-    uint64_t step, mul, seed;
-    double zn_n, zn_dv, zn_active, eps4;
-    // V'(rho) source (1-D table or polynomial)
-    int vkind, npts;
-    const double* table;
-    double tmin, dinv;
-    double c1, c2, c3;
-    int table_in_smem;
-};
-
-// C:2137-2158 projection + Z_N (reference form), then eps*Re(Phi^4) whose
-// gradient is 4 eps (p1^3 - 3 p1 p2^2, 3 p1^2 p2 - p2^3).
-template <typename R>
-__device__ __forceinline__ void complex_force(const ComplexStageParams& p, const R* tab, R tmin,
-                                              R dinv, R p1, R p2, R& d1, R& d2) {
-    R rho = sqrt(p1 * p1 + p2 * p2);
-    R rho_safe = rho > R(1e-30) ? rho : R(1e-30);
-    R dvdr;
-    if (p.vkind == TIPT_VP_POLY) dvdr = poly_vprime<R>((R)p.c1, (R)p.c2, (R)p.c3, rho);
-    else dvdr = lerp_table<R>(tab, tmin, dinv, p.npts - 2, rho);
-    R a = dvdr * p1 / rho_safe;
-    R b = dvdr * p2 / rho_safe;
-    if (p.zn_active > 0.5 && p.zn_n > 0.5 && rho > R(1e-20)) {
-        R th = atan2(p2, p1);
-        R sn = sin((R)p.zn_n * th);
-        R ir = R(1) / rho_safe;
-        R ir2 = ir * ir;
-        a += -(R)p.zn_n * (R)p.zn_dv * sn * p2 * ir2;
-        b += (R)p.zn_n * (R)p.zn_dv * sn * p1 * ir2;
-    }
-    if (p.eps4 != 0.0) {
-        const R e4 = R(4) * (R)p.eps4;
-        a += e4 * (p1 * p1 * p1 - R(3) * p1 * p2 * p2);
-        b += e4 * (R(3) * p1 * p1 * p2 - p2 * p2 * p2);
-    }
-    d1 = a;
-    d2 = b;
-}
 
 template <typename NT>
 __device__ __forceinline__ void complex_noise(const ComplexStageParams& p, uint64_t site,
@@ -172,76 +126,51 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
                     hi[f][q] = __ldg(src + idx[q]);
                     lo[f][q] = __ldg(src + N + idx[q]);
                 }
-            const float h1 = (float)p.h1, inv_dx2 = (float)p.inv_dx2;
-            const float h2h = (float)p.h2, h2l = (float)(p.h2 - (double)h2h);
-            const float inv_a2 = (float)p.inv_a2, eta = (float)p.eta, inv_mu2 = (float)p.inv_mu2;
-            float lap[4], c[4];
+            CplxIn<float> in;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                float dh, dl;
-                stencil_sums(hi[f], lo[f], dh, dl);
-                lap[f] = __fmul_rn(__fadd_rn(dh, dl), inv_dx2);
-                c[f] = __fadd_rn(hi[f][0], lo[f][0]);
+                stencil_sums(hi[f], lo[f], in.dh[f], in.dl[f]);
+                in.ch[f] = hi[f][0];
+                in.cl[f] = lo[f][0];
             }
             const float* ftab = reinterpret_cast<const float*>(s_tab);
+            const float h1 = (float)p.h1;
             // The Z_N force of the reference form (C:2152-2158) grows like 1/rho
-            // near the origin and amplifies FP32 rounding, so with Z_N active the
-            // force is evaluated in FP64 from the full hi + lo values (q1d, q2d).
-            const bool zn = p.zn_active > 0.5 && p.zn_n > 0.5;
-            auto cforce = [&](float q1, float q2, double q1d, double q2d, float& d1, float& d2) {
-                if (!zn && (p.table_in_smem || p.vkind == TIPT_VP_POLY)) {
-                    complex_force<float>(p, ftab, (float)p.tmin, (float)p.dinv, q1, q2, d1, d2);
+            // near the origin and amplifies FP32 rounding, so with Z_N active (or a
+            // table too large for shared memory) the force is evaluated in FP64 from
+            // the full hi + lo values of the centre or the midpoint.
+            const bool fp32_force = !(p.zn_active > 0.5 && p.zn_n > 0.5) &&
+                                    (p.table_in_smem || p.vkind == TIPT_VP_POLY);
+            auto force = [&](float q1, float q2, int which, float& d1, float& d2) {
+                if (fp32_force) {
+                    complex_force_v<float>(p, ftab, (float)p.tmin, (float)p.dinv, q1, q2, d1, d2);
                 } else {
+                    double q1d = (double)hi[0][0] + (double)lo[0][0];
+                    double q2d = (double)hi[1][0] + (double)lo[1][0];
+                    if (which) {
+                        q1d = (double)hi[0][0] + ((double)lo[0][0] + (double)h1 * ((double)hi[2][0] + (double)lo[2][0]));
+                        q2d = (double)hi[1][0] + ((double)lo[1][0] + (double)h1 * ((double)hi[3][0] + (double)lo[3][0]));
+                    }
                     double e1, e2;
                     complex_force<double>(p, p.table, p.tmin, p.dinv, q1d, q2d, e1, e2);
                     d1 = (float)e1;
                     d2 = (float)e2;
                 }
             };
-            float d1, d2;
-            cforce(c[0], c[1], (double)hi[0][0] + (double)lo[0][0],
-                   (double)hi[1][0] + (double)lo[1][0], d1, d2);
-            const float k1[2] = {force_v<float>(inv_a2, eta, inv_mu2, lap[0], c[2], d1),
-                                 force_v<float>(inv_a2, eta, inv_mu2, lap[1], c[3], d2)};
-            float t_hi[2], t_lo[2], pit[2], q[2];
-#pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                float e;
-                two_sum(hi[2 + a][0], __fmul_rn(h1, k1[a]), t_hi[a], e);
-                t_lo[a] = __fadd_rn(lo[2 + a][0], e);
-                pit[a] = __fadd_rn(t_hi[a], t_lo[a]);
-                q[a] = __fadd_rn(hi[a][0], __fmaf_rn(h1, c[2 + a], lo[a][0]));
-            }
-            cforce(q[0], q[1],
-                   (double)hi[0][0] + ((double)lo[0][0] + (double)h1 * ((double)hi[2][0] + (double)lo[2][0])),
-                   (double)hi[1][0] + ((double)lo[1][0] + (double)h1 * ((double)hi[3][0] + (double)lo[3][0])),
-                   d1, d2);
-            const float k2[2] = {force_v<float>(inv_a2, eta, inv_mu2, __fmaf_rn(h1, lap[2], lap[0]), pit[0], d1),
-                                 force_v<float>(inv_a2, eta, inv_mu2, __fmaf_rn(h1, lap[3], lap[1]), pit[1], d2)};
             float kick[2] = {0.0f, 0.0f};
             if (p.noise1) {
                 kick[0] = (float)(p.nfac * static_cast<const double*>(p.noise1)[s]);
                 kick[1] = (float)(p.nfac * static_cast<const double*>(p.noise2)[s]);
-            } else if (p.ns_eff != 0.0) {
-                float z1, z2;
-                gauss_pair_f(noise_key((uint64_t)s, p.step, p.mul, p.seed), z1, z2);
-                kick[0] = __fmul_rn((float)p.ns_eff, z1);
-                kick[1] = __fmul_rn((float)p.ns_eff, z2);
+            } else {
+                complex_kick_f32c(p, (uint64_t)s, kick[0], kick[1]);
             }
+            float oh[4], ol[4];
+            complex_update_f32c<float>(p, in, kick, force, oh, ol);
 #pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                const float d_hi = __fmul_rn(h2h, t_hi[a]);
-                const float d_lo = __fadd_rn(__fmaf_rn(h2h, t_hi[a], -d_hi),
-                                             __fmaf_rn(h2h, t_lo[a], __fmul_rn(h2l, t_hi[a])));
-                float nh, nl;
-                ff_add(hi[a][0], lo[a][0], d_hi, d_lo, nh, nl);
-                float* po = static_cast<float*>(p.o[a]);
-                po[s] = nh;
-                po[N + s] = nl;
-                ff_add(hi[2 + a][0], lo[2 + a][0], __fmaf_rn(h2h, k2[a], kick[a]), 0.0f, nh, nl);
-                float* vo = static_cast<float*>(p.o[2 + a]);
-                vo[s] = nh;
-                vo[N + s] = nl;
+            for (int f = 0; f < 4; ++f) {
+                float* po = static_cast<float*>(p.o[f]);
+                po[s] = oh[f];
+                po[N + s] = ol[f];
             }
         }
     }
@@ -270,6 +199,12 @@ int launch_complex_stage(int storage, ComplexStageParams p, cudaStream_t st) {
     int64_t tb = p.vkind == TIPT_VP_POLY ? 0 : (int64_t)p.npts * (storage == TIPT_F32C ? 4 : 8);
     p.table_in_smem = (tb > 0 && tb <= kMaxTableSmemC) ? 1 : 0;
     const int64_t smem = p.table_in_smem ? tb : 0;
+    if (storage == TIPT_F32C && kernel_policy() != 1) {
+        if (complex_march_supported(p)) return launch_complex_march(p, st);
+        if (kernel_policy() == 2)
+            return fail(TIPT_ERR_UNSUPPORTED, "the complex marching kernel does not take this "
+                        "call (Z_N active, noise arrays, table or shape)");
+    }
     switch (storage) {
         case TIPT_F64: return launch_complex_generic<TIPT_F64>(p, smem, st);
         case TIPT_F32: return launch_complex_generic<TIPT_F32>(p, smem, st);

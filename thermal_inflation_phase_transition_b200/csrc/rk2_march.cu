@@ -514,6 +514,193 @@ __global__ void __maxnreg__(kMarchRegs)
     }
 }
 
+// ----------------------------------------------------- complex, F32C ----
+// Complex field in compensated FP32: four planar fields (phi1, phi2, pi1, pi2;
+// hi plane then lo plane each), so a ring stage holds eight (TJ+2)-row blocks.
+// A consumer thread owns two consecutive sites of its row (one 8-byte vector
+// per plane and neighbour) and evaluates them in the two lanes of the packed
+// FP32x2 instructions with the arithmetic of the generic kernel
+// (complex_update_f32c), so the results are bitwise identical.
+template <bool WIDE>
+__global__ void __maxnreg__(kMarchRegs)
+    complex_stage_march_f32c(const __grid_constant__ CUtensorMap tm0,
+                             const __grid_constant__ CUtensorMap tm1,
+                             const __grid_constant__ CUtensorMap tm2,
+                             const __grid_constant__ CUtensorMap tm3, ComplexStageParams p,
+                             MarchGeom g) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    float* s_tab = reinterpret_cast<float*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + g.tab_bytes);
+    uint64_t* empty = full + 8;
+    unsigned char* ring = smem + g.tab_bytes + 128;
+
+    const int n0 = p.n0, n1 = p.n1, n2 = p.n2;
+    const int pitch = g.pitch;
+    const int TJ = g.TJ;
+    const uint32_t NS = (uint32_t)g.S;
+    const int rows = TJ + 2;
+    const int tpr = n2 >> 1;
+    const int nc = TJ * tpr;
+    const int t = threadIdx.x;
+
+    if (t == 0) {
+        for (uint32_t s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], nc / 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (p.table_in_smem)
+        for (int q = t; q < p.npts; q += blockDim.x) s_tab[q] = (float)__ldg(p.table + q);
+    __syncthreads();
+
+    const size_t plane_blk = (size_t)(g.stage_bytes >> 3);  // one [rows][pitch] block, bytes
+    // stage -> field f (phi1, phi2, pi1, pi2) -> component c (0 hi, 1 lo)
+    auto blk = [&](uint32_t stage, int f, int c) -> float* {
+        return reinterpret_cast<float*>(ring + (size_t)stage * g.stage_bytes +
+                                        (size_t)(2 * f + c) * plane_blk);
+    };
+
+    // ------------------------------------------------------------ producer
+    if (t >= nc) {
+        if (t != nc) return;
+        const CUtensorMap* tm[4] = {&tm0, &tm1, &tm2, &tm3};
+        const uint32_t plane_tx = (uint32_t)(8 * rows * n2 * 4);
+        RingPos w{0, 0};
+        uint32_t issued = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
+            const int ic = item / g.nJB;
+            const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+            const int npl = min(g.CI, n0 - i0) + 2;
+            for (int q = 0; q < npl; ++q) {
+                if (issued >= NS && !mbar_wait(&empty[w.stage], w.phase ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(&full[w.stage], plane_tx);
+                int iw = i0 - 1 + q;
+                iw = iw < 0 ? iw + n0 : (iw >= n0 ? iw - n0 : iw);
+                for (int rr = 0; rr < rows; ++rr) {
+                    int jr = j0 - 1 + rr;
+                    jr = jr < 0 ? jr + n1 : (jr >= n1 ? jr - n1 : jr);
+                    for (int kb = 0; kb < n2; kb += g.BK) {
+                        const int o = rr * pitch + kb;
+#pragma unroll
+                        for (int f = 0; f < 4; ++f) {
+                            // plane iw = hi, plane n0 + iw = lo
+                            tma_row(blk(w.stage, f, 0) + o, tm[f], kb, jr, iw, &full[w.stage]);
+                            tma_row(blk(w.stage, f, 1) + o, tm[f], kb, jr, n0 + iw, &full[w.stage]);
+                        }
+                    }
+                }
+                ++issued;
+                w.next(NS);
+            }
+        }
+        if (!ok) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+        RingPos d = w;
+        for (uint32_t k = 0; k < NS && k < issued; ++k) {
+            d.stage = d.stage == 0 ? NS - 1 : d.stage - 1;
+            if (d.stage == NS - 1) d.phase ^= 1u;
+            (void)mbar_wait(&full[d.stage], d.phase);
+        }
+        return;
+    }
+
+    // ----------------------------------------------------------- consumers
+    const int lane = t & 31;
+    const int r = 1 + t / tpr;                 // own tile row (1..TJ)
+    const int k0 = 2 * (t - (r - 1) * tpr);    // first of the two own columns
+    const int kml = k0 == 0 ? n2 - 1 : k0 - 1;
+    const int kpr = k0 + 2 == n2 ? 0 : k0 + 2;
+    const float tminf = (float)p.tmin, dinvf = (float)p.dinv;
+    const int64_t N = (int64_t)n0 * n1 * n2;
+    const int orow = r * pitch, urow = (r - 1) * pitch, drow = (r + 1) * pitch;
+    auto force = [&](float2 q1, float2 q2, int, float2& d1, float2& d2) {
+        complex_force_v<float2>(p, s_tab, tminf, dinvf, q1, q2, d1, d2);
+    };
+
+    RingPos pm{0, 0};
+    for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
+        const int ic = item / g.nJB;
+        const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+        const int ni = min(g.CI, n0 - i0);
+        const int jw = j0 + r - 1;
+        RingPos pc = pm, pp;
+        pc.next(NS);
+        pp = pc;
+        pp.next(NS);
+        if (!mbar_wait(&full[pm.stage], pm.phase) || !mbar_wait(&full[pc.stage], pc.phase)) {
+            if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+            return;
+        }
+        for (int q = 0; q < ni; ++q) {
+            if (!mbar_wait(&full[pp.stage], pp.phase)) {
+                if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+                return;
+            }
+            const int i = i0 + q;
+            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2 + k0;
+            CplxIn<float2> in;
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const float* sc = blk(pc.stage, f, c);
+                    const float2 ce = *reinterpret_cast<const float2*>(sc + orow + k0);
+                    const float2 jm = *reinterpret_cast<const float2*>(sc + urow + k0);
+                    const float2 jp = *reinterpret_cast<const float2*>(sc + drow + k0);
+                    const float2 im = *reinterpret_cast<const float2*>(blk(pm.stage, f, c) + orow + k0);
+                    const float2 ip = *reinterpret_cast<const float2*>(blk(pp.stage, f, c) + orow + k0);
+                    const float kl = sc[orow + kml], kr = sc[orow + kpr];
+                    // lanes = sites k0, k0+1; neighbours in the order ip, im, jp, jm, kp, km
+                    const float2 nb[6] = {ip, im, jp, jm, make_float2(ce.y, kr), make_float2(kl, ce.x)};
+                    float2 acc;
+                    if (c == 0) {  // dh = sum (hi_n - hi_c)
+                        acc = v_sub(nb[0], ce);
+#pragma unroll
+                        for (int n = 1; n < 6; ++n) acc = v_add(acc, v_sub(nb[n], ce));
+                        in.dh[f] = acc;
+                        in.ch[f] = ce;
+                    } else {       // dl = fma(-6, lo_c, sum lo_n)
+                        acc = nb[0];
+#pragma unroll
+                        for (int n = 1; n < 6; ++n) acc = v_add(acc, nb[n]);
+                        in.dl[f] = v_fma(vs<float2>(-6.0f), ce, acc);
+                        in.cl[f] = ce;
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[pm.stage]);  // plane i-1 is no longer read
+            float2 kick[2];
+            if constexpr (WIDE)
+                complex_kick_f32c2(p, (uint64_t)rowoff, (uint64_t)(rowoff + 1), kick[0], kick[1]);
+            else
+                complex_kick_f32c2(p, (uint32_t)rowoff, (uint32_t)rowoff + 1u, kick[0], kick[1]);
+            float2 oh[4], ol[4];
+            complex_update_f32c<float2>(p, in, kick, force, oh, ol);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                float* po = static_cast<float*>(p.o[f]);
+                *reinterpret_cast<float2*>(po + rowoff) = oh[f];
+                *reinterpret_cast<float2*>(po + N + rowoff) = ol[f];
+            }
+            pm = pc;
+            pc = pp;
+            pp.next(NS);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(&empty[pm.stage]);
+            mbar_arrive(&empty[pc.stage]);
+        }
+        pm = pp;
+    }
+}
+
 // ------------------------------------------------------------------ host ---
 using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                               const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -696,6 +883,96 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
         return wide ? launch_march_k(rk2_stage_march<TIPT_F64, true>, tphi, tpi, p, g, smem, st)
                     : launch_march_k(rk2_stage_march<TIPT_F64, false>, tphi, tpi, p, g, smem, st);
     return fail(TIPT_ERR_STORAGE, "marching kernel takes F32C or F64");
+}
+
+// Complex F32C geometry: two sites per consumer thread (tpr = n2/2 per row),
+// eight planes per ring stage; the same scoring as the real field.
+static bool complex_geometry(const ComplexStageParams& p, MarchGeom& g, int64_t& smem) {
+    const int n1 = p.n1, n2 = p.n2;
+    const int es = 4, np = 8;
+    if (n2 % 2 != 0 || n2 < 16 || n2 > 1024) return false;
+    g.BK = pick_bk(n2, es);
+    if (!g.BK) return false;
+    const int per128 = 128 / es;
+    g.pitch = (n2 + per128 - 1) / per128 * per128;
+    const int tpr = n2 / 2;
+    g.tab_bytes = p.table_in_smem ? round128(p.npts * 4) : 0;
+    g.CI = g_force_ci > 0 ? g_force_ci : 64;
+    if (g.CI > p.n0) g.CI = p.n0;
+    double best = -1.0;
+    MarchGeom pick{};
+    for (int tj = 1; tj <= 64; ++tj) {
+        if (g_force_tj > 0 && tj != g_force_tj) continue;
+        if (n1 % tj || (tj * tpr) % 32 || tj * tpr > 512) continue;
+        for (int st = 3; st <= 5; ++st) {
+            if (g_force_stages > 0 && st != g_force_stages) continue;
+            MarchGeom c = g;
+            c.TJ = tj;
+            c.S = st;
+            c.stage_bytes = np * round128((tj + 2) * c.pitch * es);
+            if (smem_need(c) > kSmemPerCta) continue;
+            const int cps = ctas_per_sm(c, tpr);
+            if (cps < 1) continue;
+            const double score = cps * (tj * tpr / 32) * (double)tj / (tj + 2) + 0.01 * st;
+            if (score > best) {
+                best = score;
+                pick = c;
+            }
+        }
+    }
+    if (best < 0) return false;
+    g = pick;
+    if ((g.pitch * es) % 128 || ((g.BK * es) % 128 && g.BK != n2) || (g.BK * es) % 16 ||
+        g.stage_bytes % (128 * np) || g.tab_bytes % 128)
+        return false;
+    g.nJB = n1 / g.TJ;
+    g.nIC = (p.n0 + g.CI - 1) / g.CI;
+    g.items = g.nJB * g.nIC;
+    smem = smem_need(g);
+    return true;
+}
+
+bool complex_march_supported(const ComplexStageParams& p) {
+    if (p.noise1 || (p.zn_active > 0.5 && p.zn_n > 0.5)) return false;
+    if (p.vkind != TIPT_VP_POLY && !p.table_in_smem) return false;
+    if (!encode_fn()) return false;
+    uintptr_t a = 0;
+    for (int f = 0; f < 4; ++f)
+        a |= reinterpret_cast<uintptr_t>(p.f[f]) | reinterpret_cast<uintptr_t>(p.o[f]);
+    if (a % 16) return false;
+    MarchGeom g;
+    int64_t smem;
+    return complex_geometry(p, g, smem);
+}
+
+int launch_complex_march(const ComplexStageParams& p, cudaStream_t st) {
+    MarchGeom g;
+    int64_t smem;
+    if (!complex_geometry(p, g, smem))
+        return fail(TIPT_ERR_UNSUPPORTED, "complex marching kernel geometry");
+    const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
+    CUtensorMap tm[4];
+    for (int f = 0; f < 4; ++f)
+        if (!make_map(&tm[f], p.f[f], 2 * p.n0, p.n1, p.n2, 4, g.BK))
+            return fail(TIPT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    auto kern = wide ? complex_stage_march_f32c<true> : complex_stage_march_f32c<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return fail_cuda(e, "complex marching kernel attributes");
+    const int threads = g.TJ * (p.n2 / 2) + 32;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, (size_t)smem);
+    if (e != cudaSuccess || per_sm < 1)
+        return fail(TIPT_ERR_UNSUPPORTED, "complex marching kernel does not fit an SM (%d "
+                    "threads, %lld bytes of shared memory)", threads, (long long)smem);
+    int grid = num_sms() * per_sm;
+    if (grid > g.items) grid = g.items;
+    kern<<<grid, threads, (size_t)smem, st>>>(tm[0], tm[1], tm[2], tm[3], p, g);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "complex marching kernel launch");
 }
 
 }  // namespace tipt

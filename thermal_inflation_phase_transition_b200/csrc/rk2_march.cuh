@@ -1,11 +1,15 @@
 // Marching (2.5-D blocked) real-field stage kernel -- declarations.
 #pragma once
 
-#include "rk2_real.cuh"
+#include "rk2_complex.cuh"
 
 namespace tipt {
 
 bool march_supported(int storage, const RealStageParams& p);
 int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cudaStream_t st);
+
+// Complex field, compensated FP32, Z_N off, V'(rho) polynomial or staged in shared memory.
+bool complex_march_supported(const ComplexStageParams& p);
+int launch_complex_march(const ComplexStageParams& p, cudaStream_t st);
 
 }  // namespace tipt

@@ -136,6 +136,8 @@ constexpr int64_t kMaxTableSmem = 96 * 1024;
 // Kernel choice: 0 automatic, 1 generic kernel only, 2 marching kernel only.
 static int g_kernel_policy = 0;
 
+int kernel_policy() { return g_kernel_policy; }
+
 // A lattice whose contiguous extent is 1 (the reference's 2-D form nz = 1) is
 // relabelled so the contiguous axis is the longest non-trivial one: (nx, ny, 1)
 // -> (1, nx, ny) and (nx, 1, 1) -> (1, 1, nx).  Linear site indices, hence the

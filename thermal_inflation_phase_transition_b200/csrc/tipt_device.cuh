@@ -269,6 +269,32 @@ __device__ __forceinline__ void gauss_pair_f(uint64_t key, float& z1, float& z2)
     z2 = __fmul_rn(r, s);
 }
 
+// (z1, z2) pairs for two keys in the lanes of float2s (bitwise the same as two
+// calls of gauss_pair_f).
+__device__ __forceinline__ void gauss_pair_f2(uint64_t key0, uint64_t key1, float2& z1,
+                                              float2& z2) {
+    uint32_t h1a, l1a, h2a, l2a, h1b, l1b, h2b, l2b, qa, qb;
+    hash_words(key0, h1a, l1a, h2a, l2a);
+    hash_words(key1, h1b, l1b, h2b, l2b);
+    float ga, ka, gb, kb, xa, xb;
+    bool ca, cb;
+    log_u1_reduce(h1a, l1a, ga, ka, ca);
+    log_u1_reduce(h1b, l1b, gb, kb, cb);
+    float2 lg = log_u1_series<float2>(make_float2(ga, gb), make_float2(ka, kb));
+    lg.x = ca ? kLog1em12 : lg.x;
+    lg.y = cb ? kLog1em12 : lg.y;
+    angle_reduce(h2a, l2a, qa, xa);
+    angle_reduce(h2b, l2b, qb, xb);
+    float2 sn, cs;
+    sincos_series<float2>(make_float2(xa, xb), sn, cs);
+    float2 c, s;
+    quarter_turn(qa, sn.x, cs.x, c.x, s.x);
+    quarter_turn(qb, sn.y, cs.y, c.y, s.y);
+    const float2 r = radius_from_log<float2>(lg);
+    z1 = v_mul(r, c);
+    z2 = v_mul(r, s);
+}
+
 // ------------------------------------------------------- float-float ----
 // Error-free sum (Knuth TwoSum) and a renormalised float-float add, in lane
 // vectors; every operation is an explicit round-to-nearest intrinsic.

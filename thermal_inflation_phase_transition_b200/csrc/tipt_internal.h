@@ -30,6 +30,9 @@ int check_state(int storage, const void* phi, const void* pi, void* phi_out, voi
 int check_state_sites(int storage, const void* phi, const void* pi, void* phi_out,
                       void* pi_out, int64_t sites);
 
+// Stage kernel selection set by tipt_set_kernel_policy (0 auto, 1 generic, 2 marching).
+int kernel_policy();
+
 // Status word of the surrogate kernels' bounded waits (TIPT_ERR_TIMEOUT or 0).
 int mlp_status(int* status, int clear);
 

@@ -241,7 +241,8 @@ def main():
     ap.add_argument("--storage", choices=["f32c", "f64", "f32"], default="f32c")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["lattice", "ensemble", "surrogate"], default="lattice",
+    ap.add_argument("--workload", choices=["lattice", "complex", "ensemble", "surrogate"],
+                    default="lattice",
                     help="lattice: the 512^3 site-update headline; ensemble: Gamma estimates "
                          "per GPU-hour of the batched replica engine vs one-at-a-time launches")
     ap.add_argument("--ens-steps", type=int, default=2000)
@@ -254,6 +255,9 @@ def main():
         return
     if args.workload == "surrogate" and args.impl == "tipt":
         run_surrogate_bench(args)
+        return
+    if args.workload == "complex" and args.impl == "tipt":
+        run_complex_bench(args)
         return
 
     if args.impl == "reference":
@@ -513,6 +517,92 @@ def run_ensemble_bench(args):
     }
     print(json.dumps(line, default=lambda o: o.item() if hasattr(o, "item") else str(o)),
           flush=True)
+
+
+def run_complex_bench(args):
+    """Complex field (config 3): 512^3 compensated FP32, V = D(T^2-T0^2)|Phi|^2 - E T |Phi|^3
+    + lam/4 |Phi|^4 tabulated in |Phi| (4096 points on [0, 3]) plus eps Re(Phi^4) analytic
+    (eps = 1e-3), T = 0.98 (below T0: the U(1) breaks and strings form), hash noise per
+    component, seed 2; tile shape from the autotuner.  One step = one midpoint dt-step of
+    the whole lattice.  The plaquette winding (all three orientations, string length) runs
+    every 500 steps; it is timed separately and amortised into `ms_per_step_with_winding`."""
+    import torch
+    from thermal_inflation_phase_transition_b200 import autotune as AT
+    from thermal_inflation_phase_transition_b200 import complex_field as CF
+    from thermal_inflation_phase_transition_b200 import real_field as RF
+    from thermal_inflation_phase_transition_b200._common import table_source
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    n = args.size
+    shape = (n, n, n)
+    N = n ** 3
+    T = 0.98
+    x = np.linspace(PHI_LO, PHI_HI, NPHI)
+    tab = torch.from_numpy(toy_vprime(x, T)).to(dev)
+    vs = table_source(tab, PHI_LO, 1.0 / ((PHI_HI - PHI_LO) / (NPHI - 1)), NPHI)
+    ns = noise_scale(T)
+    tiles = AT.apply(shape, "f32c", field="complex", tune_if_missing=True)
+    g = torch.Generator(device=dev)
+    g.manual_seed(2)
+    cur = [RF.to_f32c(0.01 * torch.randn(shape, dtype=torch.float64, device=dev, generator=g))
+           for _ in range(2)]
+    cur += [torch.zeros_like(cur[0]), torch.zeros_like(cur[0])]
+    nxt = [torch.empty_like(a) for a in cur]
+
+    def step(k):
+        nonlocal cur, nxt
+        CF.rk2_step_table_into(cur, nxt, DT, DX, ETA, 1.0, 1.0, vs, eps4=1e-3, noise_scale=ns,
+                               noise_step=k, seed=2)
+        cur, nxt = nxt, cur
+
+    total = args.warmup + args.steps
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        time.sleep(0.3)
+        torch.cuda.synchronize()
+        ev0.record()
+        for k in range(args.warmup, total):
+            step(k)
+        ev1.record()
+        torch.cuda.synchronize()
+    per_step_ms = ev0.elapsed_time(ev1) / args.steps
+    # winding on the evolved field (all orientations, pierced-plaquette counts)
+    for _ in range(2):
+        wr = CF.compute_winding_number_full(cur[0], cur[1], w_site=False, w3=False)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(5):
+        wr = CF.compute_winding_number_full(cur[0], cur[1], w_site=False, w3=False)
+    ev1.record()
+    torch.cuda.synchronize()
+    wind_ms = ev0.elapsed_time(ev1) / 5
+    counts = wr.host_counts()
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    bps = 64
+    achieved = bps * N / (per_step_ms / 1000.0) / 1e9
+    line = {
+        "metric": "complex site-updates/s", "value": N / (per_step_ms / 1000.0),
+        "unit": "site-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32c", "data": "synthetic",
+        "config": {"workload": f"complex field {n}^3 periodic, FP32-compensated, V'(|Phi|) "
+                               "table 4096 + eps Re(Phi^4) eps=1e-3, T=0.98, hash noise "
+                               "per component seed 2", "lattice": [n, n, n],
+                   "tiles": list(tiles) if tiles else "heuristic",
+                   "l2": "inputs larger than L2 (state %.1f GB)" % (bps * N / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "algorithmic_bytes_per_site": bps,
+                     "kernel": "complex rk2 fused midpoint stage"},
+        "winding": {"ms": wind_ms, "every_steps": 500, "string_length": counts["string_length"],
+                    "pierced": [counts["pierced_xy"], counts["pierced_xz"], counts["pierced_yz"]]},
+        "ms_per_step_with_winding": per_step_ms + wind_ms / 500.0,
+        "gpu_launches": args.steps, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
 
 
 def run_surrogate_bench(args):

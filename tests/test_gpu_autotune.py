@@ -53,3 +53,15 @@ def test_candidates_cover_default_shapes():
     assert {tj for tj, _, _ in c} == {1, 2, 4}
     assert all(st in (3, 4, 5) for _, _, st in c)
     assert AT.candidates((128, 128, 1))  # 2-D lattices march along x
+
+
+def test_tune_complex_field(tmp_path, monkeypatch):
+    """The complex-field marching kernel is tuned under its own cache key."""
+    monkeypatch.setenv("TIPT_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    shape = (8, 16, 64)
+    res = AT.tune(shape, "f32c", steps=2, warmup=1, field="complex")
+    assert res["tried"] >= 3
+    cache = json.load(open(tmp_path / "tune.json"))
+    assert AT.cache_key(shape, "f32c", 4096, field="complex") in cache
+    assert AT.cache_key(shape, "f32c", 4096) not in cache
+    assert all((tj * 32) % 32 == 0 for tj, _, _ in AT.candidates(shape, "complex"))

@@ -1,10 +1,11 @@
-"""Tile-shape autotuner of the marching stage kernel, with a persisted JSON cache.
+"""Tile-shape autotuner of the marching stage kernels, with a persisted JSON cache.
 
-The marching kernel's tile is (rows per tile, planes per work item, ring
-stages).  The built-in heuristic scores candidates by occupancy and halo share;
+A marching kernel's tile is (rows per tile, planes per work item, ring
+stages); ``field="real"`` tunes the real-field kernel, ``field="complex"`` the
+complex-field one (compensated FP32).  The built-in heuristic scores candidates by occupancy and halo share;
 ``tune`` instead times every admissible candidate on the device (CUDA events,
 inputs larger than L2 where the lattice is) and keeps the fastest.  Results are
-cached per (GPU name, storage, lattice shape, V' table size) in a JSON file
+cached per (GPU name, field, storage, lattice shape, V' table size) in a JSON file
 (``$TIPT_AUTOTUNE_CACHE``, else ``~/.cache/tipt_b200/autotune.json``);
 ``apply`` installs a cached shape, or the heuristic when there is none.
 
@@ -20,6 +21,7 @@ import time
 import torch
 
 from . import _lib as L
+from . import complex_field as CF
 from . import real_field as RF
 from ._common import table_source
 
@@ -36,12 +38,13 @@ def cache_path() -> str:
     return os.path.join(os.path.expanduser("~"), ".cache", "tipt_b200", "autotune.json")
 
 
-def cache_key(shape, storage, table_points, device=None) -> str:
+def cache_key(shape, storage, table_points, device=None, field="real") -> str:
     dev = torch.device(device or "cuda")
     name = torch.cuda.get_device_name(dev).replace(" ", "_")
     cc = "%d.%d" % torch.cuda.get_device_capability(dev)
     nx, ny, nz = shape
-    return f"{name}|sm{cc}|{storage}|{nx}x{ny}x{nz}|table{int(table_points)}"
+    tag = "" if field == "real" else f"{field}|"
+    return f"{name}|sm{cc}|{tag}{storage}|{nx}x{ny}x{nz}|table{int(table_points)}"
 
 
 def load_cache() -> dict:
@@ -61,12 +64,16 @@ def _save_cache(c: dict) -> None:
     os.replace(tmp, p)
 
 
-def candidates(shape):
+def candidates(shape, field="real"):
     """(rows, planes, stages) the kernel may accept for this lattice (the kernel still
     rejects those that do not fit shared memory)."""
     nx, ny, nz = shape
-    n0, n1, n2 = (1, nx, ny) if nz == 1 else (nx, ny, nz)
-    tpr = n2 // 4
+    if field == "real":
+        n0, n1, n2 = (1, nx, ny) if nz == 1 else (nx, ny, nz)
+        tpr = n2 // 4
+    else:
+        n0, n1, n2 = nx, ny, nz
+        tpr = n2 // 2
     out = []
     for tj in range(1, 65):
         if n1 % tj or (tj * tpr) % 32 or tj * tpr > 512:
@@ -79,10 +86,15 @@ def candidates(shape):
     return out
 
 
-def _state(shape, storage, device):
+def _state(shape, storage, device, field="real"):
     nx, ny, nz = shape
     g = torch.Generator(device=device)
     g.manual_seed(1)
+    if field == "complex":
+        f = [torch.zeros((2, nx, ny, nz), dtype=torch.float32, device=device) for _ in range(4)]
+        for a in f[:2]:
+            a[0] = 0.5 + 0.01 * torch.randn((nx, ny, nz), generator=g, device=device)
+        return [f, [torch.empty_like(a) for a in f]]
     if storage == "f32c":
         phi = torch.zeros((2, nx, ny, nz), dtype=torch.float32, device=device)
         phi[0] = 0.01 * torch.randn((nx, ny, nz), generator=g, device=device)
@@ -93,9 +105,8 @@ def _state(shape, storage, device):
     return [phi, pi, torch.empty_like(phi), torch.empty_like(pi)]
 
 
-def _time(state, table, steps, warmup):
-    """Mean ms per stage launch (ping-pong between the two state pairs)."""
-    bufs = ((state[0], state[1]), (state[2], state[3]))
+def _time(state, table, steps, warmup, field="real"):
+    """Mean ms per stage launch (ping-pong between the two state sets)."""
     vs = table_source(table, 0.0, (table.numel() - 1) / 3.0, table.numel())
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -103,6 +114,12 @@ def _time(state, table, steps, warmup):
         if n == warmup:
             torch.cuda.synchronize()
             e0.record()
+        if field == "complex":
+            a, b = state[n % 2], state[(n + 1) % 2]
+            CF.rk2_step_table_into(a, b, 0.05, 1.0, 1.0, 1.0, 1.0, vs, eps4=1e-3, noise_scale=0.3,
+                                   noise_step=n, seed=2)
+            continue
+        bufs = ((state[0], state[1]), (state[2], state[3]))
         (phi, pi), (po, qo) = bufs[n % 2], bufs[(n + 1) % 2]
         RF.rk2_step_table_into(phi, pi, po, qo, 0.05, 1.0, 1.0, 1.0, 1.0, vs, noise_scale=0.3,
                                noise_step=n, seed=1)
@@ -112,24 +129,24 @@ def _time(state, table, steps, warmup):
 
 
 def tune(shape, storage="f32c", *, table_points=4096, steps=10, warmup=3, persist=True,
-         device="cuda", log=None):
+         device="cuda", log=None, field="real"):
     """Time every admissible tile shape; returns {"best": [rows, planes, stages], "ms": t,
     "default_ms": t0, "tried": n} and stores it in the cache."""
-    if storage not in ("f32c", "f64"):
-        raise ValueError("the marching kernel runs F32C and F64 storage")
+    if storage not in ("f32c", "f64") or (field == "complex" and storage != "f32c"):
+        raise ValueError("the marching kernels run F32C and F64 (real) / F32C (complex)")
     dev = torch.device(device)
-    state = _state(shape, storage, dev)
+    state = _state(shape, storage, dev, field)
     table = torch.linspace(-0.1, 0.1, table_points, dtype=torch.float64, device=dev)
     L.set_kernel_policy(2)
     try:
         L.set_march_tiles(0, 0, 0)
-        default_ms = _time(state, table, steps, warmup)
+        default_ms = _time(state, table, steps, warmup, field)
         best, best_ms, tried = None, float("inf"), 0
         t_start = time.perf_counter()
-        for c in candidates(shape):
+        for c in candidates(shape, field):
             L.set_march_tiles(*c)
             try:
-                ms = _time(state, table, steps, warmup)
+                ms = _time(state, table, steps, warmup, field)
             except L.TiptError:
                 continue
             tried += 1
@@ -146,18 +163,20 @@ def tune(shape, storage="f32c", *, table_points=4096, steps=10, warmup=3, persis
            "seconds": time.perf_counter() - t_start}
     if persist:
         c = load_cache()
-        c[cache_key(shape, storage, table_points, dev)] = res
+        c[cache_key(shape, storage, table_points, dev, field)] = res
         _save_cache(c)
     return res
 
 
-def apply(shape, storage="f32c", *, table_points=4096, tune_if_missing=False, device="cuda"):
+def apply(shape, storage="f32c", *, table_points=4096, tune_if_missing=False, device="cuda",
+          field="real"):
     """Install the cached tile shape for this workload (tuning first if asked and absent).
-    Returns the installed (rows, planes, stages), or None for the built-in heuristic."""
-    key = cache_key(shape, storage, table_points, device)
+    Returns the installed (rows, planes, stages), or None for the built-in heuristic.  The
+    tile shape is a library-wide setting: apply it before the runs of that workload."""
+    key = cache_key(shape, storage, table_points, device, field)
     entry = load_cache().get(key)
     if entry is None and tune_if_missing:
-        entry = tune(shape, storage, table_points=table_points, device=device)
+        entry = tune(shape, storage, table_points=table_points, device=device, field=field)
     if entry is None or entry["ms"] >= entry.get("default_ms", float("inf")):
         L.set_march_tiles(0, 0, 0)
         return None

@@ -256,6 +256,42 @@ int tipt_observables(int storage, const void* phi, const void* pi, int64_t nx, i
                      double thr, double* out, void* workspace, int64_t workspace_bytes,
                      void* stream);
 
+/* ------------------------------------------------------------ other integrators
+ * The reference's alternative integrators with counter-based hash noise (key
+ * of (site, noise_step) at the pass-2 multiplier, seed noise_seed).  The
+ * reference updates in place inside a parallel loop; here each sub-step reads
+ * the previous sub-step's state only (outputs must not overlap inputs).
+ * Storages F64, F32 (the reference's float32 mode), F32C; V' a 1-D table or a
+ * polynomial. */
+
+/* R:2115 overdamped_euler_step_table: phi_out = phi + dt/eta_eff F(phi) +
+ * noise_scale z, F = inv_a2 lap(phi) - V'(phi)/mu^2. */
+int tipt_overdamped_step_table(int storage, const void* phi, void* phi_out, int64_t nx,
+                               int64_t ny, int64_t nz, const tipt_step_params* sp,
+                               const tipt_vsource* vp, void* stream);
+
+/* R:1974 baoab_step_table: B A O A B with gamma = sp->eta_eff, c1 = exp(-gamma dt),
+ * c2 = sqrt(1 - c1^2) noise_scale; two launches (the second updates pi_out in
+ * place). */
+int tipt_baoab_step_table(int storage, const void* phi, const void* pi, void* phi_out,
+                          void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                          const tipt_step_params* sp, const tipt_vsource* vp, void* stream);
+
+/* C:2422 / C:2223: the same for the complex field (V'(rho) projected, Z_N and
+ * eps Re Phi^4 from ct; the two components take the cosine and sine branches
+ * of one Box-Muller pair). */
+int tipt_complex_overdamped_step_table(int storage, const void* phi1, const void* phi2,
+                                       void* phi1_out, void* phi2_out, int64_t nx, int64_t ny,
+                                       int64_t nz, const tipt_step_params* sp,
+                                       const tipt_vsource* vp, const tipt_complex_terms* ct,
+                                       void* stream);
+int tipt_complex_baoab_step_table(int storage, const void* phi1, const void* phi2,
+                                  const void* pi1, const void* pi2, void* phi1_out,
+                                  void* phi2_out, void* pi1_out, void* pi2_out, int64_t nx,
+                                  int64_t ny, int64_t nz, const tipt_step_params* sp,
+                                  const tipt_vsource* vp, const tipt_complex_terms* ct,
+                                  void* stream);
+
 /* ------------------------------------------------------------ surrogate network
  * No reference counterpart (the reference estimates nucleation only by running
  * lattices).  A 6 -> 128 -> 128 -> 128 -> 17 SiLU network maps normalised

@@ -1,0 +1,119 @@
+"""BAOAB and overdamped Euler-Maruyama kernels (real and complex field, three
+storages) against the oracle's simultaneous-update restatement, with hash noise."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+from oracle import integrators as I  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+from thermal_inflation_phase_transition_b200 import complex_field as CF  # noqa: E402
+from thermal_inflation_phase_transition_b200 import real_field as RF  # noqa: E402
+
+DEV = "cuda"
+SHAPE = (6, 20, 18)
+DT, DX, MU, IA2, GAMMA, ETA, NS = 0.05, 0.9, 1.1, 0.95, 0.8, 1.3, 0.3
+
+
+def _table():
+    tab, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.01), 0.0, 4.0, 4096)
+    return tab, tmin, dinv, 4096
+
+
+def _dev(a, storage):
+    t = torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+    if storage == "f32c":
+        return RF.to_f32c(t)
+    return t.float() if storage == "f32" else t
+
+
+def _host(t, storage):
+    if storage == "f32c":
+        return RF.from_f32c(t).cpu().numpy()
+    return t.double().cpu().numpy()
+
+
+TOL = {"f64": 1e-12, "f32": 3e-6, "f32c": 2e-6}
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f32c"])
+def test_real_overdamped(storage):
+    tab, tmin, dinv, npts = _table()
+    rng = np.random.default_rng(3)
+    phi0 = rng.normal(0.4, 0.6, SHAPE)
+    ref = phi0
+    phi = _dev(phi0, storage)
+    tabd = torch.from_numpy(tab).to(DEV)
+    for n in range(3):
+        ref = I.overdamped_step_table(ref, DT, DX, ETA, MU, IA2, tab, tmin, dinv, npts, NS, n, seed=4)
+        RF.overdamped_euler_step_table(phi, DT, DX, ETA, MU, IA2, tabd, tmin, dinv, npts, NS, n,
+                                       hash_seed=4)
+    torch.cuda.synchronize()
+    got = _host(phi, storage)
+    assert np.abs(got - ref).max() <= TOL[storage] * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f32c"])
+def test_real_baoab(storage):
+    tab, tmin, dinv, npts = _table()
+    rng = np.random.default_rng(4)
+    phi0, pi0 = rng.normal(0.4, 0.6, SHAPE), rng.normal(0.0, 0.3, SHAPE)
+    rp, rq = phi0, pi0
+    phi, pi = _dev(phi0, storage), _dev(pi0, storage)
+    tabd = torch.from_numpy(tab).to(DEV)
+    for n in range(3):
+        rp, rq = I.baoab_step_table(rp, rq, DT, DX, GAMMA, MU, IA2, tab, tmin, dinv, npts, NS, n,
+                                    seed=5)
+        RF.baoab_step_table(phi, pi, DT, DX, GAMMA, MU, IA2, tabd, tmin, dinv, npts, NS, n,
+                            hash_seed=5)
+    torch.cuda.synchronize()
+    for t, r in ((phi, rp), (pi, rq)):
+        assert np.abs(_host(t, storage) - r).max() <= TOL[storage] * np.abs(r).max()
+
+
+@pytest.mark.parametrize("zn", [(0.0, 0.0, 0.0), (4.0, 0.01, 1.0)])
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_complex_baoab_and_overdamped(storage, zn):
+    tab, tmin, dinv, npts = _table()
+    rng = np.random.default_rng(5)
+    cs = (5, 18, 17)
+    f0 = [rng.normal(0.5, 0.6, cs) for _ in range(2)] + [rng.normal(0.0, 0.3, cs) for _ in range(2)]
+    tabd = torch.from_numpy(tab).to(DEV)
+    ref = list(f0)
+    dev = [_dev(a, storage) for a in f0]
+    for n in range(2):
+        ref = list(I.complex_baoab_step_table(*ref, DT, DX, GAMMA, MU, IA2, tab, tmin, dinv, npts,
+                                              NS, n, seed=6, zn=zn))
+        CF.baoab_step_table(*dev, DT, DX, GAMMA, MU, IA2, tabd, tmin, dinv, npts, NS, n, zn=zn,
+                            hash_seed=6)
+    ro = list(f0[:2])
+    od = [_dev(a, storage) for a in f0[:2]]
+    for n in range(2):
+        ro = list(I.complex_overdamped_step_table(*ro, DT, DX, ETA, MU, IA2, tab, tmin, dinv, npts,
+                                                  NS, n, seed=6, zn=zn))
+        CF.overdamped_euler_step_table(*od, DT, DX, ETA, MU, IA2, tabd, tmin, dinv, npts, NS, n,
+                                       zn=zn, hash_seed=6)
+    torch.cuda.synchronize()
+    tol = 1e-12 if storage == "f64" else (5e-5 if zn[2] else 5e-6)
+    for t, r in list(zip(dev, ref)) + list(zip(od, ro)):
+        assert np.abs(_host(t, storage) - r).max() <= tol * np.abs(r).max()
+
+
+def test_baoab_without_noise_conserves_energy_at_zero_friction():
+    """gamma -> 0, no noise: BAOAB is velocity Verlet, which keeps the energy of a
+    harmonic lattice bounded (relative change < 1e-2 over 200 steps)."""
+    from thermal_inflation_phase_transition_b200.observables import observables
+    rng = np.random.default_rng(8)
+    phi = torch.from_numpy(rng.normal(0, 0.1, (16, 16, 16))).to(DEV)
+    pi = torch.zeros_like(phi)
+    e = []
+    for n in range(200):
+        RF.baoab_step_table(phi, pi, 0.05, 1.0, 1e-12, 1.0, 1.0, None, 0.0, 1.0, 2, 0.0, n,
+                            vpoly=(0.5, 0.0, 0.0))
+        o = observables(phi, pi).cpu().numpy()
+        # E = kin + grad + 0.25 phi^2 (V = 0.25 phi^2 for V' = 0.5 phi)
+        e.append(o[0] + o[1] + 0.25 * o[4])
+    e = np.array(e)
+    assert np.abs(e / e[0] - 1).max() < 1e-2

@@ -83,6 +83,16 @@ _SIGS = {
     "tipt_observables_workspace_size": [_i64, _i64, _i64],
     "tipt_observables": [_i, _p, _p, _i64, _i64, _i64, _d, _d, _d, _d, _d, _d, _p, _p, _i64,
                          _p],
+    "tipt_overdamped_step_table": [_i, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
+                                   C.POINTER(VSource), _p],
+    "tipt_baoab_step_table": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
+                              C.POINTER(VSource), _p],
+    "tipt_complex_overdamped_step_table": [_i, _p, _p, _p, _p, _i64, _i64, _i64,
+                                           C.POINTER(StepParams), C.POINTER(VSource),
+                                           C.POINTER(ComplexTerms), _p],
+    "tipt_complex_baoab_step_table": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
+                                      C.POINTER(StepParams), C.POINTER(VSource),
+                                      C.POINTER(ComplexTerms), _p],
     "tipt_mlp_param_count": [],
     "tipt_mlp_set_policy": [_i],
     "tipt_mlp_workspace_size": [_i64],

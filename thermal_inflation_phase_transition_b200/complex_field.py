@@ -14,7 +14,7 @@ from __future__ import annotations
 import torch
 
 from . import _lib as L
-from ._common import (dims_of, need_cuda, ptr, same_layout, step_params, storage_of,
+from ._common import (dims_of, need_cuda, poly_source, ptr, same_layout, step_params, storage_of,
                       stream_handle, swap_storage, table_source)
 
 
@@ -56,6 +56,52 @@ def rk2_step_table_into(state, out, dt, dx, eta_eff, mu, inv_a2, vsource, *, zn=
     ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
     L.call("tipt_complex_rk2_step_table", st, *[ptr(a) for a in state], *[ptr(a) for a in out],
            nx, ny, nz, sp, vsource, ct, None, None, stream_handle(stream))
+
+
+def _vsource_1d(vp_table, vp_tmin, vp_dinv, vp_npts, vpoly):
+    if vpoly is not None:
+        return poly_source(*[float(c) for c in vpoly])
+    return table_source(vp_table, vp_tmin, vp_dinv, vp_npts)
+
+
+def overdamped_euler_step_table(phi1, phi2, dt, dx, eta_eff, mu, inv_a2, vp_table, vp_tmin,
+                                vp_dinv, vp_npts, noise_scale, seed, *, tmp=None,
+                                zn=(0.0, 0.0, 0.0), eps4=0.0, hash_seed=0, vpoly=None):
+    """C:2422 overdamped_euler_step_table (complex), in place; ``seed`` is the hash noise
+    step (the reference's per-step seed); ``tmp`` = two scratch fields (allocated when
+    not given)."""
+    st = storage_of(phi1)
+    need_cuda(phi1, phi2, names=["phi1", "phi2"])
+    t = tmp if tmp is not None else [torch.empty_like(phi1), torch.empty_like(phi2)]
+    same_layout(phi1, phi2, *t, names=["phi2", "tmp1", "tmp2"])
+    nx, ny, nz = dims_of(phi1)
+    vs = _vsource_1d(vp_table, vp_tmin, vp_dinv, vp_npts, vpoly)
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, seed, hash_seed)
+    ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
+    L.call("tipt_complex_overdamped_step_table", st, ptr(phi1), ptr(phi2), ptr(t[0]), ptr(t[1]),
+           nx, ny, nz, sp, vs, ct, stream_handle())
+    swap_storage(phi1, t[0])
+    swap_storage(phi2, t[1])
+
+
+def baoab_step_table(phi1, phi2, pi1, pi2, dt, dx, gamma, mu, inv_a2, vp_table, vp_tmin, vp_dinv,
+                     vp_npts, noise_scale, seed, *, tmp=None, zn=(0.0, 0.0, 0.0), eps4=0.0,
+                     hash_seed=0, vpoly=None):
+    """C:2223 baoab_step_table (complex): one BAOAB step in place; ``tmp`` = four scratch
+    fields (allocated when not given)."""
+    st = storage_of(phi1)
+    arrs = (phi1, phi2, pi1, pi2)
+    need_cuda(*arrs, names=["phi1", "phi2", "pi1", "pi2"])
+    t = tmp if tmp is not None else [torch.empty_like(a) for a in arrs]
+    same_layout(phi1, *arrs[1:], *t, names=["phi2", "pi1", "pi2", "t1", "t2", "t3", "t4"])
+    nx, ny, nz = dims_of(phi1)
+    vs = _vsource_1d(vp_table, vp_tmin, vp_dinv, vp_npts, vpoly)
+    sp = step_params(dt, dx, gamma, mu, inv_a2, noise_scale, seed, hash_seed)
+    ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
+    L.call("tipt_complex_baoab_step_table", st, *[ptr(a) for a in arrs], *[ptr(a) for a in t],
+           nx, ny, nz, sp, vs, ct, stream_handle())
+    for a, b in zip(arrs, t):
+        swap_storage(a, b)
 
 
 class WindingResult:

@@ -139,6 +139,53 @@ def rk2_fused_single_pass(phi, pi, dt, dx, eta_eff, T, T_mid, mu, lam, mphi, bos
            ptr(pi_tmp), nx, ny, nz, sp, v, v, None, stream_handle())
 
 
+def _vsource_1d(vp_table, vp_tmin, vp_dinv, vp_npts, vpoly):
+    if vpoly is not None:
+        return poly_source(*[float(c) for c in vpoly])
+    return table_source(vp_table, vp_tmin, vp_dinv, vp_npts)
+
+
+def overdamped_euler_step_table(phi, dt, dx, eta_eff, mu, inv_a2, vp_table, vp_tmin, vp_dinv,
+                                vp_npts, noise_scale, seed, *, phi_tmp=None, hash_seed=0,
+                                vpoly=None):
+    """R:2115 overdamped_euler_step_table: phi += dt/eta_eff F(phi) + noise_scale z, in place.
+
+    ``seed`` is the reference's per-step seed (the step number): here it is the hash
+    noise step; ``hash_seed`` selects an independent stream.  The update is simultaneous
+    over the lattice (the new field goes to ``phi_tmp``, then the storages swap);
+    ``phi_tmp`` is allocated when not given.  ``vpoly = (c1, c2, c3)`` replaces the
+    table by V' = c1 phi + c2 phi^2 + c3 phi^3."""
+    st = storage_of(phi)
+    need_cuda(phi, names=["phi"])
+    tmp = torch.empty_like(phi) if phi_tmp is None else phi_tmp
+    same_layout(phi, tmp, names=["phi_tmp"])
+    nx, ny, nz = dims_of(phi)
+    vs = _vsource_1d(vp_table, vp_tmin, vp_dinv, vp_npts, vpoly)
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, seed, hash_seed)
+    L.call("tipt_overdamped_step_table", st, ptr(phi), ptr(tmp), nx, ny, nz, sp, vs,
+           stream_handle())
+    swap_storage(phi, tmp)
+
+
+def baoab_step_table(phi, pi, dt, dx, gamma, mu, inv_a2, vp_table, vp_tmin, vp_dinv, vp_npts,
+                     noise_scale, seed, *, phi_tmp=None, pi_tmp=None, hash_seed=0, vpoly=None):
+    """R:1974 baoab_step_table: one BAOAB step of (phi, pi) in place (B A O A B,
+    c1 = exp(-gamma dt), c2 = sqrt(1 - c1^2) noise_scale); arguments as
+    overdamped_euler_step_table."""
+    st = storage_of(phi)
+    need_cuda(phi, pi, names=["phi", "pi"])
+    pt = torch.empty_like(phi) if phi_tmp is None else phi_tmp
+    qt = torch.empty_like(pi) if pi_tmp is None else pi_tmp
+    same_layout(phi, pi, pt, qt, names=["pi", "phi_tmp", "pi_tmp"])
+    nx, ny, nz = dims_of(phi)
+    vs = _vsource_1d(vp_table, vp_tmin, vp_dinv, vp_npts, vpoly)
+    sp = step_params(dt, dx, gamma, mu, inv_a2, noise_scale, seed, hash_seed)
+    L.call("tipt_baoab_step_table", st, ptr(phi), ptr(pi), ptr(pt), ptr(qt), nx, ny, nz, sp, vs,
+           stream_handle())
+    swap_storage(phi, pt)
+    swap_storage(pi, qt)
+
+
 def compute_energy_densities(phi, pi, dx, inv_a2, lam_val, mphi_val, mu):
     """R:2270 compute_energy_densities -> (E_kin, E_grad, E_pot) as Python floats."""
     from .observables import observables

@@ -159,6 +159,35 @@ class Simulation:
             return t.double()
         return f64(self.phi[0]), f64(self.pi[0])
 
+    # ------------------------------------------------------- checkpoints
+    def snapshot(self, writer, *, energy_params=None):
+        """Save the current state through a ``snapshots.SnapshotWriter`` in the
+        reference's layout (R:3997-4018): labelled with the index n of the last step
+        applied, time n dt, and that step's T; ``pi`` on the writer's checkpoint
+        cadence.  ``energy_params = (lam, mphi)`` adds E_kin, E_grad, E_pot."""
+        n = self.steps_done - 1
+        T = float(self.schedule[min(max(n, 0), self.schedule.shape[0] - 1), 0])
+        en = None
+        if energy_params is not None:
+            from .observables import observables
+            lam, mphi = energy_params
+            o = observables(self.phi[0], self.pi[0], dx=self.dx, inv_a2=self.inv_a2, lam=lam,
+                            mphi=mphi, mu=self.mu).tolist()
+            en = (o[0], o[1], o[2])
+        return writer.save_real(n, n * self.dt, T, self.phi[0], self.pi[0], energies=en)
+
+    def resume(self, ckpt):
+        """Continue from a checkpoint (the dict of ``snapshots.latest_checkpoint``): the
+        fields are copied into the current buffers (captured graphs stay valid) and the
+        next step is the one after the saved step.  (The reference restarts its loop at
+        the saved step index, applying that step a second time.)"""
+        from .snapshots import load_fields
+        phi, pi = load_fields(ckpt, ["phi", "pi"], self.storage, self.dev)
+        self.phi[0].copy_(phi.reshape(self.phi[0].shape))
+        self.pi[0].copy_(pi.reshape(self.pi[0].shape))
+        self.steps_done = int(ckpt["step"]) + 1
+        self._counter.fill_(self.steps_done)
+
     # ------------------------------------------------------------ stepping
     def _st(self):
         return {"f64": L.TIPT_F64, "f32": L.TIPT_F32, "f32c": L.TIPT_F32C}[self.storage]

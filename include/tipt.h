@@ -292,6 +292,28 @@ int tipt_complex_baoab_step_table(int storage, const void* phi1, const void* phi
                                   const tipt_vsource* vp, const tipt_complex_terms* ct,
                                   void* stream);
 
+/* ------------------------------------------------------------ labelling
+ * Connected components of |field| > threshold (face neighbours, open or
+ * periodic lattice), numbered 1..n in raster order of each component's first
+ * site: the label array of scipy.ndimage.label, which the reference's
+ * post-processing uses for bubbles and string voxels
+ * (postprocess/revisualize_snapshots.py:171-214, :360-392). */
+int64_t tipt_label_workspace_size(int64_t nx, int64_t ny, int64_t nz);
+
+/* labels[N] (int32, 0 = background) and *n_labels (device int32). */
+int tipt_label_components(int storage, const void* field, double threshold, int64_t nx,
+                          int64_t ny, int64_t nz, int periodic, int32_t* labels,
+                          int32_t* n_labels, void* workspace, int64_t workspace_bytes,
+                          void* stream);
+
+/* Per-label sums over the sites of each label l in 1..n_labels (arrays of
+ * n_labels + 1 entries, entry 0 unused): site count, sum of (i, j, k), sum of
+ * i^2 + j^2 + k^2, sum of the field value and the largest |value| (field may
+ * be NULL: value 0). */
+int tipt_label_stats(int storage, const void* field, const int32_t* labels, int64_t nx,
+                     int64_t ny, int64_t nz, int32_t n_labels, int64_t* count, int64_t* sum_xyz,
+                     int64_t* sum_sq, double* sum_val, double* max_abs, void* stream);
+
 /* ------------------------------------------------------------ surrogate network
  * No reference counterpart (the reference estimates nucleation only by running
  * lattices).  A 6 -> 128 -> 128 -> 128 -> 17 SiLU network maps normalised

@@ -93,6 +93,9 @@ _SIGS = {
     "tipt_complex_baoab_step_table": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
                                       C.POINTER(StepParams), C.POINTER(VSource),
                                       C.POINTER(ComplexTerms), _p],
+    "tipt_label_workspace_size": [_i64, _i64, _i64],
+    "tipt_label_components": [_i, _p, _d, _i64, _i64, _i64, _i, _p, _p, _p, _i64, _p],
+    "tipt_label_stats": [_i, _p, _p, _i64, _i64, _i64, C.c_int32, _p, _p, _p, _p, _p, _p],
     "tipt_mlp_param_count": [],
     "tipt_mlp_set_policy": [_i],
     "tipt_mlp_workspace_size": [_i64],
@@ -106,7 +109,8 @@ _SIGS = {
 }
 _RESTYPE = {"tipt_version": C.c_char_p, "tipt_status_string": C.c_char_p,
             "tipt_last_error": C.c_char_p, "tipt_observables_workspace_size": C.c_int64,
-            "tipt_mlp_param_count": C.c_int64, "tipt_mlp_workspace_size": C.c_int64}
+            "tipt_mlp_param_count": C.c_int64, "tipt_mlp_workspace_size": C.c_int64,
+            "tipt_label_workspace_size": C.c_int64}
 
 _lib = None
 

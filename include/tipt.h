@@ -292,6 +292,37 @@ int tipt_complex_baoab_step_table(int storage, const void* phi1, const void* phi
                                   const tipt_vsource* vp, const tipt_complex_terms* ct,
                                   void* stream);
 
+/* ------------------------------------------------------------ thermal V'
+ * The physics-default thermal potential (R:432-496, R:755-849, R:1415-1485):
+ * V'(phi, T) = lam phi^3 - mphi^2 phi + T^4/(2 pi^2) (cb dJ_B(u_b) du_b/dphi +
+ * cf dJ_F(u_f) du_f/dphi), u_b = sqrt(mB^2 + gb^2 phi^2 / 2 + (gb^2/4 + 2 gg^2/3) T^2) / T,
+ * u_f = sqrt(gf^2 phi^2 / 2 + gfg^2 T^2 / 6) / T, dJ from cubic splines on a
+ * uniform u grid. */
+typedef struct {
+    double lam, mphi, boson_mass_sq;
+    double boson_coupling, boson_gauge_coupling, fermion_coupling, fermion_gauge_coupling;
+    double coeff_b, coeff_f;  /* the reference's _POT_COEFFS */
+    double x_min, h;          /* spline grid: u_i = x_min + i h, i = 0..nseg */
+    int32_t nseg, pad_;
+    const double* spline;     /* device [8][nseg]: dx^3, dx^2, dx, 1 coefficients of dJ_B, then dJ_F */
+} tipt_thermal;
+
+/* dJ_B (fermion = 0) or dJ_F (1) at the n device points u (FP64 quadrature,
+ * composite 16-point Gauss-Legendre; gl_nodes / gl_weights are HOST arrays of
+ * the 16 nodes and weights on [-1, 1]); with x_cut > 0 the lattice
+ * counterterm's soft-mode part (R:461-490) is subtracted. */
+int tipt_thermal_dj(int fermion, const double* u, int32_t n, const double* gl_nodes,
+                    const double* gl_weights, double x_cut, double* out, void* stream);
+
+/* R:1435 Vprime_field: out[N] (FP64) = V'(phi, T) per site. */
+int tipt_thermal_vprime_field(int storage, const void* phi, double T, const tipt_thermal* tp,
+                              double* out, int64_t nx, int64_t ny, int64_t nz, void* stream);
+
+/* R:805-849 build_vprime_table on a (phi, T) grid: out[nT][nphi] = V'(phi_i, T_j),
+ * phi_i = linspace(phi_lo, phi_hi, nphi), T_j from the device array Ts. */
+int tipt_thermal_vprime_table(double phi_lo, double phi_hi, int32_t nphi, const double* Ts,
+                              int32_t nT, const tipt_thermal* tp, double* out, void* stream);
+
 /* ------------------------------------------------------------ labelling
  * Connected components of |field| > threshold (face neighbours, open or
  * periodic lattice), numbered 1..n in raster order of each component's first

@@ -36,6 +36,15 @@ class StepParams(C.Structure):
                 ("noise_step", C.c_uint64), ("noise_seed", C.c_uint64)]
 
 
+class Thermal(C.Structure):
+    _fields_ = [("lam", C.c_double), ("mphi", C.c_double), ("boson_mass_sq", C.c_double),
+                ("boson_coupling", C.c_double), ("boson_gauge_coupling", C.c_double),
+                ("fermion_coupling", C.c_double), ("fermion_gauge_coupling", C.c_double),
+                ("coeff_b", C.c_double), ("coeff_f", C.c_double), ("x_min", C.c_double),
+                ("h", C.c_double), ("nseg", C.c_int32), ("pad_", C.c_int32),
+                ("spline", C.c_void_p)]
+
+
 class Replica(C.Structure):
     _fields_ = [("n0", C.c_int32), ("n1", C.c_int32), ("n2", C.c_int32), ("m1", C.c_uint32),
                 ("m2", C.c_uint32), ("pad_", C.c_int32), ("offset", C.c_int64),
@@ -93,6 +102,9 @@ _SIGS = {
     "tipt_complex_baoab_step_table": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
                                       C.POINTER(StepParams), C.POINTER(VSource),
                                       C.POINTER(ComplexTerms), _p],
+    "tipt_thermal_dj": [_i, _p, C.c_int32, _p, _p, _d, _p, _p],
+    "tipt_thermal_vprime_field": [_i, _p, _d, C.POINTER(Thermal), _p, _i64, _i64, _i64, _p],
+    "tipt_thermal_vprime_table": [_d, _d, C.c_int32, _p, C.c_int32, C.POINTER(Thermal), _p, _p],
     "tipt_label_workspace_size": [_i64, _i64, _i64],
     "tipt_label_components": [_i, _p, _d, _i64, _i64, _i64, _i, _p, _p, _p, _i64, _p],
     "tipt_label_stats": [_i, _p, _p, _i64, _i64, _i64, C.c_int32, _p, _p, _p, _p, _p, _p],

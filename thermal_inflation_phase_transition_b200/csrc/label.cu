@@ -246,6 +246,16 @@ int64_t label_workspace_bytes(int64_t N) {
     return 4 * (2 * N + chunks + 64);
 }
 
+// Read (and optionally clear) the labeller's status word.
+int label_status(int* status, int clear) {
+    cudaError_t e = cudaMemcpyFromSymbol(status, g_label_status, sizeof(int));
+    if (e == cudaSuccess && clear) {
+        const int zero = 0;
+        e = cudaMemcpyToSymbol(g_label_status, &zero, sizeof(int));
+    }
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "label status");
+}
+
 }  // namespace tipt
 
 using namespace tipt;

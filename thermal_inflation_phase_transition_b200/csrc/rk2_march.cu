@@ -1001,9 +1001,12 @@ extern "C" int tipt_device_status(int* status, int clear) {
         e = cudaMemcpyToSymbol(g_device_status, &zero, sizeof(int));
         if (e != cudaSuccess) return fail_cuda(e, "clear device status");
     }
-    int mlp = 0;
-    const int rc = mlp_status(&mlp, clear);
+    int other = 0;
+    int rc = mlp_status(&other, clear);
     if (rc) return rc;
-    if (!*status) *status = mlp;
+    if (!*status) *status = other;
+    other = 0;
+    if ((rc = label_status(&other, clear))) return rc;
+    if (!*status) *status = other;
     return TIPT_OK;
 }

@@ -35,6 +35,8 @@ int kernel_policy();
 
 // Status word of the surrogate kernels' bounded waits (TIPT_ERR_TIMEOUT or 0).
 int mlp_status(int* status, int clear);
+// Status word of the labeller's bounded union-find loops.
+int label_status(int* status, int clear);
 
 struct RealStageParams;
 int launch_real_stage(int storage, RealStageParams p, cudaStream_t st);

@@ -399,6 +399,10 @@ int tipt_set_kernel_policy(int policy);
  * stages (each 0 = automatic).  Performance only; used by the autotuner. */
 int tipt_set_march_tiles(int rows, int planes, int stages);
 
+/* Row segment of the complex marching kernel (sites per segment, a divisor of
+ * nz of at least 128; 0 = automatic).  Performance only; used by the autotuner. */
+int tipt_set_march_kseg(int kseg);
+
 /* Device status word set by bounded device-side waits that expired
  * (TIPT_ERR_TIMEOUT), 0 otherwise; clear != 0 resets it.  Synchronises the
  * device.  Counterpart of the reference's host NaN/divergence guard in spirit

@@ -64,4 +64,6 @@ def test_tune_complex_field(tmp_path, monkeypatch):
     cache = json.load(open(tmp_path / "tune.json"))
     assert AT.cache_key(shape, "f32c", 4096, field="complex") in cache
     assert AT.cache_key(shape, "f32c", 4096) not in cache
-    assert all((tj * 32) % 32 == 0 for tj, _, _ in AT.candidates(shape, "complex"))
+    cands = AT.candidates(shape, "complex")
+    assert all(len(c) == 4 and 64 % c[3] == 0 for c in cands)
+    assert {c[3] for c in AT.candidates((8, 16, 512), "complex")} == {128, 256, 512}

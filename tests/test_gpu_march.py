@@ -22,6 +22,7 @@ def _reset_policy():
     yield
     L.set_kernel_policy(0)
     L.set_march_tiles(0, 0, 0)
+    L.set_march_kseg(0)
 
 
 def _state(shape, storage, seed):
@@ -140,9 +141,10 @@ def _cstate(shape, seed):
     return [RF.to_f32c(a) for a in f]
 
 
-def _crun(policy, shape, steps=3, tiles=(0, 0, 0), poly=False, eps4=1e-3):
+def _crun(policy, shape, steps=3, tiles=(0, 0, 0), poly=False, eps4=1e-3, kseg=0):
     L.set_kernel_policy(policy)
     L.set_march_tiles(*tiles)
+    L.set_march_kseg(kseg)
     a = _cstate(shape, 5)
     b = [torch.empty_like(x) for x in a]
     if poly:
@@ -208,3 +210,16 @@ def test_complex_march_vs_oracle():
     for a, r in zip(st, ref):
         got = RF.from_f32c(a).cpu().numpy()
         assert np.abs(got - r).max() <= 5e-6 * np.abs(r).max()
+
+
+@pytest.mark.parametrize("shape,kseg,tiles", [((4, 8, 512), 0, (0, 0, 0)),
+                                              ((4, 8, 512), 128, (2, 2, 4)),
+                                              ((5, 16, 256), 128, (4, 3, 3)),
+                                              ((3, 6, 256), 128, (2, 1, 5)),
+                                              ((6, 8, 384), 128, (0, 0, 0))])
+def test_complex_march_row_segments_equal_generic(shape, kseg, tiles):
+    """Rows split into segments whose end neighbours come from the halo boxes."""
+    a = _crun(1, shape)
+    b = _crun(2, shape, tiles=tiles, kseg=kseg)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)

@@ -117,6 +117,7 @@ _SIGS = {
                       C.c_float, C.c_float, _p],
     "tipt_set_kernel_policy": [_i],
     "tipt_set_march_tiles": [_i, _i, _i],
+    "tipt_set_march_kseg": [_i],
     "tipt_device_status": [C.POINTER(C.c_int), _i],
 }
 _RESTYPE = {"tipt_version": C.c_char_p, "tipt_status_string": C.c_char_p,
@@ -168,6 +169,11 @@ def set_kernel_policy(policy: int) -> None:
 def set_march_tiles(rows: int = 0, planes: int = 0, stages: int = 0) -> None:
     """Marching-kernel tile shape (0 = automatic); performance only."""
     call("tipt_set_march_tiles", int(rows), int(planes), int(stages))
+
+
+def set_march_kseg(kseg: int) -> None:
+    """Row segment of the complex marching kernel (0 = automatic; tests/tuning)."""
+    call("tipt_set_march_kseg", int(kseg))
 
 
 def device_status(clear: bool = False) -> int:

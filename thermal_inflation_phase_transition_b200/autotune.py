@@ -1,8 +1,9 @@
 """Tile-shape autotuner of the marching stage kernels, with a persisted JSON cache.
 
 A marching kernel's tile is (rows per tile, planes per work item, ring
-stages); ``field="real"`` tunes the real-field kernel, ``field="complex"`` the
-complex-field one (compensated FP32).  The built-in heuristic scores candidates by occupancy and halo share;
+stages), plus the row segment for the complex kernel; ``field="real"`` tunes
+the real-field kernel, ``field="complex"`` the complex-field one (compensated
+FP32).  The built-in heuristic scores candidates by occupancy and halo share;
 ``tune`` instead times every admissible candidate on the device (CUDA events,
 inputs larger than L2 where the lattice is) and keeps the fastest.  Results are
 cached per (GPU name, field, storage, lattice shape, V' table size) in a JSON file
@@ -65,24 +66,28 @@ def _save_cache(c: dict) -> None:
 
 
 def candidates(shape, field="real"):
-    """(rows, planes, stages) the kernel may accept for this lattice (the kernel still
+    """Tile shapes the kernel may accept for this lattice: (rows, planes, stages) for the
+    real kernel, (rows, planes, stages, row segment) for the complex one (the kernel still
     rejects those that do not fit shared memory)."""
     nx, ny, nz = shape
     if field == "real":
         n0, n1, n2 = (1, nx, ny) if nz == 1 else (nx, ny, nz)
-        tpr = n2 // 4
+        segs, planes = [None], PLANES
     else:
         n0, n1, n2 = nx, ny, nz
-        tpr = n2 // 2
+        segs = [n2] + [k for k in range(n2 - 1, 127, -1) if n2 % k == 0 and k % 32 == 0]
+        planes = (32, 64, 128, 256)
     out = []
-    for tj in range(1, 65):
-        if n1 % tj or (tj * tpr) % 32 or tj * tpr > 512:
-            continue
-        for ci in PLANES:
-            if ci > n0 and ci != PLANES[0]:
+    for ks in segs:
+        tpr = n2 // 4 if ks is None else ks // 2
+        for tj in range(1, 65):
+            if n1 % tj or (tj * tpr) % 32 or tj * tpr > 512:
                 continue
-            for st in STAGES:
-                out.append((tj, ci, st))
+            for ci in planes:
+                if ci > n0 and ci != planes[0]:
+                    continue
+                for st in STAGES:
+                    out.append((tj, ci, st) if ks is None else (tj, ci, st, ks))
     return out
 
 
@@ -144,18 +149,20 @@ def tune(shape, storage="f32c", *, table_points=4096, steps=10, warmup=3, persis
         best, best_ms, tried = None, float("inf"), 0
         t_start = time.perf_counter()
         for c in candidates(shape, field):
-            L.set_march_tiles(*c)
+            L.set_march_tiles(*c[:3])
+            L.set_march_kseg(c[3] if len(c) > 3 else 0)
             try:
                 ms = _time(state, table, steps, warmup, field)
             except L.TiptError:
                 continue
             tried += 1
             if log:
-                log(f"  rows={c[0]} planes={c[1]} stages={c[2]}: {ms:.4f} ms")
+                log(f"  tile {c}: {ms:.4f} ms")
             if ms < best_ms:
                 best, best_ms = c, ms
     finally:
         L.set_march_tiles(0, 0, 0)
+        L.set_march_kseg(0)
         L.set_kernel_policy(0)
     if best is None:
         raise RuntimeError(f"no marching tile shape accepted for {shape} {storage}")
@@ -179,6 +186,9 @@ def apply(shape, storage="f32c", *, table_points=4096, tune_if_missing=False, de
         entry = tune(shape, storage, table_points=table_points, device=device, field=field)
     if entry is None or entry["ms"] >= entry.get("default_ms", float("inf")):
         L.set_march_tiles(0, 0, 0)
+        L.set_march_kseg(0)
         return None
-    L.set_march_tiles(*entry["best"])
-    return tuple(entry["best"])
+    b = entry["best"]
+    L.set_march_tiles(*b[:3])
+    L.set_march_kseg(b[3] if len(b) > 3 else 0)
+    return tuple(b)

@@ -91,6 +91,10 @@ struct MarchGeom {
     int items;
     int tab_bytes;    // staged V' row (bytes, 128-aligned)
     int stage_bytes;  // one ring stage: phi and pi tiles
+    // complex kernel: rows split into nKS segments of KS sites (with nKS > 1 the
+    // k-1 / k+1 neighbours of a segment's end sites are copied by the edge
+    // threads); halo_off = bytes of the eight plane blocks of a stage
+    int KS, nKS, halo_off;
 };
 
 template <int S>
@@ -540,9 +544,12 @@ __global__ void __maxnreg__(kMarchRegs)
     const int TJ = g.TJ;
     const uint32_t NS = (uint32_t)g.S;
     const int rows = TJ + 2;
-    const int tpr = n2 >> 1;
+    const int KS = g.KS;
+    const bool split = g.nKS > 1;
+    const int tpr = KS >> 1;
     const int nc = TJ * tpr;
     const int t = threadIdx.x;
+    const int nJK = g.nJB * g.nKS;
 
     if (t == 0) {
         for (uint32_t s = 0; s < NS; ++s) {
@@ -555,24 +562,32 @@ __global__ void __maxnreg__(kMarchRegs)
         for (int q = t; q < p.npts; q += blockDim.x) s_tab[q] = (float)__ldg(p.table + q);
     __syncthreads();
 
-    const size_t plane_blk = (size_t)(g.stage_bytes >> 3);  // one [rows][pitch] block, bytes
+    const size_t plane_blk = (size_t)((g.halo_off) >> 3);  // one [rows][pitch] block, bytes
     // stage -> field f (phi1, phi2, pi1, pi2) -> component c (0 hi, 1 lo)
     auto blk = [&](uint32_t stage, int f, int c) -> float* {
         return reinterpret_cast<float*>(ring + (size_t)stage * g.stage_bytes +
                                         (size_t)(2 * f + c) * plane_blk);
     };
+    // split rows: the k-1 neighbour of a segment's first site and the k+1 neighbour of its
+    // last site are copied from global memory by the two edge threads of each tile row
+    // (cp.async, one plane ahead) into a per-thread double buffer after the ring:
+    // [TJ rows][2 sides][2 slots][8 = field x component]
+    float* halo = reinterpret_cast<float*>(ring + (size_t)NS * g.stage_bytes);
 
     // ------------------------------------------------------------ producer
     if (t >= nc) {
         if (t != nc) return;
         const CUtensorMap* tm[4] = {&tm0, &tm1, &tm2, &tm3};
-        const uint32_t plane_tx = (uint32_t)(8 * rows * n2 * 4);
+        const uint32_t plane_tx = (uint32_t)(8 * rows * KS * 4);
         RingPos w{0, 0};
         uint32_t issued = 0;
         bool ok = true;
         for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
-            const int ic = item / g.nJB;
-            const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+            const int ic = item / nJK;
+            const int jk = item - ic * nJK;
+            const int jb = jk / g.nKS;
+            const int k0s = (jk - jb * g.nKS) * KS;
+            const int j0 = jb * TJ, i0 = ic * g.CI;
             const int npl = min(g.CI, n0 - i0) + 2;
             for (int q = 0; q < npl; ++q) {
                 if (issued >= NS && !mbar_wait(&empty[w.stage], w.phase ^ 1u)) {
@@ -585,13 +600,14 @@ __global__ void __maxnreg__(kMarchRegs)
                 for (int rr = 0; rr < rows; ++rr) {
                     int jr = j0 - 1 + rr;
                     jr = jr < 0 ? jr + n1 : (jr >= n1 ? jr - n1 : jr);
-                    for (int kb = 0; kb < n2; kb += g.BK) {
+                    for (int kb = 0; kb < KS; kb += g.BK) {
                         const int o = rr * pitch + kb;
 #pragma unroll
                         for (int f = 0; f < 4; ++f) {
                             // plane iw = hi, plane n0 + iw = lo
-                            tma_row(blk(w.stage, f, 0) + o, tm[f], kb, jr, iw, &full[w.stage]);
-                            tma_row(blk(w.stage, f, 1) + o, tm[f], kb, jr, n0 + iw, &full[w.stage]);
+                            tma_row(blk(w.stage, f, 0) + o, tm[f], k0s + kb, jr, iw, &full[w.stage]);
+                            tma_row(blk(w.stage, f, 1) + o, tm[f], k0s + kb, jr, n0 + iw,
+                                    &full[w.stage]);
                         }
                     }
                 }
@@ -612,37 +628,70 @@ __global__ void __maxnreg__(kMarchRegs)
     // ----------------------------------------------------------- consumers
     const int lane = t & 31;
     const int r = 1 + t / tpr;                 // own tile row (1..TJ)
-    const int k0 = 2 * (t - (r - 1) * tpr);    // first of the two own columns
-    const int kml = k0 == 0 ? n2 - 1 : k0 - 1;
-    const int kpr = k0 + 2 == n2 ? 0 : k0 + 2;
+    const int k0 = 2 * (t - (r - 1) * tpr);    // first of the two own columns (in the segment)
+    const bool edge_l = k0 == 0, edge_r = k0 + 2 == KS;
+    const int kml = edge_l ? KS - 1 : k0 - 1;  // unsplit rows wrap inside the row
+    const int kpr = edge_r ? 0 : k0 + 2;
     const float tminf = (float)p.tmin, dinvf = (float)p.dinv;
     const int64_t N = (int64_t)n0 * n1 * n2;
     const int orow = r * pitch, urow = (r - 1) * pitch, drow = (r + 1) * pitch;
     auto force = [&](float2 q1, float2 q2, int, float2& d1, float2& d2) {
         complex_force_v<float2>(p, s_tab, tminf, dinvf, q1, q2, d1, d2);
     };
+    const bool edge = split && (edge_l || edge_r);
+    float* my_halo = halo + ((r - 1) * 2 + (edge_r ? 1 : 0)) * 16;
+    // issue the copies of plane i's 8 halo values (row jw, column kcol) into slot
+    auto fetch_halo = [&](int i, int jw, int kcol, int slot) {
+        const int64_t off = ((int64_t)i * n1 + jw) * n2 + kcol;
+#pragma unroll
+        for (int f = 0; f < 4; ++f)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const float* src = static_cast<const float*>(p.f[f]) + (c ? N : 0) + off;
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                                 smem_addr(my_halo + slot * 8 + 2 * f + c)),
+                             "l"(src)
+                             : "memory");
+            }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
 
     RingPos pm{0, 0};
     for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
-        const int ic = item / g.nJB;
-        const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+        const int ic = item / nJK;
+        const int jk = item - ic * nJK;
+        const int jb = jk / g.nKS;
+        const int k0s = (jk - jb * g.nKS) * KS;
+        const int j0 = jb * TJ, i0 = ic * g.CI;
         const int ni = min(g.CI, n0 - i0);
         const int jw = j0 + r - 1;
         RingPos pc = pm, pp;
         pc.next(NS);
         pp = pc;
         pp.next(NS);
+        const int kcol = edge_l ? (k0s - 1 + n2) % n2 : (k0s + KS) % n2;
+        if (edge) fetch_halo(i0, jw, kcol, 0);
         if (!mbar_wait(&full[pm.stage], pm.phase) || !mbar_wait(&full[pc.stage], pc.phase)) {
             if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+            if (edge) asm volatile("cp.async.wait_all;" ::: "memory");
             return;
         }
         for (int q = 0; q < ni; ++q) {
             if (!mbar_wait(&full[pp.stage], pp.phase)) {
                 if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+                if (edge) asm volatile("cp.async.wait_all;" ::: "memory");
                 return;
             }
             const int i = i0 + q;
-            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2 + k0;
+            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2 + k0s + k0;
+            float hv[8];
+            if (edge) {
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                const float* hs = my_halo + (q & 1) * 8;
+#pragma unroll
+                for (int e = 0; e < 8; ++e) hv[e] = hs[e];
+                if (q + 1 < ni) fetch_halo(i + 1, jw, kcol, (q + 1) & 1);
+            }
             CplxIn<float2> in;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
@@ -654,7 +703,8 @@ __global__ void __maxnreg__(kMarchRegs)
                     const float2 jp = *reinterpret_cast<const float2*>(sc + drow + k0);
                     const float2 im = *reinterpret_cast<const float2*>(blk(pm.stage, f, c) + orow + k0);
                     const float2 ip = *reinterpret_cast<const float2*>(blk(pp.stage, f, c) + orow + k0);
-                    const float kl = sc[orow + kml], kr = sc[orow + kpr];
+                    const float kl = (split && edge_l) ? hv[2 * f + c] : sc[orow + kml];
+                    const float kr = (split && edge_r) ? hv[2 * f + c] : sc[orow + kpr];
                     // lanes = sites k0, k0+1; neighbours in the order ip, im, jp, jm, kp, km
                     const float2 nb[6] = {ip, im, jp, jm, make_float2(ce.y, kr), make_float2(kl, ce.x)};
                     float2 acc;
@@ -887,48 +937,69 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
 
 // Complex F32C geometry: two sites per consumer thread (tpr = n2/2 per row),
 // eight planes per ring stage; the same scoring as the real field.
+static int g_force_kseg = 0;  // complex kernel's row segment (0 = automatic)
+
+// Candidates: segments KS dividing n2 (split segments of at least 128 sites and a
+// multiple of 32), TJ with TJ*KS/2 consumers a multiple of 32 in
+// [32, 512], ring depth S in [3, 5].  Score: consumer warps per SM x TJ/(TJ+2),
+// weighted by ring depth (a 3-stage ring prefetches nothing beyond the plane in
+// use) and by segment length.
 static bool complex_geometry(const ComplexStageParams& p, MarchGeom& g, int64_t& smem) {
     const int n1 = p.n1, n2 = p.n2;
     const int es = 4, np = 8;
     if (n2 % 2 != 0 || n2 < 16 || n2 > 1024) return false;
-    g.BK = pick_bk(n2, es);
-    if (!g.BK) return false;
-    const int per128 = 128 / es;
-    g.pitch = (n2 + per128 - 1) / per128 * per128;
-    const int tpr = n2 / 2;
     g.tab_bytes = p.table_in_smem ? round128(p.npts * 4) : 0;
     g.CI = g_force_ci > 0 ? g_force_ci : 64;
     if (g.CI > p.n0) g.CI = p.n0;
     double best = -1.0;
     MarchGeom pick{};
-    for (int tj = 1; tj <= 64; ++tj) {
-        if (g_force_tj > 0 && tj != g_force_tj) continue;
-        if (n1 % tj || (tj * tpr) % 32 || tj * tpr > 512) continue;
-        for (int st = 3; st <= 5; ++st) {
-            if (g_force_stages > 0 && st != g_force_stages) continue;
-            MarchGeom c = g;
-            c.TJ = tj;
-            c.S = st;
-            c.stage_bytes = np * round128((tj + 2) * c.pitch * es);
-            if (smem_need(c) > kSmemPerCta) continue;
-            const int cps = ctas_per_sm(c, tpr);
-            if (cps < 1) continue;
-            const double score = cps * (tj * tpr / 32) * (double)tj / (tj + 2) + 0.01 * st;
-            if (score > best) {
-                best = score;
-                pick = c;
+    for (int ks = n2; ks >= 16; --ks) {
+        if (n2 % ks) continue;
+        const bool split = ks != n2;
+        if (g_force_kseg > 0 && ks != g_force_kseg) continue;
+        if (split && (ks % 32 || ks < 128)) continue;
+        MarchGeom b = g;
+        b.KS = ks;
+        b.nKS = n2 / ks;
+        b.BK = pick_bk(ks, es);
+        if (!b.BK) continue;
+        b.pitch = (ks + 31) / 32 * 32;
+        const int tpr = ks / 2;
+        for (int tj = 1; tj <= 64; ++tj) {
+            if (g_force_tj > 0 && tj != g_force_tj) continue;
+            if (n1 % tj || (tj * tpr) % 32 || tj * tpr > 512) continue;
+            for (int st = 3; st <= 5; ++st) {
+                if (g_force_stages > 0 && st != g_force_stages) continue;
+                MarchGeom c = b;
+                c.TJ = tj;
+                c.S = st;
+                c.halo_off = np * round128((tj + 2) * c.pitch * es);
+                c.stage_bytes = c.halo_off;
+                if (smem_need(c) + (split ? tj * 2 * 16 * 4 : 0) > kSmemPerCta) continue;
+                const int cps = ctas_per_sm(c, tpr);
+                if (cps < 1) continue;
+                // measured at 512^3 and 256^3: ring depth and long segments (fewer,
+                // larger copies) outweigh consumer warps
+                const double depth = st >= 5 ? 1.0 : (st == 4 ? 0.85 : 0.3);
+                const double seg = ks >= 256 || !split ? 1.0 : ks / 256.0;
+                const double score = cps * (tj * tpr / 32) * (double)tj / (tj + 2) * depth * seg +
+                                     0.001 * ks / n2;
+                if (score > best) {
+                    best = score;
+                    pick = c;
+                }
             }
         }
     }
     if (best < 0) return false;
     g = pick;
-    if ((g.pitch * es) % 128 || ((g.BK * es) % 128 && g.BK != n2) || (g.BK * es) % 16 ||
-        g.stage_bytes % (128 * np) || g.tab_bytes % 128)
+    if ((g.pitch * es) % 128 || ((g.BK * es) % 128 && g.BK != g.KS) || (g.BK * es) % 16 ||
+        g.halo_off % (128 * np) || g.tab_bytes % 128)
         return false;
     g.nJB = n1 / g.TJ;
     g.nIC = (p.n0 + g.CI - 1) / g.CI;
-    g.items = g.nJB * g.nIC;
-    smem = smem_need(g);
+    g.items = g.nJB * g.nKS * g.nIC;
+    smem = smem_need(g) + (g.nKS > 1 ? g.TJ * 2 * 16 * 4 : 0);
     return true;
 }
 
@@ -962,7 +1033,7 @@ int launch_complex_march(const ComplexStageParams& p, cudaStream_t st) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return fail_cuda(e, "complex marching kernel attributes");
-    const int threads = g.TJ * (p.n2 / 2) + 32;
+    const int threads = g.TJ * (g.KS / 2) + 32;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, (size_t)smem);
     if (e != cudaSuccess || per_sm < 1)
@@ -981,6 +1052,13 @@ using namespace tipt;
 
 // Tile shape of the marching kernel: rows per tile, planes per i-chunk and
 // ring stages (0 = automatic).  Used by the autotuner; performance only.
+// Row segment of the complex marching kernel (0 = automatic); performance only.
+extern "C" int tipt_set_march_kseg(int kseg) {
+    if (kseg < 0) return fail(TIPT_ERR_ARG, "bad row segment");
+    g_force_kseg = kseg;
+    return TIPT_OK;
+}
+
 extern "C" int tipt_set_march_tiles(int rows, int planes, int stages) {
     if (rows < 0 || planes < 0 || stages < 0 || (stages > 0 && stages < 3) || stages > 5)
         return fail(TIPT_ERR_ARG, "bad tile shape");

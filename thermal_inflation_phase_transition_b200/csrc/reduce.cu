@@ -16,18 +16,20 @@ constexpr int kObs = 10;          // outputs
 constexpr int kRedThreads = 256;
 constexpr int kMaxRedBlocks = 1184;
 
+// Accumulators: grad = sum of squared forward differences (the constants 0.5
+// inv_a2 inv_dx2 are applied once at the end), sq = sum of pi^2 (E_kin = sq / 2,
+// bitwise the sum of pi^2 / 2: halving commutes with FP64 rounding).
 struct ObsAcc {
-    double kin, grad, pot, s1, s2, sq, above, nonfinite, mn, mx;
+    double grad, pot, s1, s2, sq, above, nonfinite, mn, mx;
 };
 
 __device__ __forceinline__ void acc_init(ObsAcc& a) {
-    a.kin = a.grad = a.pot = a.s1 = a.s2 = a.sq = a.above = a.nonfinite = 0.0;
+    a.grad = a.pot = a.s1 = a.s2 = a.sq = a.above = a.nonfinite = 0.0;
     a.mn = INFINITY;
     a.mx = -INFINITY;
 }
 
 __device__ __forceinline__ void acc_merge(ObsAcc& a, const ObsAcc& b) {
-    a.kin += b.kin;
     a.grad += b.grad;
     a.pot += b.pot;
     a.s1 += b.s1;
@@ -41,7 +43,6 @@ __device__ __forceinline__ void acc_merge(ObsAcc& a, const ObsAcc& b) {
 
 __device__ __forceinline__ ObsAcc acc_shfl_down(const ObsAcc& a, int off) {
     ObsAcc b;
-    b.kin = __shfl_down_sync(0xffffffffu, a.kin, off);
     b.grad = __shfl_down_sync(0xffffffffu, a.grad, off);
     b.pot = __shfl_down_sync(0xffffffffu, a.pot, off);
     b.s1 = __shfl_down_sync(0xffffffffu, a.s1, off);
@@ -104,8 +105,7 @@ __device__ __forceinline__ void obs_site(const ObsParams& p, ObsAcc& a, int64_t 
     const double fx = load_val<S>(p.phi, s + ox, N) - ph;
     const double fy = load_val<S>(p.phi, s + oy, N) - ph;
     const double fz = load_val<S>(p.phi, s + oz, N) - ph;
-    a.kin += 0.5 * pv * pv;
-    a.grad += 0.5 * p.inv_a2 * (fx * fx + fy * fy + fz * fz) * p.inv_dx2;
+    a.grad += fx * fx + fy * fy + fz * fz;
     const double ph2 = ph * ph;
     a.pot += (0.25 * p.lam * ph2 * ph2 - 0.5 * p.m2 * ph2) * p.inv_mu2;
     a.s1 += ph;
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kRedThreads) obs_partial_kernel(ObsParams p) {
     a = block_reduce(a);
     if (threadIdx.x == 0) {
         double* o = p.partials + (int64_t)blockIdx.x * kObs;
-        o[0] = a.kin;
+        o[0] = 0.0;  // slot kept so the workspace layout stays [G][kObs]
         o[1] = a.grad;
         o[2] = a.pot;
         o[3] = a.s1;
@@ -164,7 +164,6 @@ __global__ void __launch_bounds__(kRedThreads) obs_final_kernel(ObsParams p, int
     for (int b = threadIdx.x; b < G; b += blockDim.x) {
         const double* o = p.partials + (int64_t)b * kObs;
         ObsAcc c;
-        c.kin = o[0];
         c.grad = o[1];
         c.pot = o[2];
         c.s1 = o[3];
@@ -178,8 +177,8 @@ __global__ void __launch_bounds__(kRedThreads) obs_final_kernel(ObsParams p, int
     }
     a = block_reduce(a);
     if (threadIdx.x == 0) {
-        p.out[0] = a.kin * inv_n;
-        p.out[1] = a.grad * inv_n;
+        p.out[0] = 0.5 * a.sq * inv_n;
+        p.out[1] = 0.5 * p.inv_a2 * p.inv_dx2 * a.grad * inv_n;
         p.out[2] = a.pot * inv_n;
         p.out[3] = a.s1 * inv_n;
         p.out[4] = a.s2 * inv_n;

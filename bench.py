@@ -454,8 +454,8 @@ def run_e2e(args, shape, seed, RF, observables, torch, dev, world):
 
 
 def run_ensemble_bench(args):
-    """Config-4 ensemble (1024 x 128^2, 512 x 64^3, 256 x 96^3 replicas, T ~ U[0.98, 1.01],
-    E ~ U[0.04, 0.06]) for up to --ens-steps steps: first-passage events of the batched
+    """Batched ensemble of 1792 replicas (1024 x 128^2, 512 x 64^3, 256 x 96^3,
+    T ~ U[0.98, 1.01], E ~ U[0.04, 0.06]) for up to --ens-steps steps: first-passage events of the batched
     engine per GPU-hour, and of the same replicas launched one at a time (timed on
     --ens-plain replicas per size class and scaled by the class counts; both arms produce
     bitwise identical trajectories, hence identical events).  The one-at-a-time arm is
@@ -464,7 +464,7 @@ def run_ensemble_bench(args):
     import torch
     from thermal_inflation_phase_transition_b200 import ensemble as EN
     torch.cuda.set_device(0)
-    specs = EN.config4_specs()
+    specs = EN.mixed_lattice_specs()
     ens = EN.Ensemble(specs, check_every=10)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -503,7 +503,7 @@ def run_ensemble_bench(args):
         "metric": "Gamma estimates per GPU-hour (+-10% Poisson, 100 events each)",
         "value": est_b, "unit": "estimates/GPU-hour", "n_gpus": 1, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32c", "data": "synthetic",
-        "config": {"workload": "config-4 ensemble: 1024 x 128^2 (2-D), 512 x 64^3, 256 x 96^3 "
+        "config": {"workload": "batched ensemble: 1024 x 128^2 (2-D), 512 x 64^3, 256 x 96^3 "
                                "replicas, T~U[0.98,1.01], E~U[0.04,0.06], stop at converted "
                                "fraction (phi > 1) > 0.5", "max_steps": args.ens_steps,
                    "replicas": len(specs), "events": events, "site_updates": site_steps},
@@ -520,7 +520,7 @@ def run_ensemble_bench(args):
 
 
 def run_complex_bench(args):
-    """Complex field (config 3): 512^3 compensated FP32, V = D(T^2-T0^2)|Phi|^2 - E T |Phi|^3
+    """Complex field, 512^3 compensated FP32, V = D(T^2-T0^2)|Phi|^2 - E T |Phi|^3
     + lam/4 |Phi|^4 tabulated in |Phi| (4096 points on [0, 3]) plus eps Re(Phi^4) analytic
     (eps = 1e-3), T = 0.98 (below T0: the U(1) breaks and strings form), hash noise per
     component, seed 2; tile shape from the autotuner.  One step = one midpoint dt-step of
@@ -625,7 +625,8 @@ def run_surrogate_bench(args):
         "value": v["median_abs_rel_err"], "unit": "median |Gamma_sur/Gamma_plain - 1|",
         "n_gpus": 1, "higher_is_better": False, "vs_baseline": None, "dtype": "bf16/fp32",
         "data": "synthetic",
-        "config": {"workload": "config-5 surrogate-steered scan", "train_replicas": 20000,
+        "config": {"workload": "surrogate-steered scan of T/T0, E, D, lam with 64^3 "
+                               "verification", "train_replicas": 20000,
                    "scan_points": 64, "verify_replicas": 256, "scan_lattice": [64, 64, 64]},
         "report": rep, "wall_s": wall,
     }

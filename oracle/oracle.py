@@ -4,7 +4,7 @@ TEST INFRASTRUCTURE ONLY: the parity tests, ``__graft_entry__.smoke()`` and the
 CPU-baseline leg of ``bench.py`` use this module as the checker.  The product
 path never imports it.
 
-Also holds the FP64 potential/table builders for the BASELINE workloads (the
+Also holds the FP64 potential/table builders for the benchmark workloads (the
 toy polynomial V' = 2D(T^2-T0^2)phi - 3E T phi^2 + lam phi^3) restated from the
 table construction in R:805-849 (``build_vprime_table``): a uniform grid,
 ``table[i] = V'(lo + i*(hi-lo)/(n-1), T)``, ``dinv = 1/((hi-lo)/(n-1))``.

@@ -272,7 +272,7 @@ def gen_energies():
 
 
 # ------------------------------------------- 8. 2-D 256^2 FP64 trajectory
-def gen_config_2d():
+def gen_trajectory_2d():
     """2-D 256x256 periodic lattice, FP64, dx=1, dt=0.05, gamma=1, toy potential
     D=0.1 E=0.05 lam=0.1 T0=1 at T=1.02, 4096-point table on [0,3], midpoint
     RK2 (the reference's rk2_step_table) with hash noise seed 0 at the pass-2
@@ -299,7 +299,7 @@ def gen_config_2d():
         frac[n] = np.mean(phi > 1.0)
         if n == 99:
             phi100, pi100 = phi.copy(), pi.copy()
-    save("config_2d_256.npz", dt=dt, dx=dx, eta=eta, mu=mu, inv_a2=inv_a2, T=T, ns=ns,
+    save("trajectory_2d_256.npz", dt=dt, dx=dx, eta=eta, mu=mu, inv_a2=inv_a2, T=T, ns=ns,
          table=tab, tmin=tmin, dinv=dinv, npts=npts, phi0=phi0, noise0=noise0, phi100=phi100,
          pi100=pi100, phi2_mean=phi2, frac_above_1=frac, phi_final=phi, pi_final=pi)
 
@@ -312,4 +312,4 @@ if __name__ == "__main__":
     gen_complex()
     gen_winding()
     gen_energies()
-    gen_config_2d()
+    gen_trajectory_2d()

@@ -11,7 +11,7 @@ from thermal_inflation_phase_transition_b200 import driver as D  # noqa: E402
 
 def test_driver_2d_trajectory_matches_reference(golden):
     """2-D 256^2 FP64, 2000 graph-replayed steps: the <phi^2> curve of the reference run."""
-    g = golden("config_2d_256.npz")
+    g = golden("trajectory_2d_256.npz")
     tab = D.Table1D(g["table"], float(g["tmin"]), float(g["dinv"]))
     sched = D.constant_temperature(float(g["T"]), 2000, dt=float(g["dt"]), eta=float(g["eta"]))
     assert abs(sched[0, 1] - float(g["ns"])) < 1e-15

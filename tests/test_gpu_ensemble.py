@@ -45,9 +45,9 @@ def test_first_passage_batched_equals_plain():
     assert curves.shape[1] == 3 and (np.diff(steps) == 10).all()
 
 
-def test_ensemble_config4_shapes_step():
-    """One check interval of a reduced config-4 mix (2-D 128^2, 64^3, 96^3 replicas)."""
-    specs = EN.config4_specs(n128=8, n64=4, n96=2)
+def test_ensemble_mixed_lattice_shapes_step():
+    """One check interval of a reduced mix of 2-D 128^2, 64^3 and 96^3 replicas."""
+    specs = EN.mixed_lattice_specs(n128=8, n64=4, n96=2)
     ens = EN.Ensemble(specs, check_every=4)
     ens.run(4)
     for r in (0, 9, 13):

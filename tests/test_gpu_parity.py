@@ -256,10 +256,10 @@ def test_aliasing_is_rejected():
         RF.rk2_step_table(phi, pi, 0.05, 1, 1, 1, None, phi, pi, 1, tab, 0.0, 1.0, 8)
 
 
-def test_config_2d_trajectory_fp64(golden):
+def test_trajectory_2d_256_fp64(golden):
     """2-D 256^2, FP64, 2000 midpoint steps with hash noise: the <phi^2> curve and
     the final field against the reference's own run."""
-    g = golden("config_2d_256.npz")
+    g = golden("trajectory_2d_256.npz")
     phi = cu(g["phi0"])
     pi = torch.zeros_like(phi)
     pt, vt = torch.empty_like(phi), torch.empty_like(pi)

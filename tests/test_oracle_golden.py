@@ -163,9 +163,9 @@ def test_table_2d_blend_is_bilinear():
     np.testing.assert_allclose(row, O.toy_vprime(np.linspace(0, 3, 64), 1.0123), atol=1e-4)
 
 
-def test_config_2d_trajectory(golden):
+def test_trajectory_2d_256(golden):
     """2-D 256^2 FP64, 2000 steps: oracle vs the reference's rk2_step_table run."""
-    g = golden("config_2d_256.npz")
+    g = golden("trajectory_2d_256.npz")
     phi = g["phi0"].copy()
     pi = np.zeros_like(phi)
     tmp = [np.empty_like(phi), np.empty_like(phi)]

@@ -30,7 +30,7 @@ import torch
 from . import _lib as L
 from ._common import ptr, step_params, stream_handle
 
-__all__ = ["Ensemble", "ReplicaSpec", "toy_coefficients", "gamma_mle", "config4_specs",
+__all__ = ["Ensemble", "ReplicaSpec", "toy_coefficients", "gamma_mle", "mixed_lattice_specs",
            "plain_first_passage"]
 
 
@@ -54,7 +54,7 @@ class ReplicaSpec:
     T0: float = 1.0
 
 
-def config4_specs(n128=1024, n64=512, n96=256, seed=4, T_range=(0.98, 1.01),
+def mixed_lattice_specs(n128=1024, n64=512, n96=256, seed=4, T_range=(0.98, 1.01),
                   E_range=(0.04, 0.06)):
     """The 1792-replica ensemble: 1024 x 128^2 (2-D), 512 x 64^3, 256 x 96^3, seed = replica
     id, T ~ U[0.98, 1.01], E ~ U[0.04, 0.06] (fixed host RNG)."""

@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
         p.c2 = rp.c2;
         p.c3 = rp.c3;
         const uint32_t n12 = (uint32_t)rp.n1 * (uint32_t)rp.n2;
+        const F32CConst kc = f32c_const(p);
         for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
             const uint32_t s = (uint32_t)(ch.begin + t);
             const uint32_t q = fdiv(s, rp.m2);
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
                 x.pih = vh[0];
                 x.pil = vl[0];
                 float a, b, cc, d;
-                update_f32c<float>(p, nullptr, 0.0f, 0.0f, x, site_kick_f32c(p, (uint64_t)s), a, b,
+                update_f32c<float>(p, kc, nullptr, x, site_kick_f32c(p, kc, (uint64_t)s), a, b,
                                    cc, d);
                 float* po = static_cast<float*>(e.phi_out);
                 float* vo = static_cast<float*>(e.pi_out);

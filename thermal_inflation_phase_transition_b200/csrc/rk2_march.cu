@@ -6,17 +6,23 @@
 // memory.  Per plane the CTA needs TJ+2 rows (one halo row each side, rows
 // taken modulo n1 = periodic wrap in j) of phi and pi.
 //
-// Warp roles.  The last warp is the producer: one lane loads each plane with
-// TMA (cp.async.bulk.tensor.3d, one BK x 1 x 1 box per row segment, every
-// coordinate reduced modulo its extent, so no copy leaves the tensor) into an
-// S-stage ring.  Stage s has a `full` mbarrier (producer's expect-tx arrival +
-// the copy bytes) and an `empty` mbarrier (one arrival per consumer warp).
-// Consumer warps compute plane i from the ring (j and k neighbours), a register
-// queue (prev, cur, next) of their own four sites (i neighbours) and release a
-// stage as soon as they have read it; there is no CTA-wide barrier in the
-// loop, so warps drift freely within the ring's slack.  Each consumer thread
-// owns the site pairs {2t, 2t+1} and {n2/2 + 2t, n2/2 + 2t + 1} of its row, so
-// the 16-byte shared loads and global stores of a warp are contiguous.
+// Warp roles.  The last warp is the producer: one lane loads each plane into
+// an S-stage ring.  Real fields: the tile's rows of a plane are consecutive
+// rows of the field in global memory (and, with the pitch equal to the row
+// length, in shared memory), so each field component is one 1-D bulk copy
+// (cp.async.bulk) per run of rows -- at most three runs where the tile wraps
+// in j -- four to twelve copies per plane instead of one per row and box; the
+// producer's issue rate bounds the stage when copies are small.  The complex
+// kernel copies row segments with TMA tensor boxes (cp.async.bulk.tensor.3d,
+// every coordinate reduced modulo its extent).  Stage s has a `full` mbarrier
+// (producer's expect-tx arrival + the copy bytes) and an `empty` mbarrier (one
+// arrival per consumer warp).  Consumer warps compute plane i from the ring
+// (planes i-1, i, i+1: i, j and k neighbours) and release plane i-1 as soon
+// as they have read it; there is no CTA-wide barrier in the loop, so warps
+// drift freely within the ring's slack.  A consumer thread of the FP64 kernel
+// owns the site pairs {2t, 2t+1} and {n2/2 + 2t, n2/2 + 2t + 1} of its row, of
+// the F32C kernel four consecutive sites, so the 16-byte shared loads and
+// global stores of a warp are contiguous.
 //
 // Every mbarrier wait is bounded by the global timer (2 s); on expiry the
 // thread records TIPT_ERR_TIMEOUT in a device status word and returns; the
@@ -78,6 +84,36 @@ __device__ __forceinline__ void tma_row(void* dst, const CUtensorMap* tm, int k,
         " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
         "l"(reinterpret_cast<uint64_t>(tm)), "r"(k), "r"(j), "r"(i), "r"(smem_addr(bar))
         : "memory");
+}
+
+// 1-D bulk copy global -> shared (addresses 16-byte aligned, bytes a multiple
+// of 16), completing on a transaction-count mbarrier.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Copies the tile rows j0-1 .. j0-1+rows-1 (taken modulo n1) of plane `plane`
+// of a field into a [rows][pitch] block: runs of consecutive rows are one
+// contiguous range in global memory, and in shared memory too when the pitch
+// is the row length, so a run is one bulk copy (at most three runs: the wrap
+// at j = 0 and at j = n1); otherwise one copy per row.
+template <typename E>
+__device__ __forceinline__ void copy_tile_rows(E* dst, const E* field, int64_t plane, int j0,
+                                               int rows, int n1, int n2, int pitch, uint64_t* bar) {
+    int rr = 0;
+    while (rr < rows) {
+        int jr = j0 - 1 + rr;
+        jr = jr < 0 ? jr + n1 : (jr >= n1 ? jr - n1 : jr);
+        int len = pitch == n2 ? min(rows - rr, n1 - jr) : 1;
+        bulk_copy(dst + (size_t)rr * pitch, field + (plane * n1 + jr) * n2,
+                  (uint32_t)(len * n2 * (int)sizeof(E)), bar);
+        rr += len;
+    }
 }
 
 // -------------------------------------------------------------- params -----
@@ -153,8 +189,7 @@ constexpr int kMarchRegs = 96;
 
 template <int S, bool WIDE>
 __global__ void __maxnreg__(kMarchRegs)
-    rk2_stage_march(const __grid_constant__ CUtensorMap tm_phi,
-                    const __grid_constant__ CUtensorMap tm_pi, RealStageParams p_in, MarchGeom g) {
+    rk2_stage_march(RealStageParams p_in, MarchGeom g) {
     RealStageParams p = p_in;
     resolve_schedule(p);
     using E = typename MarchElem<S>::E;
@@ -197,6 +232,8 @@ __global__ void __maxnreg__(kMarchRegs)
     if (t >= nc) {
         if (t != nc) return;
         const uint32_t plane_tx = (uint32_t)(2 * rows * n2 * (int)sizeof(E));
+        const E* const src_phi = static_cast<const E*>(p.phi);
+        const E* const src_pi = static_cast<const E*>(p.pi);
         RingPos w{0, 0};
         uint32_t issued = 0;
         bool ok = true;
@@ -213,14 +250,8 @@ __global__ void __maxnreg__(kMarchRegs)
                 mbar_expect_tx(&full[w.stage], plane_tx);
                 int iw = i0 - 1 + q;
                 iw = iw < 0 ? iw + n0 : (iw >= n0 ? iw - n0 : iw);
-                for (int rr = 0; rr < rows; ++rr) {
-                    int jr = j0 - 1 + rr;
-                    jr = jr < 0 ? jr + n1 : (jr >= n1 ? jr - n1 : jr);
-                    for (int kb = 0; kb < n2; kb += g.BK) {
-                        tma_row(fld(w.stage, 0) + rr * pitch + kb, &tm_phi, kb, jr, iw, &full[w.stage]);
-                        tma_row(fld(w.stage, 1) + rr * pitch + kb, &tm_pi, kb, jr, iw, &full[w.stage]);
-                    }
-                }
+                copy_tile_rows(fld(w.stage, 0), src_phi, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                copy_tile_rows(fld(w.stage, 1), src_pi, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
                 ++issued;
                 w.next(NS);
             }
@@ -332,9 +363,7 @@ __global__ void __maxnreg__(kMarchRegs)
 // in the order of the generic kernel, so results are bitwise identical.
 template <bool WIDE>
 __global__ void __maxnreg__(kMarchRegs)
-    rk2_stage_march_f32c(const __grid_constant__ CUtensorMap tm_phi,
-                         const __grid_constant__ CUtensorMap tm_pi, RealStageParams p_in,
-                         MarchGeom g) {
+    rk2_stage_march_f32c(RealStageParams p_in, MarchGeom g) {
     RealStageParams p = p_in;
     resolve_schedule(p);
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -374,6 +403,8 @@ __global__ void __maxnreg__(kMarchRegs)
     if (t >= nc) {
         if (t != nc) return;
         const uint32_t plane_tx = (uint32_t)(4 * rows * n2 * 4);
+        const float* const src_phi = static_cast<const float*>(p.phi);
+        const float* const src_pi = static_cast<const float*>(p.pi);
         RingPos w{0, 0};
         uint32_t issued = 0;
         bool ok = true;
@@ -389,18 +420,11 @@ __global__ void __maxnreg__(kMarchRegs)
                 mbar_expect_tx(&full[w.stage], plane_tx);
                 int iw = i0 - 1 + q;
                 iw = iw < 0 ? iw + n0 : (iw >= n0 ? iw - n0 : iw);
-                for (int rr = 0; rr < rows; ++rr) {
-                    int jr = j0 - 1 + rr;
-                    jr = jr < 0 ? jr + n1 : (jr >= n1 ? jr - n1 : jr);
-                    for (int kb = 0; kb < n2; kb += g.BK) {
-                        const int o = rr * pitch + kb;
-                        // plane iw = hi, plane n0 + iw = lo
-                        tma_row(blk(w.stage, 0, 0) + o, &tm_phi, kb, jr, iw, &full[w.stage]);
-                        tma_row(blk(w.stage, 0, 1) + o, &tm_phi, kb, jr, n0 + iw, &full[w.stage]);
-                        tma_row(blk(w.stage, 1, 0) + o, &tm_pi, kb, jr, iw, &full[w.stage]);
-                        tma_row(blk(w.stage, 1, 1) + o, &tm_pi, kb, jr, n0 + iw, &full[w.stage]);
-                    }
-                }
+                // planes iw (hi) and n0 + iw (lo) of the planar pair
+                copy_tile_rows(blk(w.stage, 0, 0), src_phi, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                copy_tile_rows(blk(w.stage, 0, 1), src_phi, n0 + iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                copy_tile_rows(blk(w.stage, 1, 0), src_pi, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                copy_tile_rows(blk(w.stage, 1, 1), src_pi, n0 + iw, j0, rows, n1, n2, pitch, &full[w.stage]);
                 ++issued;
                 w.next(NS);
             }
@@ -421,7 +445,7 @@ __global__ void __maxnreg__(kMarchRegs)
     const int k0 = 4 * (t - (r - 1) * tpr);    // first of the four own columns
     const int kml = k0 == 0 ? n2 - 1 : k0 - 1;
     const int kpr = k0 + 4 == n2 ? 0 : k0 + 4;
-    const float tminf = (float)p.tmin, dinvf = (float)p.dinv;
+    const F32CConst kc = f32c_const(p);
     float* const phi_out = static_cast<float*>(p.phi_out);
     float* const pi_out = static_cast<float*>(p.pi_out);
     const int64_t N = (int64_t)n0 * n1 * n2;
@@ -498,8 +522,8 @@ __global__ void __maxnreg__(kMarchRegs)
                 uint64_t site;
                 if constexpr (WIDE) site = (uint64_t)(rowoff + 2 * h);
                 else site = (uint32_t)rowoff + (uint32_t)(2 * h);
-                update_f32c<float2>(p, s_tab, tminf, dinvf, in[h], site_kick_f32c2(p, site),
-                                    o[h][0], o[h][1], o[h][2], o[h][3]);
+                update_f32c<float2>(p, kc, s_tab, in[h], site_kick_f32c2(p, kc, site), o[h][0],
+                                    o[h][1], o[h][2], o[h][3]);
             }
             *reinterpret_cast<float4*>(phi_out + rowoff) = make_float4(o[0][0].x, o[0][0].y, o[1][0].x, o[1][0].y);
             *reinterpret_cast<float4*>(phi_out + N + rowoff) = make_float4(o[0][1].x, o[0][1].y, o[1][1].x, o[1][1].y);
@@ -833,8 +857,7 @@ static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, 
     const int n1 = p.n1, n2 = p.n2;
     const int es = layout_es(storage), np = layout_planes(storage);
     if (n2 % 4 != 0 || n2 < 8 || n2 > 2048) return false;
-    g.BK = pick_bk(n2, es);
-    if (!g.BK) return false;
+    g.BK = n2;  // whole rows: every copy is a 1-D bulk copy of consecutive rows
     const int per128 = 128 / es;
     g.pitch = (n2 + per128 - 1) / per128 * per128;
     const int tpr = n2 / 4;
@@ -867,11 +890,10 @@ static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, 
     }
     if (best < 0) return false;
     g = pick;
-    // every TMA destination (ring + stage*stage_bytes + f*stage_bytes/2 +
-    // (rr*pitch + kb)*8) must be 128-byte aligned
-    if ((g.pitch * es) % 128 || ((g.BK * es) % 128 && g.BK != n2) || (g.BK * es) % 16 ||
-        g.stage_bytes % (256 * np) || g.tab_bytes % 128)
-        return false;
+    // bulk-copy destinations (ring + stage*stage_bytes + block*stage_bytes/blocks +
+    // rr*pitch*es) are 128-byte aligned; sources and sizes are multiples of the
+    // 16-byte row length (n2 % 4 == 0)
+    if ((g.pitch * es) % 128 || g.stage_bytes % (256 * np) || g.tab_bytes % 128) return false;
     g.nJB = n1 / g.TJ;
     g.nIC = (p.n0 + g.CI - 1) / g.CI;
     g.items = g.nJB * g.nIC;
@@ -881,7 +903,6 @@ static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, 
 
 bool march_supported(int storage, const RealStageParams& p) {
     if (storage != TIPT_F32C && storage != TIPT_F64) return false;
-    if (!encode_fn()) return false;
     const uintptr_t a = reinterpret_cast<uintptr_t>(p.phi) | reinterpret_cast<uintptr_t>(p.pi) |
                         reinterpret_cast<uintptr_t>(p.phi_out) |
                         reinterpret_cast<uintptr_t>(p.pi_out);
@@ -893,8 +914,7 @@ bool march_supported(int storage, const RealStageParams& p) {
 }
 
 template <typename Kern>
-static int launch_march_k(Kern kern, const CUtensorMap& tphi, const CUtensorMap& tpi,
-                          const RealStageParams& p, const MarchGeom& g, int64_t smem,
+static int launch_march_k(Kern kern, const RealStageParams& p, const MarchGeom& g, int64_t smem,
                           cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
@@ -910,7 +930,7 @@ static int launch_march_k(Kern kern, const CUtensorMap& tphi, const CUtensorMap&
                     "bytes of shared memory)", threads, (long long)smem);
     int grid = num_sms() * per_sm;
     if (grid > g.items) grid = g.items;
-    kern<<<grid, threads, (size_t)smem, st>>>(tphi, tpi, p, g);
+    kern<<<grid, threads, (size_t)smem, st>>>(p, g);
     e = cudaGetLastError();
     return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "marching kernel launch");
 }
@@ -921,17 +941,12 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
     if (!geometry(storage, p, smem_table, g, smem))
         return fail(TIPT_ERR_UNSUPPORTED, "marching kernel geometry");
     const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
-    const int es = layout_es(storage), planes = layout_planes(storage) * p.n0;
-    CUtensorMap tphi, tpi;
-    if (!make_map(&tphi, p.phi, planes, p.n1, p.n2, es, g.BK) ||
-        !make_map(&tpi, p.pi, planes, p.n1, p.n2, es, g.BK))
-        return fail(TIPT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     if (storage == TIPT_F32C)
-        return wide ? launch_march_k(rk2_stage_march_f32c<true>, tphi, tpi, p, g, smem, st)
-                    : launch_march_k(rk2_stage_march_f32c<false>, tphi, tpi, p, g, smem, st);
+        return wide ? launch_march_k(rk2_stage_march_f32c<true>, p, g, smem, st)
+                    : launch_march_k(rk2_stage_march_f32c<false>, p, g, smem, st);
     if (storage == TIPT_F64)
-        return wide ? launch_march_k(rk2_stage_march<TIPT_F64, true>, tphi, tpi, p, g, smem, st)
-                    : launch_march_k(rk2_stage_march<TIPT_F64, false>, tphi, tpi, p, g, smem, st);
+        return wide ? launch_march_k(rk2_stage_march<TIPT_F64, true>, p, g, smem, st)
+                    : launch_march_k(rk2_stage_march<TIPT_F64, false>, p, g, smem, st);
     return fail(TIPT_ERR_STORAGE, "marching kernel takes F32C or F64");
 }
 

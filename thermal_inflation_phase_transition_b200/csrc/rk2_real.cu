@@ -18,7 +18,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
     using TT = typename std::conditional<S == TIPT_F32C, float, double>::type;
     TT* s_tab = reinterpret_cast<TT*>(smem_raw);
     if (p.table_in_smem) stage_table<TT>(p, s_tab);
-    const float tminf = (float)p.tmin, dinvf = (float)p.dinv;
+    const F32CConst kc = f32c_const(p);
 
     const int64_t n12 = (int64_t)p.n1 * p.n2;
     const int64_t N = (int64_t)p.n0 * n12;
@@ -83,8 +83,8 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
             x.pih = vh[0];
             x.pil = vl[0];
             float a, b, c, d;
-            update_f32c<float>(p, reinterpret_cast<const float*>(s_tab), tminf, dinvf, x,
-                               site_kick_f32c(p, (uint64_t)s), a, b, c, d);
+            update_f32c<float>(p, kc, reinterpret_cast<const float*>(s_tab), x,
+                               site_kick_f32c(p, kc, (uint64_t)s), a, b, c, d);
             float* po = static_cast<float*>(p.phi_out);
             float* vo = static_cast<float*>(p.pi_out);
             po[s] = a;

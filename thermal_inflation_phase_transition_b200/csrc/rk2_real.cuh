@@ -106,13 +106,43 @@ __device__ __forceinline__ void vset(float2& v, int l, float x) {
     else v.x = x;
 }
 
+// FP32 constants of a compensated-FP32 stage, rounded once per launch from the
+// FP64 parameters (after the schedule is resolved) and passed to the per-site
+// arithmetic, so the loop does no FP64 -> FP32 conversion.
+struct F32CConst {
+    float h1, h2h, h2l;            // h2 = h2h + h2l
+    float inv_dx2, inv_a2, eta, inv_mu2;
+    float c1, c2, c3;              // polynomial V'
+    float tmin, dinv, last;        // table lookup: (x - tmin) dinv clamped to [0, last]
+    float ns;                      // hash noise amplitude
+};
+
+__device__ __forceinline__ F32CConst f32c_const(const RealStageParams& p) {
+    F32CConst k;
+    k.h1 = (float)p.h1;
+    k.h2h = (float)p.h2;
+    k.h2l = (float)(p.h2 - (double)k.h2h);
+    k.inv_dx2 = (float)p.inv_dx2;
+    k.inv_a2 = (float)p.inv_a2;
+    k.eta = (float)p.eta;
+    k.inv_mu2 = (float)p.inv_mu2;
+    k.c1 = (float)p.c1;
+    k.c2 = (float)p.c2;
+    k.c3 = (float)p.c3;
+    k.tmin = (float)p.tmin;
+    k.dinv = (float)p.dinv;
+    k.last = (float)(p.npts - 2);
+    k.ns = (float)p.ns_eff;
+    return k;
+}
+
 template <typename V>
-__device__ __forceinline__ V vprime_v(const RealStageParams& p, const float* s_tab, V x, float tmin,
-                                      float dinv) {
+__device__ __forceinline__ V vprime_v(const RealStageParams& p, const F32CConst& kc,
+                                      const float* s_tab, V x) {
     constexpr int NL = sizeof(V) / sizeof(float);
     if (p.vkind == TIPT_VP_POLY) {
-        const V d = v_fma(v_mul(v_mul(vs<V>((float)p.c3), x), x), x, v_mul(vs<V>((float)p.c1), x));
-        return p.c2 != 0.0 ? v_fma(v_mul(vs<V>((float)p.c2), x), x, d) : d;
+        const V d = v_fma(v_mul(v_mul(vs<V>(kc.c3), x), x), x, v_mul(vs<V>(kc.c1), x));
+        return p.c2 != 0.0 ? v_fma(v_mul(vs<V>(kc.c2), x), x, d) : d;
     }
     if (!p.table_in_smem) {
         V r;
@@ -122,8 +152,8 @@ __device__ __forceinline__ V vprime_v(const RealStageParams& p, const float* s_t
                                                  (double)vlane(x, l)));
         return r;
     }
-    const V fidx = v_mul(v_sub(x, vs<V>(tmin)), vs<V>(dinv));
-    const float last = (float)(p.npts - 2);
+    const V fidx = v_mul(v_sub(x, vs<V>(kc.tmin)), vs<V>(kc.dinv));
+    const float last = kc.last;
     V fi, a, b;
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
@@ -219,29 +249,27 @@ __device__ __forceinline__ V force_v(V inv_a2, V eta, V inv_mu2, V lap, V pv, V 
 }
 
 template <typename V>
-__device__ __forceinline__ void update_f32c(const RealStageParams& p, const float* s_tab,
-                                            float tminf, float dinvf, const F32CIn<V>& x, V kick,
+__device__ __forceinline__ void update_f32c(const RealStageParams& p, const F32CConst& kc,
+                                            const float* s_tab, const F32CIn<V>& x, V kick,
                                             V& phh, V& phl, V& pih, V& pil) {
-    const V h1 = vs<V>((float)p.h1);
-    const float h2f = (float)p.h2;
-    const V h2h = vs<V>(h2f);
-    const V h2l = vs<V>((float)(p.h2 - (double)h2f));
-    const V inv_dx2 = vs<V>((float)p.inv_dx2);
-    const V inv_a2 = vs<V>((float)p.inv_a2), eta = vs<V>((float)p.eta),
-            inv_mu2 = vs<V>((float)p.inv_mu2);
+    const V h1 = vs<V>(kc.h1);
+    const V h2h = vs<V>(kc.h2h);
+    const V h2l = vs<V>(kc.h2l);
+    const V inv_dx2 = vs<V>(kc.inv_dx2);
+    const V inv_a2 = vs<V>(kc.inv_a2), eta = vs<V>(kc.eta), inv_mu2 = vs<V>(kc.inv_mu2);
     const V lap = v_mul(v_add(x.dh_phi, x.dl_phi), inv_dx2);
     const V lapv = v_mul(v_add(x.dh_pi, x.dl_pi), inv_dx2);
     const V lap2 = v_fma(h1, lapv, lap);  // Laplacian of phi + h1 pi
     const V phc = v_add(x.phh, x.phl);
     const V pvc = v_add(x.pih, x.pil);
-    const V k1 = force_v(inv_a2, eta, inv_mu2, lap, pvc, vprime_v<V>(p, s_tab, phc, tminf, dinvf));
+    const V k1 = force_v(inv_a2, eta, inv_mu2, lap, pvc, vprime_v<V>(p, kc, s_tab, phc));
     // pi~ = pi + h1 k1 as {t_hi, t_lo}
     V t_hi, t_e;
     two_sum(x.pih, v_mul(h1, k1), t_hi, t_e);
     const V t_lo = v_add(x.pil, t_e);
     const V pit = v_add(t_hi, t_lo);
     const V pht = v_add(x.phh, v_fma(h1, pvc, x.phl));
-    const V k2 = force_v(inv_a2, eta, inv_mu2, lap2, pit, vprime_v<V>(p, s_tab, pht, tminf, dinvf));
+    const V k2 = force_v(inv_a2, eta, inv_mu2, lap2, pit, vprime_v<V>(p, kc, s_tab, pht));
     // phi + h2 pi~ with the product's rounding error kept
     const V d_hi = v_mul(h2h, t_hi);
     const V d_lo = v_add(v_fma(h2h, t_hi, v_neg(d_hi)), v_fma(h2h, t_lo, v_mul(h2l, t_hi)));
@@ -264,13 +292,15 @@ __device__ __forceinline__ void stencil_sums(const float hi[7], const float lo[7
 }
 
 // Noise increment for one F32C site: array value * nfac, or ns * z (FP32 z).
-__device__ __forceinline__ float site_kick_f32c(const RealStageParams& p, uint64_t site) {
+__device__ __forceinline__ float site_kick_f32c(const RealStageParams& p, const F32CConst& kc,
+                                                uint64_t site) {
     if (p.noise) return (float)(p.nfac * static_cast<const double*>(p.noise)[site]);
     if (p.ns_eff == 0.0) return 0.0f;
-    return __fmul_rn((float)p.ns_eff, gauss_cos_f(noise_key(site, p.step, p.mul, p.seed)));
+    return __fmul_rn(kc.ns, gauss_cos_f(noise_key(site, p.step, p.mul, p.seed)));
 }
 // The same for two consecutive sites (s, s + 1) in the lanes of a float2.
-__device__ __forceinline__ float2 site_kick_f32c2(const RealStageParams& p, uint64_t s) {
+__device__ __forceinline__ float2 site_kick_f32c2(const RealStageParams& p, const F32CConst& kc,
+                                                  uint64_t s) {
     if (p.noise) {
         const double* n = static_cast<const double*>(p.noise);
         return make_float2((float)(p.nfac * n[s]), (float)(p.nfac * n[s + 1]));
@@ -278,7 +308,7 @@ __device__ __forceinline__ float2 site_kick_f32c2(const RealStageParams& p, uint
     if (p.ns_eff == 0.0) return make_float2(0.0f, 0.0f);
     const float2 z = gauss_cos_f2(noise_key(s, p.step, p.mul, p.seed),
                                   noise_key(s + 1, p.step, p.mul, p.seed));
-    return v_mul(vs<float2>((float)p.ns_eff), z);
+    return v_mul(vs<float2>(kc.ns), z);
 }
 
 }  // namespace tipt

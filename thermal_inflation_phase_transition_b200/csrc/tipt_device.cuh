@@ -87,15 +87,14 @@ __device__ __forceinline__ V vs(float x) { return v_splat(x, V{}); }
 // FP32 Box-Muller for the compensated-FP32 storage.  The hash is the same
 // integer computation; only the Gaussian transform runs in FP32, from the
 // 53-bit integers m1, m2 (u = m * 2^-53) held as 32-bit halves (hi < 2^21):
-//  * log(u1): for u1 >= 1/2 the distance d = 1 - u1 is formed from the halves
-//    (exact to 2^-45 absolute) and log(u1) = log(1 + g) with g = -d; for
-//    u1 < 1/2 the FP32 value of u1 is split into exponent k and mantissa
-//    1 + g in [3/4, 3/2).  log(1 + g) = 2 atanh(s), s = g / (2 + g), summed as
-//    2 s (1 + s^2/3 + ... + s^14/15) (the atanh series; |s| <= 1/3, truncation
-//    below 2e-8).  The reference's clamp u1 >= 1e-12 is m1 <= 9007.
-//  * cos/sin(2 pi u2): 2 u2 = m2 * 2^-52; the nearest quarter turn q is read
-//    from the high half (exact), the remainder x lies in [-pi/4, pi/4] and the
-//    Taylor series of sin (to x^9) and cos (to x^10) are truncated below 3e-9.
+//  * log(u1): the atanh series of log(1 + g), g = u1 - 1 formed exactly from
+//    the halves, for u1 >= 1/2; the hardware base-2 logarithm for u1 < 1/2
+//    (log_u1 below).  The reference's clamp u1 >= 1e-12 is m1 <= 9007.
+//  * cos/sin(2 pi u2) (complex field): 2 u2 = m2 * 2^-52; the nearest quarter
+//    turn q is read from the high half (exact), the remainder x lies in
+//    [-pi/4, pi/4] and the Taylor series of sin (to x^9) and cos (to x^10) are
+//    truncated below 3e-9.  cos alone (real field): the nearest half turn, x in
+//    [-pi/2, pi/2] and the cos series to x^12 (truncated below 7e-9).
 //  * sqrt via rsqrt and one Newton step.
 // The absolute error of z against the FP64 reference value is a few 1e-7.
 __device__ __forceinline__ void hash_words(uint64_t x, uint32_t& h1, uint32_t& l1, uint32_t& h2,
@@ -104,8 +103,10 @@ __device__ __forceinline__ void hash_words(uint64_t x, uint32_t& h1, uint32_t& l
     x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
     x = x ^ (x >> 31);
     const uint64_t m1 = x >> 11;
-    x = (x * 0x2545F4914F6CDD1Dull) ^ 0x9E3779B97F4A7C15ull;
-    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    // (y ^ C) ^ ((y ^ C) >> 30) = y ^ (y >> 30) ^ (C ^ (C >> 30)): one xor fewer
+    constexpr uint64_t kC = 0x9E3779B97F4A7C15ull, kCs = kC ^ (kC >> 30);
+    x = x * 0x2545F4914F6CDD1Dull;
+    x = (x ^ (x >> 30) ^ kCs) * 0xBF58476D1CE4E5B9ull;
     x = x ^ (x >> 31);
     const uint64_t m2 = x >> 11;
     h1 = (uint32_t)(m1 >> 32);
@@ -114,31 +115,29 @@ __device__ __forceinline__ void hash_words(uint64_t x, uint32_t& h1, uint32_t& l
     l2 = (uint32_t)m2;
 }
 
-constexpr float kLn2Hi = 0.693147182464599609375f;   // ln 2 rounded to FP32
-constexpr float kLn2Lo = -1.904654299957768e-09f;    // ln 2 - kLn2Hi
+
+// log(u1) for one lane from the halves h, l of m1 (u1 = m1 2^-53):
+//  * u1 >= 1/2: g = u1 - 1 = (h - 2^21) 2^-21 + l 2^-53 (exact to 2^-45), and
+//    log(1 + g) = 2 atanh(s), s = g / (2 + g) in [-1/3, 0], summed as
+//    2 s (1 + s^2/3 + ... + s^14/15) (the atanh series, truncated below 2e-8);
+//  * u1 < 1/2: log2(u1) ln 2 with the hardware base-2 logarithm (lg2.approx;
+//    |log2 u1| >= 1 there, so its absolute error of about 2^-22 is a relative
+//    error below 2e-7).
+// Both are formed and one is selected, so the lanes of a warp do not diverge.
+// The reference's clamp u1 >= 1e-12 is m1 <= 9007.
+constexpr float kLn2 = 0.693147182464599609375f;     // ln 2 rounded to FP32
 constexpr float kLog1em12 = -27.631021115928547f;    // log(1e-12)
 
-// Integer half of the log reduction for one lane: g (log1p argument) and k
-// (power of two), plus the clamp flag.  Both reductions are formed and one is
-// selected, so lanes of a warp do not diverge.
-__device__ __forceinline__ void log_u1_reduce(uint32_t h, uint32_t l, float& g, float& k,
-                                              bool& clamp) {
-    clamp = (h == 0u) && (l <= 9007u);
-    const float lo = __fmul_rn((float)l, 0x1p-53f);
-    // u1 >= 1/2: g = -(1 - u1) = -((2^21 - h) 2^-21 - l 2^-53)
-    const float g_hi = __fmaf_rn(-(float)((1u << 21) - h), 0x1p-21f, lo);
-    // u1 < 1/2: mantissa of the FP32 value of u1 in [3/4, 3/2), exponent e
-    const float u = __fmaf_rn((float)h, 0x1p-21f, lo);
-    const uint32_t b = __float_as_uint(u);
-    const uint32_t up = (b >> 22) & 1u;
-    const int e = (int)((b >> 23) & 0xffu) - 127 + (int)up;
-    const float g_lo = __fsub_rn(__uint_as_float((b & 0x007fffffu) | ((127u - up) << 23)), 1.0f);
-    const bool big = h >= (1u << 20);
-    g = big ? g_hi : g_lo;
-    k = big ? 0.0f : (float)e;
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
 
-__device__ __forceinline__ float log_u1_series1(float g, float k) {
+__device__ __forceinline__ float log_u1(uint32_t h, uint32_t l) {
+    const float lo = __fmul_rn((float)l, 0x1p-53f);
+    const float hf = (float)h;  // exact: h < 2^21
+    const float g = __fmaf_rn(__fsub_rn(hf, 0x1p21f), 0x1p-21f, lo);
     const float s = __fdividef(g, __fadd_rn(2.0f, g));
     const float w = __fmul_rn(s, s);
     float poly = __fmaf_rn(w, 1.0f / 15.0f, 1.0f / 13.0f);
@@ -149,16 +148,10 @@ __device__ __forceinline__ float log_u1_series1(float g, float k) {
     poly = __fmaf_rn(w, poly, 1.0f / 3.0f);
     poly = __fmul_rn(w, poly);
     const float two_s = __fadd_rn(s, s);
-    const float l1p = __fmaf_rn(two_s, poly, two_s);
-    return __fmaf_rn(k, kLn2Hi, __fmaf_rn(k, kLn2Lo, l1p));
-}
-
-// Series in lane vectors: evaluated lane by lane with immediate coefficients
-// (bitwise the same for both lane widths).
-template <typename V>
-__device__ __forceinline__ V log_u1_series(V g, V k) {
-    if constexpr (sizeof(V) == 4) return log_u1_series1(g, k);
-    else return make_float2(log_u1_series1(g.x, k.x), log_u1_series1(g.y, k.y));
+    const float near = __fmaf_rn(two_s, poly, two_s);
+    const float far = __fmul_rn(lg2_approx(__fmaf_rn(hf, 0x1p-21f, lo)), kLn2);
+    const float lg = h >= (1u << 20) ? near : far;
+    return (h == 0u && l <= 9007u) ? kLog1em12 : lg;
 }
 
 // Integer half of the angle reduction: quarter turns q and the remainder x.
@@ -214,41 +207,55 @@ __device__ __forceinline__ V radius_from_log(V lg) {
     else return make_float2(radius_from_log1(lg.x), radius_from_log1(lg.y));
 }
 
+// cos(2 pi u2) alone (the real field draws only the cos branch): half-turn
+// reduction 2 u2 = q + x/pi with q = round(m2 2^-52) in {0, 1, 2} and
+// x in [-pi/2, pi/2], cos = (-1)^q cos x; the Taylor series of cos x to x^12
+// is truncated below 7e-9 on that interval.  Returns the sign bit (q odd) with
+// the cos x value.
+__device__ __forceinline__ void half_turn_reduce(uint32_t h, uint32_t l, uint32_t& sign,
+                                                 float& x) {
+    const uint32_t q = (h + (1u << 19)) >> 20;        // nearest multiple of 2^52 in m2
+    const int rh = (int)h - (int)(q << 20);            // |rh| <= 2^19, exact in FP32
+    // x = pi * 2^-52 * (rh 2^32 + l)
+    x = __fmaf_rn((float)rh, 2.99605662e-6f /* pi 2^-20 */, __fmul_rn((float)l, 6.97573699e-16f));
+    sign = q << 31;                                    // q = 2 shifts out: even
+}
+
+__device__ __forceinline__ float cos_series1(float x) {
+    const float x2 = __fmul_rn(x, x);
+    float c = __fmaf_rn(x2, 2.08767570e-9f, -2.75573192e-7f);  // 1/12!, -1/10!
+    c = __fmaf_rn(x2, c, 2.48015873e-5f);                      // 1/8!
+    c = __fmaf_rn(x2, c, -1.38888889e-3f);                     // -1/6!
+    c = __fmaf_rn(x2, c, 4.16666667e-2f);                      // 1/4!
+    c = __fmaf_rn(x2, c, -0.5f);
+    return __fmaf_rn(x2, c, 1.0f);
+}
+
+__device__ __forceinline__ float flip_sign(float v, uint32_t sign) {
+    return __uint_as_float(__float_as_uint(v) ^ sign);
+}
+
 // z (cos branch) for one key, FP32.
 __device__ __forceinline__ float gauss_cos_f(uint64_t key) {
-    uint32_t h1, l1, h2, l2, q;
+    uint32_t h1, l1, h2, l2, sg;
     hash_words(key, h1, l1, h2, l2);
-    float g, k, x, sn, cs, c, s;
-    bool clamp;
-    log_u1_reduce(h1, l1, g, k, clamp);
-    float lg = log_u1_series<float>(g, k);
-    lg = clamp ? kLog1em12 : lg;
-    angle_reduce(h2, l2, q, x);
-    sincos_series<float>(x, sn, cs);
-    quarter_turn(q, sn, cs, c, s);
-    return __fmul_rn(radius_from_log<float>(lg), c);
+    float x;
+    const float lg = log_u1(h1, l1);
+    half_turn_reduce(h2, l2, sg, x);
+    return __fmul_rn(radius_from_log<float>(lg), flip_sign(cos_series1(x), sg));
 }
 
 // z for two keys in the two lanes of a float2 (bitwise the same as two calls
 // of gauss_cos_f).
 __device__ __forceinline__ float2 gauss_cos_f2(uint64_t key0, uint64_t key1) {
-    uint32_t h1a, l1a, h2a, l2a, h1b, l1b, h2b, l2b, qa, qb;
+    uint32_t h1a, l1a, h2a, l2a, h1b, l1b, h2b, l2b, sa, sb;
     hash_words(key0, h1a, l1a, h2a, l2a);
     hash_words(key1, h1b, l1b, h2b, l2b);
-    float ga, ka, gb, kb, xa, xb;
-    bool ca, cb;
-    log_u1_reduce(h1a, l1a, ga, ka, ca);
-    log_u1_reduce(h1b, l1b, gb, kb, cb);
-    float2 lg = log_u1_series<float2>(make_float2(ga, gb), make_float2(ka, kb));
-    lg.x = ca ? kLog1em12 : lg.x;
-    lg.y = cb ? kLog1em12 : lg.y;
-    angle_reduce(h2a, l2a, qa, xa);
-    angle_reduce(h2b, l2b, qb, xb);
-    float2 sn, cs;
-    sincos_series<float2>(make_float2(xa, xb), sn, cs);
-    float2 c, s;
-    quarter_turn(qa, sn.x, cs.x, c.x, s.x);
-    quarter_turn(qb, sn.y, cs.y, c.y, s.y);
+    float xa, xb;
+    const float2 lg = make_float2(log_u1(h1a, l1a), log_u1(h1b, l1b));
+    half_turn_reduce(h2a, l2a, sa, xa);
+    half_turn_reduce(h2b, l2b, sb, xb);
+    const float2 c = make_float2(flip_sign(cos_series1(xa), sa), flip_sign(cos_series1(xb), sb));
     return v_mul(radius_from_log<float2>(lg), c);
 }
 
@@ -256,11 +263,8 @@ __device__ __forceinline__ float2 gauss_cos_f2(uint64_t key0, uint64_t key1) {
 __device__ __forceinline__ void gauss_pair_f(uint64_t key, float& z1, float& z2) {
     uint32_t h1, l1, h2, l2, q;
     hash_words(key, h1, l1, h2, l2);
-    float g, k, x, sn, cs, c, s;
-    bool clamp;
-    log_u1_reduce(h1, l1, g, k, clamp);
-    float lg = log_u1_series<float>(g, k);
-    lg = clamp ? kLog1em12 : lg;
+    float x, sn, cs, c, s;
+    const float lg = log_u1(h1, l1);
     angle_reduce(h2, l2, q, x);
     sincos_series<float>(x, sn, cs);
     quarter_turn(q, sn, cs, c, s);
@@ -276,13 +280,8 @@ __device__ __forceinline__ void gauss_pair_f2(uint64_t key0, uint64_t key1, floa
     uint32_t h1a, l1a, h2a, l2a, h1b, l1b, h2b, l2b, qa, qb;
     hash_words(key0, h1a, l1a, h2a, l2a);
     hash_words(key1, h1b, l1b, h2b, l2b);
-    float ga, ka, gb, kb, xa, xb;
-    bool ca, cb;
-    log_u1_reduce(h1a, l1a, ga, ka, ca);
-    log_u1_reduce(h1b, l1b, gb, kb, cb);
-    float2 lg = log_u1_series<float2>(make_float2(ga, gb), make_float2(ka, kb));
-    lg.x = ca ? kLog1em12 : lg.x;
-    lg.y = cb ? kLog1em12 : lg.y;
+    float xa, xb;
+    const float2 lg = make_float2(log_u1(h1a, l1a), log_u1(h1b, l1b));
     angle_reduce(h2a, l2a, qa, xa);
     angle_reduce(h2b, l2b, qb, xb);
     float2 sn, cs;

@@ -83,6 +83,8 @@ __device__ __forceinline__ float2 v_splat(float x, float2) { return make_float2(
 
 template <typename V>
 __device__ __forceinline__ V vs(float x) { return v_splat(x, V{}); }
+__device__ __forceinline__ float v_neg(float a) { return -a; }
+__device__ __forceinline__ float2 v_neg(float2 a) { return make_float2(-a.x, -a.y); }
 
 // FP32 Box-Muller for the compensated-FP32 storage.  The hash is the same
 // integer computation; only the Gaussian transform runs in FP32, from the
@@ -134,24 +136,54 @@ __device__ __forceinline__ float lg2_approx(float x) {
     return y;
 }
 
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// The arithmetic of log_u1 in lane vectors (one or two lanes; the packed
+// instructions round each lane as the scalar ones, so both give the same bits).
+template <typename V>
+__device__ __forceinline__ V log_u1_v(V hf, V lo) {
+    const V g = v_fma(v_sub(hf, vs<V>(0x1p21f)), vs<V>(0x1p-21f), lo);
+    const V d = v_add(vs<V>(2.0f), g);
+    V r;
+    if constexpr (sizeof(V) == 4) r = rcp_approx(d);
+    else r = make_float2(rcp_approx(d.x), rcp_approx(d.y));
+    const V s = v_mul(g, r);
+    const V w = v_mul(s, s);
+    V poly = v_fma(w, vs<V>(1.0f / 15.0f), vs<V>(1.0f / 13.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 11.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 9.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 7.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 5.0f));
+    poly = v_fma(w, poly, vs<V>(1.0f / 3.0f));
+    poly = v_mul(w, poly);
+    const V two_s = v_add(s, s);
+    return v_fma(two_s, poly, two_s);  // log(1 + g): the u1 >= 1/2 branch
+}
+
 __device__ __forceinline__ float log_u1(uint32_t h, uint32_t l) {
     const float lo = __fmul_rn((float)l, 0x1p-53f);
     const float hf = (float)h;  // exact: h < 2^21
-    const float g = __fmaf_rn(__fsub_rn(hf, 0x1p21f), 0x1p-21f, lo);
-    const float s = __fdividef(g, __fadd_rn(2.0f, g));
-    const float w = __fmul_rn(s, s);
-    float poly = __fmaf_rn(w, 1.0f / 15.0f, 1.0f / 13.0f);
-    poly = __fmaf_rn(w, poly, 1.0f / 11.0f);
-    poly = __fmaf_rn(w, poly, 1.0f / 9.0f);
-    poly = __fmaf_rn(w, poly, 1.0f / 7.0f);
-    poly = __fmaf_rn(w, poly, 1.0f / 5.0f);
-    poly = __fmaf_rn(w, poly, 1.0f / 3.0f);
-    poly = __fmul_rn(w, poly);
-    const float two_s = __fadd_rn(s, s);
-    const float near = __fmaf_rn(two_s, poly, two_s);
+    const float near = log_u1_v<float>(hf, lo);
     const float far = __fmul_rn(lg2_approx(__fmaf_rn(hf, 0x1p-21f, lo)), kLn2);
     const float lg = h >= (1u << 20) ? near : far;
     return (h == 0u && l <= 9007u) ? kLog1em12 : lg;
+}
+
+// log_u1 for two keys in the lanes of a float2.
+__device__ __forceinline__ float2 log_u1_2(uint32_t ha, uint32_t la, uint32_t hb, uint32_t lb) {
+    const float2 lo = v_mul(make_float2((float)la, (float)lb), vs<float2>(0x1p-53f));
+    const float2 hf = make_float2((float)ha, (float)hb);
+    const float2 near = log_u1_v<float2>(hf, lo);
+    const float2 u = v_fma(hf, vs<float2>(0x1p-21f), lo);
+    const float2 far = v_mul(make_float2(lg2_approx(u.x), lg2_approx(u.y)), vs<float2>(kLn2));
+    float2 lg = make_float2(ha >= (1u << 20) ? near.x : far.x, hb >= (1u << 20) ? near.y : far.y);
+    lg.x = (ha == 0u && la <= 9007u) ? kLog1em12 : lg.x;
+    lg.y = (hb == 0u && lb <= 9007u) ? kLog1em12 : lg.y;
+    return lg;
 }
 
 // Integer half of the angle reduction: quarter turns q and the remainder x.
@@ -194,17 +226,14 @@ __device__ __forceinline__ void quarter_turn(uint32_t q, float sn, float cs, flo
     s = (qq >= 2u) ? -b : b;
 }
 
-__device__ __forceinline__ float radius_from_log1(float lg) {
-    const float v = __fmul_rn(-2.0f, lg);   // > 0
-    const float y = rsqrtf(v);
-    const float r = __fmul_rn(v, y);
-    return __fmaf_rn(__fmul_rn(0.5f, y), __fmaf_rn(-r, r, v), r);  // one Newton step
-}
-
 template <typename V>
 __device__ __forceinline__ V radius_from_log(V lg) {
-    if constexpr (sizeof(V) == 4) return radius_from_log1(lg);
-    else return make_float2(radius_from_log1(lg.x), radius_from_log1(lg.y));
+    const V v = v_mul(vs<V>(-2.0f), lg);  // > 0
+    V y;
+    if constexpr (sizeof(V) == 4) y = rsqrtf(v);
+    else y = make_float2(rsqrtf(v.x), rsqrtf(v.y));
+    const V r = v_mul(v, y);
+    return v_fma(v_mul(vs<V>(0.5f), y), v_fma(v_neg(r), r, v), r);  // one Newton step
 }
 
 // cos(2 pi u2) alone (the real field draws only the cos branch): half-turn
@@ -221,14 +250,15 @@ __device__ __forceinline__ void half_turn_reduce(uint32_t h, uint32_t l, uint32_
     sign = q << 31;                                    // q = 2 shifts out: even
 }
 
-__device__ __forceinline__ float cos_series1(float x) {
-    const float x2 = __fmul_rn(x, x);
-    float c = __fmaf_rn(x2, 2.08767570e-9f, -2.75573192e-7f);  // 1/12!, -1/10!
-    c = __fmaf_rn(x2, c, 2.48015873e-5f);                      // 1/8!
-    c = __fmaf_rn(x2, c, -1.38888889e-3f);                     // -1/6!
-    c = __fmaf_rn(x2, c, 4.16666667e-2f);                      // 1/4!
-    c = __fmaf_rn(x2, c, -0.5f);
-    return __fmaf_rn(x2, c, 1.0f);
+template <typename V>
+__device__ __forceinline__ V cos_series(V x) {
+    const V x2 = v_mul(x, x);
+    V c = v_fma(x2, vs<V>(2.08767570e-9f), vs<V>(-2.75573192e-7f));  // 1/12!, -1/10!
+    c = v_fma(x2, c, vs<V>(2.48015873e-5f));                         // 1/8!
+    c = v_fma(x2, c, vs<V>(-1.38888889e-3f));                        // -1/6!
+    c = v_fma(x2, c, vs<V>(4.16666667e-2f));                         // 1/4!
+    c = v_fma(x2, c, vs<V>(-0.5f));
+    return v_fma(x2, c, vs<V>(1.0f));
 }
 
 __device__ __forceinline__ float flip_sign(float v, uint32_t sign) {
@@ -242,7 +272,7 @@ __device__ __forceinline__ float gauss_cos_f(uint64_t key) {
     float x;
     const float lg = log_u1(h1, l1);
     half_turn_reduce(h2, l2, sg, x);
-    return __fmul_rn(radius_from_log<float>(lg), flip_sign(cos_series1(x), sg));
+    return __fmul_rn(radius_from_log<float>(lg), flip_sign(cos_series<float>(x), sg));
 }
 
 // z for two keys in the two lanes of a float2 (bitwise the same as two calls
@@ -252,10 +282,11 @@ __device__ __forceinline__ float2 gauss_cos_f2(uint64_t key0, uint64_t key1) {
     hash_words(key0, h1a, l1a, h2a, l2a);
     hash_words(key1, h1b, l1b, h2b, l2b);
     float xa, xb;
-    const float2 lg = make_float2(log_u1(h1a, l1a), log_u1(h1b, l1b));
+    const float2 lg = log_u1_2(h1a, l1a, h1b, l1b);
     half_turn_reduce(h2a, l2a, sa, xa);
     half_turn_reduce(h2b, l2b, sb, xb);
-    const float2 c = make_float2(flip_sign(cos_series1(xa), sa), flip_sign(cos_series1(xb), sb));
+    const float2 cx = cos_series<float2>(make_float2(xa, xb));
+    const float2 c = make_float2(flip_sign(cx.x, sa), flip_sign(cx.y, sb));
     return v_mul(radius_from_log<float2>(lg), c);
 }
 
@@ -281,7 +312,7 @@ __device__ __forceinline__ void gauss_pair_f2(uint64_t key0, uint64_t key1, floa
     hash_words(key0, h1a, l1a, h2a, l2a);
     hash_words(key1, h1b, l1b, h2b, l2b);
     float xa, xb;
-    const float2 lg = make_float2(log_u1(h1a, l1a), log_u1(h1b, l1b));
+    const float2 lg = log_u1_2(h1a, l1a, h1b, l1b);
     angle_reduce(h2a, l2a, qa, xa);
     angle_reduce(h2b, l2b, qb, xb);
     float2 sn, cs;
@@ -297,8 +328,6 @@ __device__ __forceinline__ void gauss_pair_f2(uint64_t key0, uint64_t key1, floa
 // ------------------------------------------------------- float-float ----
 // Error-free sum (Knuth TwoSum) and a renormalised float-float add, in lane
 // vectors; every operation is an explicit round-to-nearest intrinsic.
-__device__ __forceinline__ float v_neg(float a) { return -a; }
-__device__ __forceinline__ float2 v_neg(float2 a) { return make_float2(-a.x, -a.y); }
 
 template <typename V>
 __device__ __forceinline__ void two_sum(V a, V b, V& s, V& e) {

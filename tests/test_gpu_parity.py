@@ -398,6 +398,26 @@ def test_observables_vs_oracle(storage):
     np.testing.assert_allclose(o, want, rtol=tol, atol=tol)
 
 
+@pytest.mark.parametrize("storage", ["f64", "f32", "f32c"])
+@pytest.mark.parametrize("shape", [(70, 12, 16), (1, 24, 32), (24, 32, 1), (5, 3, 2048)])
+def test_observables_marching_vs_oracle(storage, shape):
+    """Shapes with nz % 4 == 0 take the marching reduction (plane chunks of 64, the
+    i+1 / j+1 / k+1 wraps at the chunk and lattice edges)."""
+    rng = np.random.default_rng(22)
+    phi, pi = rng.normal(0.7, 0.6, shape), rng.normal(0, 0.4, shape)
+    if storage == "f32":
+        phi, pi = phi.astype(np.float32).astype(np.float64), pi.astype(np.float32).astype(np.float64)
+    o = observables(as_state(phi, storage), as_state(pi, storage), dx=0.8, inv_a2=0.9, lam=0.1,
+                    mphi=0.2, mu=1.1, thr=1.0).cpu().numpy()
+    r = O.observables(phi, pi, 0.8, 0.9, 0.1, 0.2, 1.1, 1.0)
+    want = np.array([r[k] for k in O.OBS_NAMES])
+    tol = 1e-12 if storage != "f32c" else 1e-7
+    np.testing.assert_allclose(o, want, rtol=tol, atol=tol)
+    o2 = observables(as_state(phi, storage), None).cpu().numpy()
+    r2 = O.observables(phi, None, 1.0, 1.0, 0.0, 0.0, 1.0, 1.0)
+    np.testing.assert_allclose(o2, np.array([r2[k] for k in O.OBS_NAMES]), rtol=tol, atol=tol)
+
+
 def test_observables_counts_nonfinite():
     phi = torch.zeros((8, 8, 8), dtype=torch.float64, device=DEV)
     phi[1, 2, 3] = float("nan")

@@ -157,6 +157,102 @@ __global__ void __launch_bounds__(kRedThreads) obs_partial_kernel(ObsParams p) {
     }
 }
 
+// Marching form for n2 % 4 == 0 (the bandwidth path).  A thread owns four
+// consecutive sites (j, k0..k0+3) of a row and walks a chunk of kObsPlanes
+// planes along i: plane i+1 is its i-neighbour and next centre, so every value
+// is read from memory once (the j+1 row and the k0+4 site come from the
+// neighbouring threads' reads through L1).  Block (x, y) reduces the 256
+// threads of column group x over plane chunk y; the partition depends on the
+// shape only.
+constexpr int kObsPlanes = 64;
+
+template <int S>
+__device__ __forceinline__ void load4(const void* f, int64_t s, int64_t N, double v[4]) {
+    if constexpr (S == TIPT_F64) {
+        const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(f) + s);
+        const double2 a = __ldg(q), b = __ldg(q + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else if constexpr (S == TIPT_F32) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(static_cast<const float*>(f) + s));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    } else {
+        const float* g = static_cast<const float*>(f);
+        const float4 h = __ldg(reinterpret_cast<const float4*>(g + s));
+        const float4 l = __ldg(reinterpret_cast<const float4*>(g + N + s));
+        v[0] = (double)h.x + (double)l.x;
+        v[1] = (double)h.y + (double)l.y;
+        v[2] = (double)h.z + (double)l.z;
+        v[3] = (double)h.w + (double)l.w;
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(kRedThreads) obs_march_kernel(ObsParams p) {
+    const int n0 = p.n0, n1 = p.n1, n2 = p.n2;
+    const int64_t n12 = (int64_t)n1 * n2;
+    const int64_t N = (int64_t)n0 * n12;
+    const int tpr = n2 >> 2;
+    const int64_t cols = (int64_t)n1 * tpr;
+    const int64_t col = (int64_t)blockIdx.x * kRedThreads + threadIdx.x;
+    ObsAcc a;
+    acc_init(a);
+    if (col < cols) {
+        const int j = (int)(col / tpr);
+        const int k0 = 4 * (int)(col - (int64_t)j * tpr);
+        const int64_t rj = (int64_t)j * n2 + k0;                          // in-plane offset
+        const int64_t rjp = (int64_t)(j + 1 < n1 ? j + 1 : 0) * n2 + k0;  // row j+1
+        const int64_t rkp = (int64_t)j * n2 + (k0 + 4 < n2 ? k0 + 4 : 0); // site k0+4
+        const int i0 = blockIdx.y * kObsPlanes;
+        const int ni = min(kObsPlanes, n0 - i0);
+        double ph[4], pn[4], pv[4], jp[4], kp;
+        load4<S>(p.phi, (int64_t)i0 * n12 + rj, N, ph);
+        for (int q = 0; q < ni; ++q) {
+            const int i = i0 + q;
+            const int64_t pc = (int64_t)i * n12;
+            const int64_t pnx = (int64_t)(i + 1 < n0 ? i + 1 : 0) * n12;
+            load4<S>(p.phi, pnx + rj, N, pn);
+            load4<S>(p.phi, pc + rjp, N, jp);
+            if (p.pi) load4<S>(p.pi, pc + rj, N, pv);
+            else pv[0] = pv[1] = pv[2] = pv[3] = 0.0;
+            kp = load_val<S>(p.phi, pc + rkp, N);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const double c = ph[u];
+                // forward differences, R:2303-2308
+                const double fx = pn[u] - c;
+                const double fy = jp[u] - c;
+                const double fz = (u < 3 ? ph[u + 1] : kp) - c;
+                a.grad += fx * fx + fy * fy + fz * fz;
+                const double c2 = c * c;
+                a.pot += (0.25 * p.lam * c2 * c2 - 0.5 * p.m2 * c2) * p.inv_mu2;
+                a.s1 += c;
+                a.s2 += c2;
+                a.sq += pv[u] * pv[u];
+                a.above += c > p.thr ? 1.0 : 0.0;
+                a.nonfinite += (isfinite(c) && isfinite(pv[u])) ? 0.0 : 1.0;
+                a.mn = fmin(a.mn, c);
+                a.mx = fmax(a.mx, c);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) ph[u] = pn[u];
+        }
+    }
+    a = block_reduce(a);
+    if (threadIdx.x == 0) {
+        double* o = p.partials + ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * kObs;
+        o[0] = 0.0;
+        o[1] = a.grad;
+        o[2] = a.pot;
+        o[3] = a.s1;
+        o[4] = a.s2;
+        o[5] = a.sq;
+        o[6] = a.above;
+        o[7] = a.mn;
+        o[8] = a.mx;
+        o[9] = a.nonfinite;
+    }
+}
+
 __global__ void __launch_bounds__(kRedThreads) obs_final_kernel(ObsParams p, int G, double inv_n) {
     ObsAcc a;
     acc_init(a);
@@ -198,7 +294,24 @@ int obs_blocks(int64_t rows) {
     return (int)g;
 }
 
-int64_t obs_workspace_bytes(int64_t rows) { return (int64_t)obs_blocks(rows) * kObs * 8; }
+// Grid of the marching form: (row groups of 256 four-site columns, plane chunks).
+static bool obs_march_grid(int n0, int n1, int n2, dim3& grid) {
+    if (n2 % 4 != 0 || n2 < 8) return false;
+    const int64_t cols = (int64_t)n1 * (n2 / 4);
+    const int64_t gx = (cols + kRedThreads - 1) / kRedThreads;
+    const int64_t gy = (n0 + kObsPlanes - 1) / kObsPlanes;
+    if (gx > 0x7fffffff || gy > 65535) return false;
+    grid = dim3((unsigned)gx, (unsigned)gy, 1);
+    return true;
+}
+
+int64_t obs_workspace_bytes(int n0, int n1, int n2) {
+    int64_t g = obs_blocks((int64_t)n0 * n1);
+    dim3 grid;
+    if (obs_march_grid(n0, n1, n2, grid) && (int64_t)grid.x * grid.y > g)
+        g = (int64_t)grid.x * grid.y;
+    return g * kObs * 8;
+}
 
 int launch_observables(int storage, const void* phi, const void* pi, int n0, int n1, int n2,
                        double dx, double inv_a2, double lam, double mphi, double mu, double thr,
@@ -218,11 +331,23 @@ int launch_observables(int storage, const void* phi, const void* pi, int n0, int
     p.partials = partials;
     p.out = out;
     const int64_t N = (int64_t)n0 * n1 * n2;
-    const int G = obs_blocks((int64_t)n0 * n1);
-    switch (storage) {
-        case TIPT_F64: obs_partial_kernel<TIPT_F64><<<G, kRedThreads, 0, st>>>(p); break;
-        case TIPT_F32: obs_partial_kernel<TIPT_F32><<<G, kRedThreads, 0, st>>>(p); break;
-        default: obs_partial_kernel<TIPT_F32C><<<G, kRedThreads, 0, st>>>(p); break;
+    int G = obs_blocks((int64_t)n0 * n1);
+    dim3 grid;
+    const bool march = (reinterpret_cast<uintptr_t>(phi) | reinterpret_cast<uintptr_t>(pi)) % 16 == 0 &&
+                       obs_march_grid(n0, n1, n2, grid);
+    if (march) {
+        G = (int)(grid.x * grid.y);
+        switch (storage) {
+            case TIPT_F64: obs_march_kernel<TIPT_F64><<<grid, kRedThreads, 0, st>>>(p); break;
+            case TIPT_F32: obs_march_kernel<TIPT_F32><<<grid, kRedThreads, 0, st>>>(p); break;
+            default: obs_march_kernel<TIPT_F32C><<<grid, kRedThreads, 0, st>>>(p); break;
+        }
+    } else {
+        switch (storage) {
+            case TIPT_F64: obs_partial_kernel<TIPT_F64><<<G, kRedThreads, 0, st>>>(p); break;
+            case TIPT_F32: obs_partial_kernel<TIPT_F32><<<G, kRedThreads, 0, st>>>(p); break;
+            default: obs_partial_kernel<TIPT_F32C><<<G, kRedThreads, 0, st>>>(p); break;
+        }
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "observables partial launch");
@@ -237,7 +362,9 @@ using namespace tipt;
 
 extern "C" int64_t tipt_observables_workspace_size(int64_t nx, int64_t ny, int64_t nz) {
     if (nx < 1 || ny < 1 || nz < 1) return 0;
-    return obs_workspace_bytes(nz == 1 ? nx : nx * ny);  // rows of the walk
+    // (nx, ny, 1) is walked as (1, nx, ny)
+    if (nz == 1) return obs_workspace_bytes(1, (int)nx, (int)ny);
+    return obs_workspace_bytes((int)nx, (int)ny, (int)nz);
 }
 
 extern "C" int tipt_observables(int storage, const void* phi, const void* pi, int64_t nx,
@@ -257,7 +384,7 @@ extern "C" int tipt_observables(int storage, const void* phi, const void* pi, in
         ny = nx;
         nx = 1;
     }
-    const int64_t need = obs_workspace_bytes(nx * ny);
+    const int64_t need = obs_workspace_bytes((int)nx, (int)ny, (int)nz);
     if (workspace_bytes < need)
         return fail(TIPT_ERR_ARG, "workspace of %lld bytes is smaller than the %lld needed",
                     (long long)workspace_bytes, (long long)need);

@@ -83,25 +83,12 @@ __device__ __forceinline__ float2 v_atleast(float2 a, float m) {
 template <typename V>
 __device__ __forceinline__ V cvprime_v(const ComplexStageParams& p, const float* s_tab, V x,
                                        float tmin, float dinv) {
-    constexpr int NL = sizeof(V) / sizeof(float);
     if (p.vkind == TIPT_VP_POLY) {
         const V d = v_fma(v_mul(v_mul(vs<V>((float)p.c3), x), x), x, v_mul(vs<V>((float)p.c1), x));
         return p.c2 != 0.0 ? v_fma(v_mul(vs<V>((float)p.c2), x), x, d) : d;
     }
-    const V fidx = v_mul(v_sub(x, vs<V>(tmin)), vs<V>(dinv));
-    const float last = (float)(p.npts - 2);
-    V fi, a, b;
-#pragma unroll
-    for (int l = 0; l < NL; ++l) {
-        float c = vlane(fidx, l);
-        c = c > 0.0f ? c : 0.0f;
-        c = c < last ? c : last;
-        const int idx = (int)c;
-        vset(fi, l, (float)idx);
-        vset(a, l, s_tab[idx]);
-        vset(b, l, s_tab[idx + 1]);
-    }
-    return v_fma(v_sub(fidx, fi), v_sub(b, a), a);
+    return lerp_table_f32<V>(s_tab, v_mul(v_sub(x, vs<V>(tmin)), vs<V>(dinv)),
+                             (float)(p.npts - 2));
 }
 
 // dV/dphi_a of V(rho) + eps Re(Phi^4): V'(rho) phi_a / rho plus

@@ -483,7 +483,13 @@ __global__ void __maxnreg__(kMarchRegs)
                     const float4 jp = *reinterpret_cast<const float4*>(sc + drow + k0);
                     const float4 im = *reinterpret_cast<const float4*>(blk(pm.stage, f, c) + orow + k0);
                     const float4 ip = *reinterpret_cast<const float4*>(blk(pp.stage, f, c) + orow + k0);
-                    const float kl = sc[orow + kml], kr = sc[orow + kpr];
+                    // k-1 of site 0 and k+1 of site 3 are the neighbouring lanes' end
+                    // values (shuffles); shared-memory reads only at warp and row ends,
+                    // which keeps the four-site stride off conflicting banks
+                    float kl = __shfl_up_sync(0xffffffffu, ce.w, 1);
+                    float kr = __shfl_down_sync(0xffffffffu, ce.x, 1);
+                    if (lane == 0 || k0 == 0) kl = sc[orow + kml];
+                    if (lane == 31 || k0 + 4 == n2) kr = sc[orow + kpr];
                     // site pairs (0,1) and (2,3): centre and the six neighbours
                     const float2 cc[2] = {make_float2(ce.x, ce.y), make_float2(ce.z, ce.w)};
                     const float2 nb[2][6] = {
@@ -727,8 +733,12 @@ __global__ void __maxnreg__(kMarchRegs)
                     const float2 jp = *reinterpret_cast<const float2*>(sc + drow + k0);
                     const float2 im = *reinterpret_cast<const float2*>(blk(pm.stage, f, c) + orow + k0);
                     const float2 ip = *reinterpret_cast<const float2*>(blk(pp.stage, f, c) + orow + k0);
-                    const float kl = (split && edge_l) ? hv[2 * f + c] : sc[orow + kml];
-                    const float kr = (split && edge_r) ? hv[2 * f + c] : sc[orow + kpr];
+                    // k-1 / k+1 from the neighbouring lanes; at warp, row and segment
+                    // ends from shared memory or the copied segment halo
+                    float kl = __shfl_up_sync(0xffffffffu, ce.y, 1);
+                    float kr = __shfl_down_sync(0xffffffffu, ce.x, 1);
+                    if (lane == 0 || edge_l) kl = (split && edge_l) ? hv[2 * f + c] : sc[orow + kml];
+                    if (lane == 31 || edge_r) kr = (split && edge_r) ? hv[2 * f + c] : sc[orow + kpr];
                     // lanes = sites k0, k0+1; neighbours in the order ip, im, jp, jm, kp, km
                     const float2 nb[6] = {ip, im, jp, jm, make_float2(ce.y, kr), make_float2(kl, ce.x)};
                     float2 acc;

@@ -98,13 +98,6 @@ __device__ __forceinline__ double vprime_d(const RealStageParams& p, const doubl
 // V'(x) in FP32 (F32C storage) for a lane vector: the polynomial, the float
 // row staged in shared memory, or (long 1-D tables) the FP64 table in global
 // memory.  Lane by lane the same operations as lerp_table<float>.
-__device__ __forceinline__ float vlane(float v, int) { return v; }
-__device__ __forceinline__ float vlane(float2 v, int l) { return l ? v.y : v.x; }
-__device__ __forceinline__ void vset(float& v, int, float x) { v = x; }
-__device__ __forceinline__ void vset(float2& v, int l, float x) {
-    if (l) v.y = x;
-    else v.x = x;
-}
 
 // FP32 constants of a compensated-FP32 stage, rounded once per launch from the
 // FP64 parameters (after the schedule is resolved) and passed to the per-site
@@ -152,20 +145,7 @@ __device__ __forceinline__ V vprime_v(const RealStageParams& p, const F32CConst&
                                                  (double)vlane(x, l)));
         return r;
     }
-    const V fidx = v_mul(v_sub(x, vs<V>(kc.tmin)), vs<V>(kc.dinv));
-    const float last = kc.last;
-    V fi, a, b;
-#pragma unroll
-    for (int l = 0; l < NL; ++l) {
-        float c = vlane(fidx, l);
-        c = c > 0.0f ? c : 0.0f;
-        c = c < last ? c : last;
-        const int idx = (int)c;
-        vset(fi, l, (float)idx);
-        vset(a, l, s_tab[idx]);
-        vset(b, l, s_tab[idx + 1]);
-    }
-    return v_fma(v_sub(fidx, fi), v_sub(b, a), a);
+    return lerp_table_f32<V>(s_tab, v_mul(v_sub(x, vs<V>(kc.tmin)), vs<V>(kc.dinv)), kc.last);
 }
 
 // Noise increment for one site (FP64): array value * nfac, or ns_eff * z.

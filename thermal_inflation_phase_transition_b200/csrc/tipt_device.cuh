@@ -369,6 +369,34 @@ __device__ __forceinline__ R lerp_table(const R* __restrict__ t, R tmin, R dinv,
     return rn_fma(frac, rn_sub(t[idx + 1], a), a);
 }
 
+// FP32 lookup in a V' row staged in shared memory, for a lane vector of
+// fractional indices fidx = (x - tmin) dinv: the lerp_table rule lane by lane
+// (index clamped to [0, last], fraction unclamped).
+__device__ __forceinline__ float vlane(float v, int) { return v; }
+__device__ __forceinline__ float vlane(float2 v, int l) { return l ? v.y : v.x; }
+__device__ __forceinline__ void vset(float& v, int, float x) { v = x; }
+__device__ __forceinline__ void vset(float2& v, int l, float x) {
+    if (l) v.y = x;
+    else v.x = x;
+}
+
+template <typename V>
+__device__ __forceinline__ V lerp_table_f32(const float* s_tab, V fidx, float last) {
+    constexpr int NL = sizeof(V) / sizeof(float);
+    V fi, a, b;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        float c = vlane(fidx, l);
+        c = c > 0.0f ? c : 0.0f;
+        c = c < last ? c : last;
+        const int idx = (int)c;
+        vset(fi, l, (float)idx);
+        vset(a, l, s_tab[idx]);
+        vset(b, l, s_tab[idx + 1]);
+    }
+    return v_fma(v_sub(fidx, fi), v_sub(b, a), a);
+}
+
 // Polynomial V'(x) = c1 x + c2 x^2 + c3 x^3 (zero-coupling inline V', R:2228:
 // dV = lam*ph*ph*ph - mphi_sq*ph, evaluated in that order).
 template <typename R>

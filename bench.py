@@ -245,6 +245,10 @@ def main():
                     default="lattice",
                     help="lattice: the 512^3 site-update headline; ensemble: Gamma estimates "
                          "per GPU-hour of the batched replica engine vs one-at-a-time launches")
+    ap.add_argument("--decomp", choices=["replicas", "slab"], default="replicas",
+                    help="N > 1: independent n^3 replicas per rank (default), or one "
+                         "(N n) x n x n lattice in x-slabs of n planes per rank with a halo "
+                         "exchange of the ghost planes every step (slab.Slab)")
     ap.add_argument("--ens-steps", type=int, default=2000)
     ap.add_argument("--ens-plain", type=int, default=6,
                     help="replicas per size class timed one at a time")
@@ -301,6 +305,15 @@ def main():
         return [a, b], [torch.empty_like(a), torch.empty_like(b)]
 
     cur, nxt = make_state()
+    slab = None
+    if args.decomp == "slab":
+        from thermal_inflation_phase_transition_b200.slab import Slab
+        slab = Slab((world * n, n, n), rank=rank, world=world)
+        loc = [slab.empty(args.storage, dev) for _ in range(4)]
+        for a, b in zip(loc[:2], cur):
+            slab.interior(a).copy_(b)
+        cur, nxt = loc[:2], loc[2:]
+        seed = 1  # one lattice: the noise is keyed by the lattice-wide site index
     stream = torch.cuda.current_stream()
     # per-step V' sources prepared outside the timed region (they only pack scalars)
     total = args.warmup + args.steps
@@ -309,8 +322,13 @@ def main():
     def step(s):
         nonlocal cur, nxt
         T = temperature(s)
-        RF.rk2_step_table_into(cur[0], cur[1], nxt[0], nxt[1], DT, DX, ETA, 1.0, 1.0,
-                               vsources[s], noise_scale=noise_scale(T), noise_step=s, seed=seed)
+        if slab is not None:  # ghost-plane exchange, then the slab's planes
+            slab.step(cur[0], cur[1], nxt[0], nxt[1], DT, DX, ETA, 1.0, 1.0, vsources[s],
+                      noise_scale=noise_scale(T), noise_step=s, seed=seed)
+        else:
+            RF.rk2_step_table_into(cur[0], cur[1], nxt[0], nxt[1], DT, DX, ETA, 1.0, 1.0,
+                                   vsources[s], noise_scale=noise_scale(T), noise_step=s,
+                                   seed=seed)
         cur, nxt = nxt, cur
 
     for s in range(args.warmup):
@@ -342,11 +360,13 @@ def main():
     achieved = bps * N / (per_step_ms / 1000.0) / 1e9
     traffic = read_traffic(args.storage, n)
     # sanity: the state really advanced and stayed finite
+    if slab is not None:
+        slab.exchange(cur[0], cur[1])  # the last outputs' ghost planes
     o = observables(cur[0], cur[1]).cpu().numpy()
     finite_ok = bool(o[9] == 0)
 
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and slab is None:
         e2e = run_e2e(args, shape, seed, RF, observables, torch, dev, world)
 
     cpu = None
@@ -368,7 +388,10 @@ def main():
                        "storage": args.storage, "state_bytes": bps // 2 * N,
                        "l2": "inputs larger than L2 (state %.1f GB vs 126 MB L2)"
                              % (bps * N / 1e9),
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "parallelism": (f"x-slabs x{world} of a {world * n}x{n}x{n} lattice, "
+                                       "ghost-plane exchange every step"
+                                       if slab is not None else
+                                       f"replicas x{world}" if world > 1 else "single GPU"),
                        "finite_after_run": finite_ok},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

@@ -121,6 +121,22 @@ int tipt_rk2_step_table(int storage, const void* phi, const void* pi, void* phi_
                         const tipt_step_params* sp, const tipt_vsource* vp, const void* noise,
                         void* stream);
 
+/* rk2_step_table on one x-slab of a lattice of nx_global x ny x nz sites split
+ * along x across ranks (the multi-GPU form; no reference counterpart -- the
+ * reference's only decomposition is CosmoLattice's MPI slabs,
+ * simulation/run_cosmolattice.py:148-152).  The arrays hold nx_local + 2
+ * planes: plane 0 is lattice plane i_lo - 1 and plane nx_local + 1 is lattice
+ * plane i_lo + nx_local (both modulo nx_global; the ghost planes, filled by
+ * the caller's halo exchange before the call), planes 1..nx_local are lattice
+ * planes i_lo .. i_lo + nx_local - 1.  Computes planes 1..nx_local into
+ * phi_out / pi_out (their ghost planes are not written) with the inline hash
+ * noise keyed by the lattice-wide site index, so the ranks together reproduce
+ * the single-lattice step bit for bit.  nz >= 2. */
+int tipt_rk2_step_table_slab(int storage, const void* phi, const void* pi, void* phi_out,
+                             void* pi_out, int64_t nx_local, int64_t ny, int64_t nz, int64_t i_lo,
+                             int64_t nx_global, const tipt_step_params* sp,
+                             const tipt_vsource* vp, void* stream);
+
 /* rk2_step_table with the per-step scalars read on the device, for step loops
  * captured once into a CUDA graph and replayed (the reference's host loop
  * R:3619-3768 recomputes them each step on the host).  The step index is
@@ -255,6 +271,17 @@ int tipt_observables(int storage, const void* phi, const void* pi, int64_t nx, i
                      int64_t nz, double dx, double inv_a2, double lam, double mphi, double mu,
                      double thr, double* out, void* workspace, int64_t workspace_bytes,
                      void* stream);
+
+/* tipt_observables over the computed planes 1..nx_local of a slab laid out as
+ * for tipt_rk2_step_table_slab (the forward difference of the last plane reads
+ * the upper ghost plane): means are divided by n_global_sites, so the sums over
+ * ranks of out[0..6] and out[9] and the min / max over ranks of out[7] / out[8]
+ * give the lattice's observables.  workspace: tipt_observables_workspace_size(
+ * nx_local + 2, ny, nz) bytes. */
+int tipt_observables_slab(int storage, const void* phi, const void* pi, int64_t nx_local,
+                          int64_t ny, int64_t nz, int64_t n_global_sites, double dx,
+                          double inv_a2, double lam, double mphi, double mu, double thr,
+                          double* out, void* workspace, int64_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------ other integrators
  * The reference's alternative integrators with counter-based hash noise (key

@@ -77,6 +77,8 @@ _SIGS = {
                              _p],
     "tipt_rk2_step_table_sched": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
                                   C.POINTER(VSource), _p, _i64, _p, _i64, _p],
+    "tipt_rk2_step_table_slab": [_i, _p, _p, _p, _p, _i64, _i64, _i64, _i64, _i64,
+                                 C.POINTER(StepParams), C.POINTER(VSource), _p],
     "tipt_counter_add": [_p, _i64, _p],
     "tipt_ensemble_step": [_i, _p, _p, _p, _p, _i64, _p, _p, C.c_int32, _p,
                            C.POINTER(StepParams), _p, _i64, _p],
@@ -92,6 +94,8 @@ _SIGS = {
     "tipt_observables_workspace_size": [_i64, _i64, _i64],
     "tipt_observables": [_i, _p, _p, _i64, _i64, _i64, _d, _d, _d, _d, _d, _d, _p, _p, _i64,
                          _p],
+    "tipt_observables_slab": [_i, _p, _p, _i64, _i64, _i64, _i64, _d, _d, _d, _d, _d, _d, _p,
+                              _p, _i64, _p],
     "tipt_overdamped_step_table": [_i, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
                                    C.POINTER(VSource), _p],
     "tipt_baoab_step_table": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),

@@ -204,6 +204,31 @@ int tipt_rk2_step_table(int storage, const void* phi, const void* pi, void* phi_
     return launch_real_stage(storage, p, (cudaStream_t)stream);
 }
 
+int tipt_rk2_step_table_slab(int storage, const void* phi, const void* pi, void* phi_out,
+                             void* pi_out, int64_t nx_local, int64_t ny, int64_t nz, int64_t i_lo,
+                             int64_t nx_global, const tipt_step_params* sp,
+                             const tipt_vsource* vp, void* stream) {
+    int rc;
+    if (nx_local < 1 || nz < 2) return fail(TIPT_ERR_ARG, "slab needs nx_local >= 1 and nz >= 2");
+    if (i_lo < 0 || i_lo + nx_local > nx_global)
+        return fail(TIPT_ERR_ARG, "slab planes [%lld, %lld) outside the %lld-plane lattice",
+                    (long long)i_lo, (long long)(i_lo + nx_local), (long long)nx_global);
+    if ((rc = check_state(storage, phi, pi, phi_out, pi_out, nx_local + 2, ny, nz))) return rc;
+    if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
+    if ((rc = check_vsource(vp, "vp"))) return rc;
+    RealStageParams p = stage_params(phi, pi, phi_out, pi_out, nx_local + 2, ny, nz, sp, vp);
+    p.h1 = 0.5 * sp->dt;
+    p.h2 = sp->dt;
+    p.noise = nullptr;
+    p.nfac = 1.0;
+    p.ns_eff = sp->noise_scale;
+    p.mul = kPass2Mul;
+    p.i_begin = 1;
+    p.i_end = (int)nx_local + 1;
+    p.site_offset = (long long)(i_lo - 1) * ny * nz;  // array plane 1 = lattice plane i_lo
+    return launch_real_stage(storage, p, (cudaStream_t)stream);
+}
+
 int tipt_rk2_step_table_sched(int storage, const void* phi, const void* pi, void* phi_out,
                               void* pi_out, int64_t nx, int64_t ny, int64_t nz,
                               const tipt_step_params* sp, const tipt_vsource* vp,

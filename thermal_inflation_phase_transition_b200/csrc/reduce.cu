@@ -87,6 +87,7 @@ struct ObsParams {
     const void* phi;
     const void* pi;
     int n0, n1, n2;
+    int i_begin, i_end;  // planes reduced (the i+1 neighbour of the last may lie outside)
     double inv_dx2, inv_a2, lam, m2, inv_mu2, thr;
     double* partials;  // [G][kObs]
     double* out;       // [kObs]
@@ -121,13 +122,13 @@ template <int S>
 __global__ void __launch_bounds__(kRedThreads) obs_partial_kernel(ObsParams p) {
     const int64_t n12 = (int64_t)p.n1 * p.n2;
     const int64_t N = (int64_t)p.n0 * n12;
-    const int64_t rows = (int64_t)p.n0 * p.n1;
+    const int64_t rows = (int64_t)p.i_end * p.n1;
     const int lane = threadIdx.x & 31;
     const int wpb = kRedThreads / 32;
     ObsAcc a;
     acc_init(a);
-    for (int64_t row = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); row < rows;
-         row += (int64_t)gridDim.x * wpb) {
+    for (int64_t row = (int64_t)p.i_begin * p.n1 + (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5);
+         row < rows; row += (int64_t)gridDim.x * wpb) {
         const int64_t i = row / p.n1;
         const int64_t j = row - i * p.n1;
         const int64_t ox = (i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12;
@@ -202,8 +203,8 @@ __global__ void __launch_bounds__(kRedThreads) obs_march_kernel(ObsParams p) {
         const int64_t rj = (int64_t)j * n2 + k0;                          // in-plane offset
         const int64_t rjp = (int64_t)(j + 1 < n1 ? j + 1 : 0) * n2 + k0;  // row j+1
         const int64_t rkp = (int64_t)j * n2 + (k0 + 4 < n2 ? k0 + 4 : 0); // site k0+4
-        const int i0 = blockIdx.y * kObsPlanes;
-        const int ni = min(kObsPlanes, n0 - i0);
+        const int i0 = p.i_begin + blockIdx.y * kObsPlanes;
+        const int ni = min(kObsPlanes, p.i_end - i0);
         double ph[4], pn[4], pv[4], jp[4], kp;
         load4<S>(p.phi, (int64_t)i0 * n12 + rj, N, ph);
         for (int q = 0; q < ni; ++q) {
@@ -294,7 +295,8 @@ int obs_blocks(int64_t rows) {
     return (int)g;
 }
 
-// Grid of the marching form: (row groups of 256 four-site columns, plane chunks).
+// Grid of the marching form over n0 planes: (row groups of 256 four-site
+// columns, plane chunks).
 static bool obs_march_grid(int n0, int n1, int n2, dim3& grid) {
     if (n2 % 4 != 0 || n2 < 8) return false;
     const int64_t cols = (int64_t)n1 * (n2 / 4);
@@ -313,15 +315,20 @@ int64_t obs_workspace_bytes(int n0, int n1, int n2) {
     return g * kObs * 8;
 }
 
+// Reduces planes [i_begin, i_end) of an n0-plane array; means are taken over
+// n_sites (the whole lattice, also when the array is one slab of it).
 int launch_observables(int storage, const void* phi, const void* pi, int n0, int n1, int n2,
-                       double dx, double inv_a2, double lam, double mphi, double mu, double thr,
-                       double* out, double* partials, cudaStream_t st) {
+                       int i_begin, int i_end, double n_sites, double dx, double inv_a2,
+                       double lam, double mphi, double mu, double thr, double* out,
+                       double* partials, cudaStream_t st) {
     ObsParams p;
     p.phi = phi;
     p.pi = pi;
     p.n0 = n0;
     p.n1 = n1;
     p.n2 = n2;
+    p.i_begin = i_begin;
+    p.i_end = i_end;
     p.inv_dx2 = 1.0 / (dx * dx);
     p.inv_a2 = inv_a2;
     p.lam = lam;
@@ -330,11 +337,11 @@ int launch_observables(int storage, const void* phi, const void* pi, int n0, int
     p.thr = thr;
     p.partials = partials;
     p.out = out;
-    const int64_t N = (int64_t)n0 * n1 * n2;
-    int G = obs_blocks((int64_t)n0 * n1);
+    const int planes = i_end - i_begin;
+    int G = obs_blocks((int64_t)planes * n1);
     dim3 grid;
     const bool march = (reinterpret_cast<uintptr_t>(phi) | reinterpret_cast<uintptr_t>(pi)) % 16 == 0 &&
-                       obs_march_grid(n0, n1, n2, grid);
+                       obs_march_grid(planes, n1, n2, grid);
     if (march) {
         G = (int)(grid.x * grid.y);
         switch (storage) {
@@ -351,7 +358,7 @@ int launch_observables(int storage, const void* phi, const void* pi, int n0, int
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "observables partial launch");
-    obs_final_kernel<<<1, kRedThreads, 0, st>>>(p, G, 1.0 / (double)N);
+    obs_final_kernel<<<1, kRedThreads, 0, st>>>(p, G, 1.0 / n_sites);
     e = cudaGetLastError();
     return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "observables final launch");
 }
@@ -388,7 +395,33 @@ extern "C" int tipt_observables(int storage, const void* phi, const void* pi, in
     if (workspace_bytes < need)
         return fail(TIPT_ERR_ARG, "workspace of %lld bytes is smaller than the %lld needed",
                     (long long)workspace_bytes, (long long)need);
-    return launch_observables(storage, phi, pi, (int)nx, (int)ny, (int)nz, dx, inv_a2, lam, mphi,
-                              mu, thr, out, static_cast<double*>(workspace),
-                              (cudaStream_t)stream);
+    return launch_observables(storage, phi, pi, (int)nx, (int)ny, (int)nz, 0, (int)nx,
+                              (double)(nx * ny * nz), dx, inv_a2, lam, mphi, mu, thr, out,
+                              static_cast<double*>(workspace), (cudaStream_t)stream);
+}
+
+extern "C" int tipt_observables_slab(int storage, const void* phi, const void* pi,
+                                     int64_t nx_local, int64_t ny, int64_t nz,
+                                     int64_t n_global_sites, double dx, double inv_a2, double lam,
+                                     double mphi, double mu, double thr, double* out,
+                                     void* workspace, int64_t workspace_bytes, void* stream) {
+    int rc;
+    if (nx_local < 1 || nz < 2)
+        return fail(TIPT_ERR_ARG, "slab needs nx_local >= 1 and nz >= 2");
+    const int64_t n0 = nx_local + 2;
+    if ((rc = check_storage(storage)) || (rc = check_dims(n0, ny, nz))) return rc;
+    if (n_global_sites < nx_local * ny * nz)
+        return fail(TIPT_ERR_ARG, "n_global_sites smaller than the slab");
+    const int eb = elem_align(storage);
+    if ((rc = check_ptr(phi, eb, "phi")) || (rc = check_ptr(out, 8, "out")) ||
+        (rc = check_ptr(workspace, 8, "workspace")))
+        return rc;
+    if (pi && (rc = check_ptr(pi, eb, "pi"))) return rc;
+    const int64_t need = obs_workspace_bytes((int)n0, (int)ny, (int)nz);
+    if (workspace_bytes < need)
+        return fail(TIPT_ERR_ARG, "workspace of %lld bytes is smaller than the %lld needed",
+                    (long long)workspace_bytes, (long long)need);
+    return launch_observables(storage, phi, pi, (int)n0, (int)ny, (int)nz, 1, (int)nx_local + 1,
+                              (double)n_global_sites, dx, inv_a2, lam, mphi, mu, thr, out,
+                              static_cast<double*>(workspace), (cudaStream_t)stream);
 }

@@ -239,8 +239,8 @@ __global__ void __maxnreg__(kMarchRegs)
         bool ok = true;
         for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
             const int ic = item / g.nJB;
-            const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
-            const int npl = min(g.CI, n0 - i0) + 2;
+            const int j0 = (item - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
+            const int npl = min(g.CI, p.i_end - i0) + 2;
             for (int q = 0; q < npl; ++q) {
                 // stage w.stage last held position issued - NS, released in phase w.phase ^ 1
                 if (issued >= NS && !mbar_wait(&empty[w.stage], w.phase ^ 1u)) {
@@ -285,8 +285,8 @@ __global__ void __maxnreg__(kMarchRegs)
     RingPos pm{0, 0};  // ring position of plane i-1 for the current iteration
     for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
         const int ic = item / g.nJB;
-        const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
-        const int ni = min(g.CI, n0 - i0);
+        const int j0 = (item - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
+        const int ni = min(g.CI, p.i_end - i0);
         const int jw = j0 + r - 1;
         RingPos pc = pm, pp;
         pc.next(NS);
@@ -333,8 +333,8 @@ __global__ void __maxnreg__(kMarchRegs)
                     const E pv[7] = {ce[1][u], ip[1][u], im[1][u], jp[1][u], jm[1][u],
                                      u ? kr[1] : ce[1][1], u ? ce[1][0] : kl[1]};
                     uint64_t site;
-                    if constexpr (WIDE) site = (uint64_t)(rowoff + col + u);
-                    else site = (uint32_t)rowoff + (uint32_t)(col + u);
+                    if constexpr (WIDE) site = (uint64_t)(rowoff + p.site_offset + col + u);
+                    else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)(col + u);
                     site_update<S>(p, s_tab, tminf, dinvf, ph, pv, site, op[u], ov[u]);
                 }
                 st_pair_g(phi_out + rowoff + col, op[0], op[1]);
@@ -410,8 +410,8 @@ __global__ void __maxnreg__(kMarchRegs)
         bool ok = true;
         for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
             const int ic = item / g.nJB;
-            const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
-            const int npl = min(g.CI, n0 - i0) + 2;
+            const int j0 = (item - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
+            const int npl = min(g.CI, p.i_end - i0) + 2;
             for (int q = 0; q < npl; ++q) {
                 if (issued >= NS && !mbar_wait(&empty[w.stage], w.phase ^ 1u)) {
                     ok = false;
@@ -454,8 +454,8 @@ __global__ void __maxnreg__(kMarchRegs)
     RingPos pm{0, 0};
     for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
         const int ic = item / g.nJB;
-        const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
-        const int ni = min(g.CI, n0 - i0);
+        const int j0 = (item - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
+        const int ni = min(g.CI, p.i_end - i0);
         const int jw = j0 + r - 1;
         RingPos pc = pm, pp;
         pc.next(NS);
@@ -526,8 +526,8 @@ __global__ void __maxnreg__(kMarchRegs)
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 uint64_t site;
-                if constexpr (WIDE) site = (uint64_t)(rowoff + 2 * h);
-                else site = (uint32_t)rowoff + (uint32_t)(2 * h);
+                if constexpr (WIDE) site = (uint64_t)(rowoff + p.site_offset + 2 * h);
+                else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)(2 * h);
                 update_f32c<float2>(p, kc, s_tab, in[h], site_kick_f32c2(p, kc, site), o[h][0],
                                     o[h][1], o[h][2], o[h][3]);
             }
@@ -872,8 +872,9 @@ static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, 
     g.pitch = (n2 + per128 - 1) / per128 * per128;
     const int tpr = n2 / 4;
     g.tab_bytes = round128((int)smem_table);
+    const int nplanes = p.i_end - p.i_begin;
     g.CI = g_force_ci > 0 ? g_force_ci : 64;
-    if (g.CI > p.n0) g.CI = p.n0;
+    if (g.CI > nplanes) g.CI = nplanes;
     // Candidates: TJ with TJ*tpr consumers a multiple of 32 in [32, 512], ring
     // depth S in [3, 5].  Score = consumer warps per SM x TJ/(TJ+2) (the share
     // of loaded rows that are not halo), deeper rings preferred on ties.
@@ -905,7 +906,7 @@ static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, 
     // 16-byte row length (n2 % 4 == 0)
     if ((g.pitch * es) % 128 || g.stage_bytes % (256 * np) || g.tab_bytes % 128) return false;
     g.nJB = n1 / g.TJ;
-    g.nIC = (p.n0 + g.CI - 1) / g.CI;
+    g.nIC = (nplanes + g.CI - 1) / g.CI;
     g.items = g.nJB * g.nIC;
     smem = smem_need(g);
     return true;
@@ -950,7 +951,9 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
     int64_t smem;
     if (!geometry(storage, p, smem_table, g, smem))
         return fail(TIPT_ERR_UNSUPPORTED, "marching kernel geometry");
-    const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
+    // 64-bit noise-key sites when an index (array + offset) can exceed 32 bits
+    const bool wide = (int64_t)p.n0 * p.n1 * p.n2 + (p.site_offset > 0 ? p.site_offset : 0) >
+                      0xFFFFFFFFll;
     if (storage == TIPT_F32C)
         return wide ? launch_march_k(rk2_stage_march_f32c<true>, p, g, smem, st)
                     : launch_march_k(rk2_stage_march_f32c<false>, p, g, smem, st);

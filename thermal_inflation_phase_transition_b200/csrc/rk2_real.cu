@@ -22,8 +22,9 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
 
     const int64_t n12 = (int64_t)p.n1 * p.n2;
     const int64_t N = (int64_t)p.n0 * n12;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < N;
-         s += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s_end = (int64_t)p.i_end * n12;
+    for (int64_t s = (int64_t)p.i_begin * n12 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+         s < s_end; s += (int64_t)gridDim.x * blockDim.x) {
         const int k = (int)(s % p.n2);
         const int64_t r = s / p.n2;
         const int j = (int)(r % p.n1);
@@ -46,7 +47,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
             }
             double a, b;
             update_f64(p, reinterpret_cast<const double*>(s_tab), ph, pv,
-                       site_noise<double>(p, (uint64_t)s), a, b);
+                       site_noise<double>(p, (uint64_t)(s + p.site_offset)), a, b);
             static_cast<double*>(p.phi_out)[s] = a;
             static_cast<double*>(p.pi_out)[s] = b;
         } else if constexpr (S == TIPT_F32) {
@@ -60,7 +61,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
             }
             float a, b;
             update_f32(p, reinterpret_cast<const double*>(s_tab), ph, pv,
-                       site_noise<float>(p, (uint64_t)s), a, b);
+                       site_noise<float>(p, (uint64_t)(s + p.site_offset)), a, b);
             static_cast<float*>(p.phi_out)[s] = a;
             static_cast<float*>(p.pi_out)[s] = b;
         } else {
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
             x.pil = vl[0];
             float a, b, c, d;
             update_f32c<float>(p, kc, reinterpret_cast<const float*>(s_tab), x,
-                               site_kick_f32c(p, kc, (uint64_t)s), a, b, c, d);
+                               site_kick_f32c(p, kc, (uint64_t)(s + p.site_offset)), a, b, c, d);
             float* po = static_cast<float*>(p.phi_out);
             float* vo = static_cast<float*>(p.pi_out);
             po[s] = a;
@@ -120,7 +121,7 @@ static int launch_generic(RealStageParams p, int64_t smem, cudaStream_t st) {
                                              (int)smem);
         if (e != cudaSuccess) return fail_cuda(e, "rk2_stage_generic smem attribute");
     }
-    const int64_t N = (int64_t)p.n0 * p.n1 * p.n2;
+    const int64_t N = (int64_t)(p.i_end - p.i_begin) * p.n1 * p.n2;
     int64_t blocks = (N + 255) / 256;
     const int64_t cap = (int64_t)num_sms() * 8;
     if (blocks > cap) blocks = cap;
@@ -155,7 +156,11 @@ static void canonical_shape(RealStageParams& p) {
 }
 
 int launch_real_stage(int storage, RealStageParams p, cudaStream_t st) {
-    canonical_shape(p);
+    if (p.i_end == 0) {
+        canonical_shape(p);
+        p.i_begin = 0;
+        p.i_end = p.n0;
+    }
     const int64_t tb = table_smem_bytes(storage, p);
     p.table_in_smem = (tb > 0 && tb <= kMaxTableSmem) ? 1 : 0;
     if (p.vkind == TIPT_VP_TABLE2D && !p.table_in_smem)

@@ -42,6 +42,11 @@ struct RealStageParams {
     long long offset;
     long long sched_len;  // steps beyond the schedule reuse its last entry
     double ns_mult;
+    // Planes computed: [i_begin, i_end) of the n0 planes (all planes, periodic
+    // in i, when i_end = 0); the noise key's site is the array index plus
+    // site_offset (a slab of a larger lattice keys by the global index).
+    int i_begin, i_end;
+    long long site_offset;
 };
 
 // Resolve the per-step scalars of a scheduled launch (no-op otherwise).

@@ -241,7 +241,7 @@ def main():
     ap.add_argument("--storage", choices=["f32c", "f64", "f32"], default="f32c")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["lattice", "complex", "ensemble", "surrogate"],
+    ap.add_argument("--workload", choices=["lattice", "complex", "ensemble", "surrogate", "extras"],
                     default="lattice",
                     help="lattice: the 512^3 site-update headline; ensemble: Gamma estimates "
                          "per GPU-hour of the batched replica engine vs one-at-a-time launches")
@@ -262,6 +262,9 @@ def main():
         return
     if args.workload == "complex" and args.impl == "tipt":
         run_complex_bench(args)
+        return
+    if args.workload == "extras" and args.impl == "tipt":
+        run_extras_bench(args)
         return
 
     if args.impl == "reference":
@@ -626,6 +629,190 @@ def run_complex_bench(args):
         "gpu_launches": args.steps, "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
+
+
+def _dev_ms(fn, reps, warm=3):
+    """Mean device time of fn() over reps calls (CUDA events, after warm-up)."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_extras_bench(args):
+    """The components beyond the RK2 stepper, each on the device with a CPU path of the
+    reference's algorithm timed beside it on the host:
+      * overdamped Euler-Maruyama and BAOAB (R:2115, R:1974), 512^3 compensated FP32,
+        1-D V' table (4096 points) at T = 1.0, hash noise; algorithmic bytes per site:
+        16 (overdamped: phi hi+lo read and written) and 32 (BAOAB: phi and pi);
+        CPU: the numpy simultaneous-update restatement on a 96^3 sample, one thread;
+      * connected-component labelling of |phi| > 1 (scipy.ndimage.label's numbering) on
+        a 512^3 compensated-FP32 field of smooth bubbles (band-limited noise); CPU:
+        scipy.ndimage.label on a 256^3 field of the same kind;
+      * thermal V': dJ_B + dJ_F quadrature on the 256-point grid and a 4096 x 256 (phi, T)
+        table; CPU: scipy.integrate.quad of the same integrands on 16 grid points;
+      * snapshot: device->host copy and npz write of a 256^3 compensated-FP32 state.
+    One JSON line per component (none is the headline metric)."""
+    import torch
+    from oracle import integrators as OI
+    from oracle import oracle as O
+    from thermal_inflation_phase_transition_b200 import labels as LB
+    from thermal_inflation_phase_transition_b200 import real_field as RF
+    from thermal_inflation_phase_transition_b200 import thermal as TH
+    from thermal_inflation_phase_transition_b200.snapshots import SnapshotWriter
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    n = args.size
+    N = n ** 3
+    tab_np, tmin, dinv = O.build_table(lambda x: toy_vprime(x, 1.0), PHI_LO, PHI_HI, NPHI)
+    tab = torch.from_numpy(tab_np).to(dev)
+    ns = noise_scale(1.0)
+    lines = []
+
+    # ---- integrators
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    phi = RF.to_f32c(0.01 * torch.randn((n, n, n), dtype=torch.float64, device=dev, generator=g))
+    pi = torch.zeros_like(phi)
+    ptmp, qtmp = torch.empty_like(phi), torch.empty_like(pi)
+    step = [0]
+
+    def od():
+        RF.overdamped_euler_step_table(phi, DT, DX, ETA, 1.0, 1.0, tab, tmin, dinv, NPHI, ns,
+                                       step[0], phi_tmp=ptmp)
+        step[0] += 1
+
+    def ba():
+        RF.baoab_step_table(phi, pi, DT, DX, ETA, 1.0, 1.0, tab, tmin, dinv, NPHI, ns, step[0],
+                            phi_tmp=ptmp, pi_tmp=qtmp)
+        step[0] += 1
+
+    m = 96
+    rng = np.random.default_rng(3)
+    cphi, cpi = rng.normal(0.0, 0.01, (m, m, m)), np.zeros((m, m, m))
+    for name, fn, bps, cpu_fn in (
+            ("overdamped Euler-Maruyama step", od, 16,
+             lambda: OI.overdamped_step_table(cphi, DT, DX, ETA, 1.0, 1.0, tab_np, tmin, dinv,
+                                              NPHI, ns, 1, sweep="jacobi")),
+            ("BAOAB step", ba, 32,
+             lambda: OI.baoab_step_table(cphi, cpi, DT, DX, ETA, 1.0, 1.0, tab_np, tmin, dinv,
+                                         NPHI, ns, 1, sweep="jacobi"))):
+        ms = _dev_ms(fn, 20)
+        t0 = time.perf_counter()
+        cpu_fn()
+        cpu_s = time.perf_counter() - t0
+        ach = bps * N / (ms / 1e3) / 1e9
+        lines.append({
+            "metric": f"{name} site-updates/s", "value": N / (ms / 1e3), "unit": "site-updates/s",
+            "ms_per_step": ms, "dtype": "f32c", "data": "synthetic",
+            "config": {"workload": f"{name}, {n}^3 compensated FP32, 1-D V' table 4096, hash noise",
+                       "lattice": [n, n, n]},
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "algorithmic_bytes_per_site": bps},
+            "cpu_baseline": {"value": m ** 3 / cpu_s, "unit": "site-updates/s", "cores": 1,
+                             "kind": "port", "sample": f"one step of the numpy simultaneous-update "
+                                                       f"restatement on {m}^3"}})
+    assert int(RF.from_f32c(phi).isfinite().all()) == 1
+    del phi, pi, ptmp, qtmp
+    torch.cuda.empty_cache()
+
+    # ---- labelling
+    def bubbles(side, dev_):
+        gen = torch.Generator(device=dev_)
+        gen.manual_seed(11)
+        w = torch.randn((side, side, side), dtype=torch.float32, device=dev_, generator=gen)
+        f = torch.fft.rfftn(w)
+        k = [torch.fft.fftfreq(side, device=dev_)] * 2 + [torch.fft.rfftfreq(side, device=dev_)]
+        k2 = k[0][:, None, None] ** 2 + k[1][None, :, None] ** 2 + k[2][None, None, :] ** 2
+        f *= torch.exp(-k2 * (side / 6.0) ** 2)
+        x = torch.fft.irfftn(f, s=(side, side, side))
+        return (x / x.std()).double()  # unit variance: |x| > 1 covers about a third
+
+    fld = RF.to_f32c(bubbles(n, dev))
+    lab_n = [0]
+
+    def lab():
+        lab_n[0] = LB.label(fld, 1.0)[1]
+
+    ms = _dev_ms(lab, 5, warm=2)
+    from scipy import ndimage
+    c = 256
+    cf = np.abs(bubbles(c, dev).cpu().numpy()) > 1.0
+    t0 = time.perf_counter()
+    _, nc = ndimage.label(cf)
+    cpu_s = time.perf_counter() - t0
+    lines.append({
+        "metric": "labelling sites/s", "value": N / (ms / 1e3), "unit": "sites/s", "ms": ms,
+        "dtype": "f32c", "data": "synthetic",
+        "config": {"workload": f"|phi| > 1 components, {n}^3 field of smooth bubbles "
+                               "(band-limited noise), face connectivity, open lattice",
+                   "lattice": [n, n, n], "components": lab_n[0]},
+        "cpu_baseline": {"value": c ** 3 / cpu_s, "unit": "sites/s", "cores": 1,
+                         "kind": "reference", "sample": f"scipy.ndimage.label on a {c}^3 field "
+                                                       f"of the same kind ({nc} components)"}})
+    del fld
+    torch.cuda.empty_cache()
+
+    # ---- thermal V'
+    tp = [None]
+
+    def therm():
+        tp[0] = TH.ThermalPotential(counterterm=(1.0, 1000.0), device=dev)
+        tp[0].table_2d(0.0, 3000.0, 4096, 900.0, 1100.0, 256)
+
+    t0 = time.perf_counter()
+    therm()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    therm()
+    torch.cuda.synchronize()
+    gpu_s = time.perf_counter() - t1
+    from scipy import integrate
+    us = np.linspace(0.0, 100.0, 16)
+    t0 = time.perf_counter()
+    for u in us:
+        for sgn in (-1.0, 1.0):
+            integrate.quad(lambda y: y * y * u / (math.sqrt(y * y + u * u) *
+                                                  (math.exp(math.sqrt(y * y + u * u)) + sgn))
+                           if y * y + u * u > 0 else 0.0, 0.0, 100.0, limit=200)
+    cpu_s = time.perf_counter() - t0
+    lines.append({
+        "metric": "thermal V' build seconds", "value": gpu_s, "unit": "s",
+        "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "dJ_B + dJ_F quadrature on the 256-point u grid with the lattice "
+                               "counterterm, not-a-knot splines, 4096 x 256 (phi, T) V' table"},
+        "cpu_baseline": {"value": cpu_s * 512 / 32, "unit": "s", "cores": 1, "kind": "reference",
+                         "sample": "scipy.integrate.quad of the same two integrands on 16 of "
+                                   "the 256 grid points, scaled to 256 points x 2 integrands "
+                                   "(the table and counterterm not included)"}})
+
+    # ---- snapshot
+    sn = 256
+    st = RF.to_f32c(0.01 * torch.randn((sn, sn, sn), dtype=torch.float64, device=dev))
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        w = SnapshotWriter(d, background=False)
+        t0 = time.perf_counter()
+        path = w.save_real(0, 0.0, 1.0, st, st)
+        wall = time.perf_counter() - t0
+        size = os.path.getsize(path)
+    lines.append({
+        "metric": "snapshot write seconds", "value": wall, "unit": "s", "higher_is_better": False,
+        "dtype": "f32c", "data": "synthetic",
+        "config": {"workload": f"checkpoint (phi and pi, float64 hi+lo plus lo planes, "
+                               f"compressed npz) of a {sn}^3 compensated-FP32 state",
+                   "file_bytes": size}})
+    for ln in lines:
+        print(json.dumps(ln), flush=True)
 
 
 def run_surrogate_bench(args):

@@ -117,3 +117,56 @@ def test_baoab_without_noise_conserves_energy_at_zero_friction():
         e.append(o[0] + o[1] + 0.25 * o[4])
     e = np.array(e)
     assert np.abs(e / e[0] - 1).max() < 1e-2
+
+
+# ----------------------------------------------- marching kernel (F32C) ----
+from thermal_inflation_phase_transition_b200 import _lib as L  # noqa: E402
+
+
+def _run_real(kind, shape, policy, vpoly, steps=3):
+    tab, tmin, dinv, npts = _table()
+    tabd = torch.from_numpy(tab).to(DEV)
+    rng = np.random.default_rng(8)
+    phi = _dev(rng.normal(0.4, 0.6, shape), "f32c")
+    pi = _dev(rng.normal(0.0, 0.3, shape), "f32c")
+    L.set_kernel_policy(policy)
+    try:
+        for n in range(steps):
+            if kind == "overdamped":
+                RF.overdamped_euler_step_table(phi, DT, DX, ETA, MU, IA2, tabd, tmin, dinv, npts,
+                                               NS, n, hash_seed=4, vpoly=vpoly)
+            else:
+                RF.baoab_step_table(phi, pi, DT, DX, GAMMA, MU, IA2, tabd, tmin, dinv, npts, NS,
+                                    n, hash_seed=4, vpoly=vpoly)
+        torch.cuda.synchronize()
+    finally:
+        L.set_kernel_policy(0)
+    return phi.clone(), pi.clone()
+
+
+@pytest.mark.parametrize("kind", ["overdamped", "baoab"])
+@pytest.mark.parametrize("shape", [(8, 12, 64), (5, 6, 32), (33, 8, 128), (3, 4, 8)])
+@pytest.mark.parametrize("vpoly", [None, (-0.02, -0.15, 0.1)])
+def test_real_integrators_marching_equals_generic(kind, shape, vpoly):
+    """Compensated FP32 with nz % 4 == 0 runs on the marching ring: bitwise the
+    generic kernel's result (same per-site arithmetic)."""
+    a = _run_real(kind, shape, 1, vpoly)
+    b = _run_real(kind, shape, 0, vpoly)
+    assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
+    assert L.device_status() == 0
+
+
+def test_real_overdamped_marching_vs_oracle():
+    tab, tmin, dinv, npts = _table()
+    shape = (10, 8, 32)
+    rng = np.random.default_rng(3)
+    ref = rng.normal(0.4, 0.6, shape)
+    phi = _dev(ref, "f32c")
+    tabd = torch.from_numpy(tab).to(DEV)
+    for n in range(3):
+        ref = I.overdamped_step_table(ref, DT, DX, ETA, MU, IA2, tab, tmin, dinv, npts, NS, n, seed=4)
+        RF.overdamped_euler_step_table(phi, DT, DX, ETA, MU, IA2, tabd, tmin, dinv, npts, NS, n,
+                                       hash_seed=4)
+    torch.cuda.synchronize()
+    got = _host(phi, "f32c")
+    assert np.abs(got - ref).max() <= TOL["f32c"] * np.abs(ref).max()

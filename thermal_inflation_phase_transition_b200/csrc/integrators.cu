@@ -21,21 +21,11 @@
 // float-float state updates).
 #include <cstring>
 
-#include "rk2_complex.cuh"
+#include "integrators.cuh"
+#include "rk2_march.cuh"
 #include "tipt_internal.h"
 
 namespace tipt {
-
-enum { kOD = 0, kBA1 = 1, kBA2 = 2 };
-
-struct AltParams {
-    const void* f[4];  // real: phi, pi; complex: phi1, phi2, pi1, pi2
-    void* o[4];
-    int n0, n1, n2;
-    double h, dto, inv_dx2, inv_mu2, inv_a2, c1, c2, ns;
-    uint64_t step, seed;
-    ComplexStageParams v;  // V' source, Z_N and eps terms (the force fields only)
-};
 
 // FP64 Laplacian in the reference order (ip, im, jp, jm, kp, km, then - 6 c).
 __device__ __forceinline__ double lap_d(const double q[7], double inv_dx2) {
@@ -57,24 +47,8 @@ __device__ __forceinline__ double vprime_alt_d(const ComplexStageParams& v, cons
     if (v.vkind == TIPT_VP_POLY) return poly_vprime<double>(v.c1, v.c2, v.c3, x);
     return lerp_table<double>(tab, v.tmin, v.dinv, v.npts - 2, x);
 }
-__device__ __forceinline__ float vprime_alt_f(const ComplexStageParams& v, const float* s_tab,
-                                              float x) {
-    if (v.vkind == TIPT_VP_POLY)
-        return poly_vprime<float>((float)v.c1, (float)v.c2, (float)v.c3, x);
-    if (v.table_in_smem) return lerp_table<float>(s_tab, (float)v.tmin, (float)v.dinv, v.npts - 2, x);
-    return (float)lerp_table<double>(v.table, v.tmin, v.dinv, v.npts - 2, (double)x);
-}
-
 __device__ __forceinline__ double force_d(const AltParams& p, double lap, double dv) {
     return __dsub_rn(__dmul_rn(p.inv_a2, lap), __dmul_rn(dv, p.inv_mu2));
-}
-
-// a + h*b as float-float (h split into hh + hl), the product error kept.
-__device__ __forceinline__ void ff_axpy(float ah, float al, float hh, float hl, float bh, float bl,
-                                        float& oh, float& ol) {
-    const float d_hi = __fmul_rn(hh, bh);
-    const float d_lo = __fadd_rn(__fmaf_rn(hh, bh, -d_hi), __fmaf_rn(hh, bl, __fmul_rn(hl, bh)));
-    ff_add(ah, al, d_hi, d_lo, oh, ol);
 }
 
 template <typename TT>
@@ -146,44 +120,24 @@ __global__ void __launch_bounds__(256) alt_real_kernel(AltParams p) {
             }
             float dh, dl;
             stencil_sums(hh, hl, dh, dl);
-            const float lap = __fmul_rn(__fadd_rn(dh, dl), (float)p.inv_dx2);
-            const float F = __fsub_rn(__fmul_rn((float)p.inv_a2, lap),
-                                      __fmul_rn(vprime_alt_f(p.v, s_tab, __fadd_rn(hh[0], hl[0])),
-                                                (float)p.inv_mu2));
+            const float vp = vprime_alt_f(p.v, s_tab, __fadd_rn(hh[0], hl[0]));
             const float z = noisy ? gauss_cos_f(key) : 0.0f;
             float* out0 = static_cast<float*>(p.o[0]);
             float* out1 = static_cast<float*>(p.o[1]);
-            if constexpr (MODE == kOD) {
-                float a, b;
-                ff_add(hh[0], hl[0], __fmaf_rn((float)p.dto, F, __fmul_rn((float)p.ns, z)), 0.0f, a, b);
-                out0[s] = a;
-                out0[N + s] = b;
-            } else {
+            float vh = 0.0f, vl = 0.0f, ah, al, bh, bl;
+            if constexpr (MODE != kOD) {
                 const float* pif = static_cast<const float*>(p.f[1]);
-                float vh = pif[s], vl = pif[N + s];
-                const float h = (float)p.h, hlo = (float)(p.h - (double)h);
-                if constexpr (MODE == kBA1) {
-                    ff_add(vh, vl, __fmul_rn(h, F), 0.0f, vh, vl);   // pi'
-                    float ah, al;
-                    ff_axpy(hh[0], hl[0], h, hlo, vh, vl, ah, al);   // phi'
-                    const float c1h = (float)p.c1, c1l = (float)(p.c1 - (double)c1h);
-                    const float ph_ = __fmul_rn(c1h, vh);
-                    const float pl_ = __fadd_rn(__fmaf_rn(c1h, vh, -ph_),
-                                                __fmaf_rn(c1h, vl, __fmul_rn(c1l, vh)));
-                    float oh, ol;
-                    ff_add(ph_, pl_, __fmul_rn((float)p.c2, z), 0.0f, oh, ol);  // pi''
-                    float fh, fl;
-                    ff_axpy(ah, al, h, hlo, oh, ol, fh, fl);           // phi''
-                    out0[s] = fh;
-                    out0[N + s] = fl;
-                    out1[s] = oh;
-                    out1[N + s] = ol;
-                } else {
-                    float oh, ol;
-                    ff_add(vh, vl, __fmul_rn(h, F), 0.0f, oh, ol);
-                    out1[s] = oh;
-                    out1[N + s] = ol;
-                }
+                vh = pif[s];
+                vl = pif[N + s];
+            }
+            alt_real_site_f32c<MODE>(p, hh[0], hl[0], dh, dl, vp, z, vh, vl, ah, al, bh, bl);
+            if constexpr (MODE != kBA2) {
+                out0[s] = ah;
+                out0[N + s] = al;
+            }
+            if constexpr (MODE != kOD) {
+                out1[s] = bh;
+                out1[N + s] = bl;
             }
         }
     }
@@ -349,6 +303,10 @@ static int launch_alt_k(const AltParams& p, cudaStream_t st) {
 
 template <int MODE, bool CPLX>
 static int launch_alt(int storage, const AltParams& p, cudaStream_t st) {
+    // the real field in compensated FP32 on the marching ring where the shape allows
+    // (bitwise the generic kernel's results; kernel_policy 1 forces the generic one)
+    if (!CPLX && storage == TIPT_F32C && kernel_policy() != 1 && alt_march_supported(p))
+        return launch_alt_march(MODE, p, st);
     switch (storage) {
         case TIPT_F64: return launch_alt_k<TIPT_F64, MODE, CPLX>(p, st);
         case TIPT_F32: return launch_alt_k<TIPT_F32, MODE, CPLX>(p, st);

@@ -29,6 +29,7 @@
 // producer drains the copies it issued (bounded) before it exits.
 #include <cuda.h>
 
+#include "integrators.cuh"
 #include "rk2_march.cuh"
 #include "tipt_internal.h"
 
@@ -548,6 +549,210 @@ __global__ void __maxnreg__(kMarchRegs)
     }
 }
 
+// ------------------------------- alternative integrators, F32C marching ----
+// Overdamped Euler-Maruyama and the two BAOAB passes of the real field
+// (R:2115, R:1974) on the marching ring: the stencil reads phi alone, so a
+// ring stage holds the hi and lo planes of phi (half an RK2 stage); pi (the
+// BAOAB passes) is read and written at the thread's own four sites.  The
+// per-site arithmetic is alt_real_site_f32c, which the generic kernel runs
+// too, so both give the same bits.
+template <int MODE, bool WIDE>
+__global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    float* s_tab = reinterpret_cast<float*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + g.tab_bytes);
+    uint64_t* empty = full + 8;
+    unsigned char* ring = smem + g.tab_bytes + 128;
+
+    const int n0 = p.n0, n1 = p.n1, n2 = p.n2;
+    const int pitch = g.pitch;
+    const int TJ = g.TJ;
+    const uint32_t NS = (uint32_t)g.S;
+    const int rows = TJ + 2;
+    const int tpr = n2 >> 2;
+    const int nc = TJ * tpr;
+    const int t = threadIdx.x;
+
+    if (t == 0) {
+        for (uint32_t s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], nc / 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (p.v.table_in_smem)
+        for (int q = t; q < p.v.npts; q += blockDim.x) s_tab[q] = (float)__ldg(p.v.table + q);
+    __syncthreads();
+
+    const size_t plane_blk = (size_t)(g.stage_bytes >> 1);  // one [rows][pitch] block
+    auto blk = [&](uint32_t stage, int c) -> float* {       // c: 0 hi, 1 lo
+        return reinterpret_cast<float*>(ring + (size_t)stage * g.stage_bytes + (size_t)c * plane_blk);
+    };
+
+    // ------------------------------------------------------------ producer
+    if (t >= nc) {
+        if (t != nc) return;
+        const uint32_t plane_tx = (uint32_t)(2 * rows * n2 * 4);
+        const float* const src = static_cast<const float*>(p.f[0]);
+        RingPos w{0, 0};
+        uint32_t issued = 0;
+        bool ok = true;
+        for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
+            const int ic = item / g.nJB;
+            const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+            const int npl = min(g.CI, n0 - i0) + 2;
+            for (int q = 0; q < npl; ++q) {
+                if (issued >= NS && !mbar_wait(&empty[w.stage], w.phase ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(&full[w.stage], plane_tx);
+                int iw = i0 - 1 + q;
+                iw = iw < 0 ? iw + n0 : (iw >= n0 ? iw - n0 : iw);
+                copy_tile_rows(blk(w.stage, 0), src, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                copy_tile_rows(blk(w.stage, 1), src, n0 + iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                ++issued;
+                w.next(NS);
+            }
+        }
+        if (!ok) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+        RingPos d = w;
+        for (uint32_t k = 0; k < NS && k < issued; ++k) {
+            d.stage = d.stage == 0 ? NS - 1 : d.stage - 1;
+            if (d.stage == NS - 1) d.phase ^= 1u;
+            (void)mbar_wait(&full[d.stage], d.phase);
+        }
+        return;
+    }
+
+    // ----------------------------------------------------------- consumers
+    const int lane = t & 31;
+    const int r = 1 + t / tpr;
+    const int k0 = 4 * (t - (r - 1) * tpr);
+    const int kml = k0 == 0 ? n2 - 1 : k0 - 1;
+    const int kpr = k0 + 4 == n2 ? 0 : k0 + 4;
+    const int64_t N = (int64_t)n0 * n1 * n2;
+    const int orow = r * pitch, urow = (r - 1) * pitch, drow = (r + 1) * pitch;
+    const bool noisy = (MODE == kOD && p.ns != 0.0) || (MODE == kBA1 && p.c2 != 0.0);
+    const float tminf = (float)p.v.tmin, dinvf = (float)p.v.dinv, last = (float)(p.v.npts - 2);
+    const float* const pif = static_cast<const float*>(p.f[1]);
+    float* const o0 = static_cast<float*>(p.o[0]);
+    float* const o1 = static_cast<float*>(p.o[1]);
+
+    RingPos pm{0, 0};
+    for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
+        const int ic = item / g.nJB;
+        const int j0 = (item - ic * g.nJB) * TJ, i0 = ic * g.CI;
+        const int ni = min(g.CI, n0 - i0);
+        const int jw = j0 + r - 1;
+        RingPos pc = pm, pp;
+        pc.next(NS);
+        pp = pc;
+        pp.next(NS);
+        if (!mbar_wait(&full[pm.stage], pm.phase) || !mbar_wait(&full[pc.stage], pc.phase)) {
+            if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+            return;
+        }
+        for (int q = 0; q < ni; ++q) {
+            if (!mbar_wait(&full[pp.stage], pp.phase)) {
+                if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+                return;
+            }
+            const int64_t rowoff = ((int64_t)(i0 + q) * n1 + jw) * n2 + k0;
+            float2 dsum[2][2], cen[2][2];  // [pair][hi, lo]
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const float* sc = blk(pc.stage, c);
+                const float4 ce = *reinterpret_cast<const float4*>(sc + orow + k0);
+                const float4 jm = *reinterpret_cast<const float4*>(sc + urow + k0);
+                const float4 jp = *reinterpret_cast<const float4*>(sc + drow + k0);
+                const float4 im = *reinterpret_cast<const float4*>(blk(pm.stage, c) + orow + k0);
+                const float4 ip = *reinterpret_cast<const float4*>(blk(pp.stage, c) + orow + k0);
+                float kl = __shfl_up_sync(0xffffffffu, ce.w, 1);
+                float kr = __shfl_down_sync(0xffffffffu, ce.x, 1);
+                if (lane == 0 || k0 == 0) kl = sc[orow + kml];
+                if (lane == 31 || k0 + 4 == n2) kr = sc[orow + kpr];
+                const float2 cc[2] = {make_float2(ce.x, ce.y), make_float2(ce.z, ce.w)};
+                const float2 nb[2][6] = {
+                    {make_float2(ip.x, ip.y), make_float2(im.x, im.y), make_float2(jp.x, jp.y),
+                     make_float2(jm.x, jm.y), make_float2(ce.y, ce.z), make_float2(kl, ce.x)},
+                    {make_float2(ip.z, ip.w), make_float2(im.z, im.w), make_float2(jp.z, jp.w),
+                     make_float2(jm.z, jm.w), make_float2(ce.w, kr), make_float2(ce.y, ce.z)}};
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    float2 acc;
+                    if (c == 0) {  // dh = sum (hi_n - hi_c)
+                        acc = v_sub(nb[h][0], cc[h]);
+#pragma unroll
+                        for (int n = 1; n < 6; ++n) acc = v_add(acc, v_sub(nb[h][n], cc[h]));
+                    } else {       // dl = fma(-6, lo_c, sum lo_n)
+                        acc = nb[h][0];
+#pragma unroll
+                        for (int n = 1; n < 6; ++n) acc = v_add(acc, nb[h][n]);
+                        acc = v_fma(vs<float2>(-6.0f), cc[h], acc);
+                    }
+                    dsum[h][c] = acc;
+                    cen[h][c] = cc[h];
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[pm.stage]);  // plane i-1 is no longer read
+            float4 vh4 = make_float4(0.f, 0.f, 0.f, 0.f), vl4 = vh4;
+            if constexpr (MODE != kOD) {
+                vh4 = *reinterpret_cast<const float4*>(pif + rowoff);
+                vl4 = *reinterpret_cast<const float4*>(pif + N + rowoff);
+            }
+            const float vhv[4] = {vh4.x, vh4.y, vh4.z, vh4.w};
+            const float vlv[4] = {vl4.x, vl4.y, vl4.z, vl4.w};
+            float ah[4], al[4], bh[4], bl[4];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint64_t site;
+                if constexpr (WIDE) site = (uint64_t)(rowoff + 2 * h);
+                else site = (uint32_t)rowoff + (uint32_t)(2 * h);
+                float2 z = make_float2(0.0f, 0.0f);
+                if (noisy)
+                    z = gauss_cos_f2(noise_key(site, p.step, kPass2Mul, p.seed),
+                                     noise_key(site + 1, p.step, kPass2Mul, p.seed));
+                const float2 x = v_add(cen[h][0], cen[h][1]);
+                float2 vp;
+                if (p.v.vkind == TIPT_VP_POLY) {
+                    const float2 d = v_fma(v_mul(v_mul(vs<float2>((float)p.v.c3), x), x), x,
+                                           v_mul(vs<float2>((float)p.v.c1), x));
+                    vp = p.v.c2 != 0.0 ? v_fma(v_mul(vs<float2>((float)p.v.c2), x), x, d) : d;
+                } else {
+                    vp = lerp_table_f32<float2>(s_tab, v_mul(v_sub(x, vs<float2>(tminf)),
+                                                             vs<float2>(dinvf)), last);
+                }
+                alt_real_site_f32c<MODE>(p, cen[h][0].x, cen[h][1].x, dsum[h][0].x, dsum[h][1].x,
+                                         vp.x, z.x, vhv[2 * h], vlv[2 * h], ah[2 * h], al[2 * h],
+                                         bh[2 * h], bl[2 * h]);
+                alt_real_site_f32c<MODE>(p, cen[h][0].y, cen[h][1].y, dsum[h][0].y, dsum[h][1].y,
+                                         vp.y, z.y, vhv[2 * h + 1], vlv[2 * h + 1], ah[2 * h + 1],
+                                         al[2 * h + 1], bh[2 * h + 1], bl[2 * h + 1]);
+            }
+            if constexpr (MODE != kBA2) {
+                *reinterpret_cast<float4*>(o0 + rowoff) = make_float4(ah[0], ah[1], ah[2], ah[3]);
+                *reinterpret_cast<float4*>(o0 + N + rowoff) = make_float4(al[0], al[1], al[2], al[3]);
+            }
+            if constexpr (MODE != kOD) {
+                *reinterpret_cast<float4*>(o1 + rowoff) = make_float4(bh[0], bh[1], bh[2], bh[3]);
+                *reinterpret_cast<float4*>(o1 + N + rowoff) = make_float4(bl[0], bl[1], bl[2], bl[3]);
+            }
+            pm = pc;
+            pc = pp;
+            pp.next(NS);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(&empty[pm.stage]);
+            mbar_arrive(&empty[pc.stage]);
+        }
+        pm = pp;
+    }
+}
+
 // ----------------------------------------------------- complex, F32C ----
 // Complex field in compensated FP32: four planar fields (phi1, phi2, pi1, pi2;
 // hi plane then lo plane each), so a ring stage holds eight (TJ+2)-row blocks.
@@ -862,17 +1067,17 @@ static int ctas_per_sm(const MarchGeom& g, int tpr) {
 static int layout_es(int storage) { return storage == TIPT_F64 ? 8 : 4; }
 static int layout_planes(int storage) { return storage == TIPT_F64 ? 1 : 2; }
 
-static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, MarchGeom& g,
-                     int64_t& smem) {
-    const int n1 = p.n1, n2 = p.n2;
-    const int es = layout_es(storage), np = layout_planes(storage);
+// Tile geometry of the real-field marching kernels: n1 x n2 rows, nplanes
+// planes to compute, `comps` component planes of `es`-byte elements per ring
+// stage (RK2: phi and pi, hi and lo for F32C; the alternative integrators: phi).
+static bool geometry_dims(int n1, int n2, int nplanes, int es, int comps, int64_t smem_table,
+                          MarchGeom& g, int64_t& smem) {
     if (n2 % 4 != 0 || n2 < 8 || n2 > 2048) return false;
     g.BK = n2;  // whole rows: every copy is a 1-D bulk copy of consecutive rows
     const int per128 = 128 / es;
     g.pitch = (n2 + per128 - 1) / per128 * per128;
     const int tpr = n2 / 4;
     g.tab_bytes = round128((int)smem_table);
-    const int nplanes = p.i_end - p.i_begin;
     g.CI = g_force_ci > 0 ? g_force_ci : 64;
     if (g.CI > nplanes) g.CI = nplanes;
     // Candidates: TJ with TJ*tpr consumers a multiple of 32 in [32, 512], ring
@@ -888,7 +1093,7 @@ static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, 
             MarchGeom c = g;
             c.TJ = tj;
             c.S = st;
-            c.stage_bytes = 2 * np * round128((tj + 2) * c.pitch * es);
+            c.stage_bytes = comps * round128((tj + 2) * c.pitch * es);
             if (smem_need(c) > kSmemPerCta) continue;
             const int cps = ctas_per_sm(c, tpr);
             if (cps < 1) continue;
@@ -904,12 +1109,18 @@ static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, 
     // bulk-copy destinations (ring + stage*stage_bytes + block*stage_bytes/blocks +
     // rr*pitch*es) are 128-byte aligned; sources and sizes are multiples of the
     // 16-byte row length (n2 % 4 == 0)
-    if ((g.pitch * es) % 128 || g.stage_bytes % (256 * np) || g.tab_bytes % 128) return false;
+    if ((g.pitch * es) % 128 || g.stage_bytes % (128 * comps) || g.tab_bytes % 128) return false;
     g.nJB = n1 / g.TJ;
     g.nIC = (nplanes + g.CI - 1) / g.CI;
     g.items = g.nJB * g.nIC;
     smem = smem_need(g);
     return true;
+}
+
+static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, MarchGeom& g,
+                     int64_t& smem) {
+    return geometry_dims(p.n1, p.n2, p.i_end - p.i_begin, layout_es(storage),
+                         2 * layout_planes(storage), smem_table, g, smem);
 }
 
 bool march_supported(int storage, const RealStageParams& p) {
@@ -961,6 +1172,56 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
         return wide ? launch_march_k(rk2_stage_march<TIPT_F64, true>, p, g, smem, st)
                     : launch_march_k(rk2_stage_march<TIPT_F64, false>, p, g, smem, st);
     return fail(TIPT_ERR_STORAGE, "marching kernel takes F32C or F64");
+}
+
+// The real-field alternative integrators on the marching ring: compensated
+// FP32, polynomial V' or a table staged in shared memory, n2 % 4 == 0.
+static bool alt_geometry(const AltParams& p, MarchGeom& g, int64_t& smem) {
+    if (p.v.vkind != TIPT_VP_POLY && !p.v.table_in_smem) return false;
+    const int64_t tb = p.v.vkind == TIPT_VP_POLY ? 0 : (int64_t)p.v.npts * 4;
+    return geometry_dims(p.n1, p.n2, p.n0, 4, 2, tb, g, smem);
+}
+
+bool alt_march_supported(const AltParams& p) {
+    uintptr_t a = reinterpret_cast<uintptr_t>(p.f[0]) | reinterpret_cast<uintptr_t>(p.f[1]) |
+                  reinterpret_cast<uintptr_t>(p.o[0]) | reinterpret_cast<uintptr_t>(p.o[1]);
+    if (a % 16) return false;
+    MarchGeom g;
+    int64_t smem;
+    return alt_geometry(p, g, smem);
+}
+
+template <int MODE>
+static int launch_alt_march_k(const AltParams& p, cudaStream_t st) {
+    MarchGeom g;
+    int64_t smem;
+    if (!alt_geometry(p, g, smem)) return fail(TIPT_ERR_UNSUPPORTED, "integrator march geometry");
+    const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
+    auto kern = wide ? alt_march_f32c<MODE, true> : alt_march_f32c<MODE, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return fail_cuda(e, "integrator march attributes");
+    const int threads = g.TJ * (p.n2 / 4) + 32;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, (size_t)smem);
+    if (e != cudaSuccess || per_sm < 1)
+        return fail(TIPT_ERR_UNSUPPORTED, "integrator march kernel does not fit an SM");
+    int grid = num_sms() * per_sm;
+    if (grid > g.items) grid = g.items;
+    kern<<<grid, threads, (size_t)smem, st>>>(p, g);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "integrator march launch");
+}
+
+int launch_alt_march(int mode, const AltParams& p, cudaStream_t st) {
+    switch (mode) {
+        case kOD: return launch_alt_march_k<kOD>(p, st);
+        case kBA1: return launch_alt_march_k<kBA1>(p, st);
+        default: return launch_alt_march_k<kBA2>(p, st);
+    }
 }
 
 // Complex F32C geometry: two sites per consumer thread (tpr = n2/2 per row),

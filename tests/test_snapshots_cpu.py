@@ -71,3 +71,25 @@ def test_complex_schema(tmp_path):
     p = SN.write_metadata(str(tmp_path), Nx=3, Ny=4, Nz=5, dt=0.05, integrator="rk2_nonfused")
     with np.load(p) as z:
         assert int(z["Nx"]) == 3 and str(z["integrator"]) == "rk2_nonfused"
+
+
+def test_compressed_and_stored_archives_hold_the_same_arrays(tmp_path):
+    """compress=True deflates the members as the reference's np.savez_compressed;
+    the default stores them; np.load returns the same keys and arrays."""
+    import zipfile
+    rng = np.random.default_rng(1)
+    phi = to_f32c(torch.from_numpy(rng.normal(size=(3, 4, 8))))
+    pi = to_f32c(torch.from_numpy(rng.normal(size=(3, 4, 8))))
+    out = {}
+    for comp in (False, True):
+        d = tmp_path / str(comp)
+        w = SN.SnapshotWriter(str(d), background=False, compress=comp)
+        path = w.save_real(5, 0.25, 1.0, phi, pi)
+        with zipfile.ZipFile(path) as zf:
+            kinds = {i.compress_type for i in zf.infolist()}
+        assert kinds == ({zipfile.ZIP_DEFLATED} if comp else {zipfile.ZIP_STORED})
+        with np.load(path) as z:
+            out[comp] = {k: z[k] for k in z.files}
+    assert out[False].keys() == out[True].keys()
+    for k in out[False]:
+        np.testing.assert_array_equal(out[False][k], out[True][k])

@@ -170,3 +170,41 @@ def test_real_overdamped_marching_vs_oracle():
     torch.cuda.synchronize()
     got = _host(phi, "f32c")
     assert np.abs(got - ref).max() <= TOL["f32c"] * np.abs(ref).max()
+
+
+def _run_complex(kind, shape, policy, vpoly, zn, eps4, steps=3):
+    from oracle import oracle as O2
+    tab, tmin, dinv = O2.build_table(lambda x: O2.toy_vprime_rho(x, 0.98), 0.0, 3.0, 2048)
+    tabd = torch.from_numpy(tab).to(DEV)
+    rng = np.random.default_rng(12)
+    f = [_dev(rng.normal(0.3, 0.5, shape), "f32c") for _ in range(2)]
+    v = [_dev(rng.normal(0.0, 0.3, shape), "f32c") for _ in range(2)]
+    L.set_kernel_policy(policy)
+    try:
+        for n in range(steps):
+            if kind == "overdamped":
+                CF.overdamped_euler_step_table(f[0], f[1], DT, DX, ETA, MU, IA2, tabd, tmin, dinv,
+                                               2048, NS, n, zn=zn, eps4=eps4, hash_seed=5,
+                                               vpoly=vpoly)
+            else:
+                CF.baoab_step_table(f[0], f[1], v[0], v[1], DT, DX, GAMMA, MU, IA2, tabd, tmin,
+                                    dinv, 2048, NS, n, zn=zn, eps4=eps4, hash_seed=5, vpoly=vpoly)
+        torch.cuda.synchronize()
+    finally:
+        L.set_kernel_policy(0)
+    return [a.clone() for a in f + v]
+
+
+@pytest.mark.parametrize("kind", ["overdamped", "baoab"])
+@pytest.mark.parametrize("shape", [(8, 12, 64), (5, 6, 32), (3, 4, 8)])
+@pytest.mark.parametrize("vpoly,zn,eps4", [(None, (0.0, 0.0, 0.0), 1e-3),
+                                           ((-0.02, -0.15, 0.1), (0.0, 0.0, 0.0), 0.0),
+                                           (None, (4.0, 0.01, 1.0), 0.0)])
+def test_complex_integrators_marching_equals_generic(kind, shape, vpoly, zn, eps4):
+    """The complex field's integrators on the marching ring (Z_N off) equal the generic
+    kernel bit for bit; with Z_N on both calls take the generic kernel."""
+    a = _run_complex(kind, shape, 1, vpoly, zn, eps4)
+    b = _run_complex(kind, shape, 0, vpoly, zn, eps4)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    assert L.device_status() == 0

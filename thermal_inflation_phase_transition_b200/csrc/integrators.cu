@@ -303,10 +303,10 @@ static int launch_alt_k(const AltParams& p, cudaStream_t st) {
 
 template <int MODE, bool CPLX>
 static int launch_alt(int storage, const AltParams& p, cudaStream_t st) {
-    // the real field in compensated FP32 on the marching ring where the shape allows
-    // (bitwise the generic kernel's results; kernel_policy 1 forces the generic one)
-    if (!CPLX && storage == TIPT_F32C && kernel_policy() != 1 && alt_march_supported(p))
-        return launch_alt_march(MODE, p, st);
+    // compensated FP32 on the marching ring where the shape allows (bitwise the
+    // generic kernel's results; kernel_policy 1 forces the generic one)
+    if (storage == TIPT_F32C && kernel_policy() != 1 && alt_march_supported(p, CPLX))
+        return launch_alt_march(MODE, CPLX, p, st);
     switch (storage) {
         case TIPT_F64: return launch_alt_k<TIPT_F64, MODE, CPLX>(p, st);
         case TIPT_F32: return launch_alt_k<TIPT_F32, MODE, CPLX>(p, st);

@@ -550,14 +550,16 @@ __global__ void __maxnreg__(kMarchRegs)
 }
 
 // ------------------------------- alternative integrators, F32C marching ----
-// Overdamped Euler-Maruyama and the two BAOAB passes of the real field
-// (R:2115, R:1974) on the marching ring: the stencil reads phi alone, so a
-// ring stage holds the hi and lo planes of phi (half an RK2 stage); pi (the
-// BAOAB passes) is read and written at the thread's own four sites.  The
-// per-site arithmetic is alt_real_site_f32c, which the generic kernel runs
-// too, so both give the same bits.
-template <int MODE, bool WIDE>
+// Overdamped Euler-Maruyama and the two BAOAB passes (R:2115, R:1974; complex
+// C:2422, C:2223) on the marching ring: the stencil reads the field alone, so
+// a ring stage holds the hi and lo planes of phi (real) or of phi1 and phi2
+// (complex); pi (the BAOAB passes) is read and written at the thread's own
+// four sites.  The per-component arithmetic is alt_real_site_f32c and the
+// complex force complex_force_v, which the generic kernels run too, so both
+// give the same bits.
+template <int MODE, bool CPLX, bool WIDE>
 __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g) {
+    constexpr int NF = CPLX ? 2 : 1;  // stencil fields
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     float* s_tab = reinterpret_cast<float*>(smem);
@@ -585,16 +587,16 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
         for (int q = t; q < p.v.npts; q += blockDim.x) s_tab[q] = (float)__ldg(p.v.table + q);
     __syncthreads();
 
-    const size_t plane_blk = (size_t)(g.stage_bytes >> 1);  // one [rows][pitch] block
-    auto blk = [&](uint32_t stage, int c) -> float* {       // c: 0 hi, 1 lo
-        return reinterpret_cast<float*>(ring + (size_t)stage * g.stage_bytes + (size_t)c * plane_blk);
+    const size_t plane_blk = (size_t)(g.stage_bytes / (2 * NF));  // one [rows][pitch] block
+    auto blk = [&](uint32_t stage, int f, int c) -> float* {     // field f, c: 0 hi, 1 lo
+        return reinterpret_cast<float*>(ring + (size_t)stage * g.stage_bytes +
+                                        (size_t)(2 * f + c) * plane_blk);
     };
 
     // ------------------------------------------------------------ producer
     if (t >= nc) {
         if (t != nc) return;
-        const uint32_t plane_tx = (uint32_t)(2 * rows * n2 * 4);
-        const float* const src = static_cast<const float*>(p.f[0]);
+        const uint32_t plane_tx = (uint32_t)(2 * NF * rows * n2 * 4);
         RingPos w{0, 0};
         uint32_t issued = 0;
         bool ok = true;
@@ -610,8 +612,13 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
                 mbar_expect_tx(&full[w.stage], plane_tx);
                 int iw = i0 - 1 + q;
                 iw = iw < 0 ? iw + n0 : (iw >= n0 ? iw - n0 : iw);
-                copy_tile_rows(blk(w.stage, 0), src, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
-                copy_tile_rows(blk(w.stage, 1), src, n0 + iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    const float* src = static_cast<const float*>(p.f[f]);
+                    copy_tile_rows(blk(w.stage, f, 0), src, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                    copy_tile_rows(blk(w.stage, f, 1), src, n0 + iw, j0, rows, n1, n2, pitch,
+                                   &full[w.stage]);
+                }
                 ++issued;
                 w.next(NS);
             }
@@ -636,9 +643,6 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
     const int orow = r * pitch, urow = (r - 1) * pitch, drow = (r + 1) * pitch;
     const bool noisy = (MODE == kOD && p.ns != 0.0) || (MODE == kBA1 && p.c2 != 0.0);
     const float tminf = (float)p.v.tmin, dinvf = (float)p.v.dinv, last = (float)(p.v.npts - 2);
-    const float* const pif = static_cast<const float*>(p.f[1]);
-    float* const o0 = static_cast<float*>(p.o[0]);
-    float* const o1 = static_cast<float*>(p.o[1]);
 
     RingPos pm{0, 0};
     for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
@@ -660,85 +664,104 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
                 return;
             }
             const int64_t rowoff = ((int64_t)(i0 + q) * n1 + jw) * n2 + k0;
-            float2 dsum[2][2], cen[2][2];  // [pair][hi, lo]
+            float2 dsum[2][NF][2], cen[2][NF][2];  // [pair][field][hi, lo]
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const float* sc = blk(pc.stage, c);
-                const float4 ce = *reinterpret_cast<const float4*>(sc + orow + k0);
-                const float4 jm = *reinterpret_cast<const float4*>(sc + urow + k0);
-                const float4 jp = *reinterpret_cast<const float4*>(sc + drow + k0);
-                const float4 im = *reinterpret_cast<const float4*>(blk(pm.stage, c) + orow + k0);
-                const float4 ip = *reinterpret_cast<const float4*>(blk(pp.stage, c) + orow + k0);
-                float kl = __shfl_up_sync(0xffffffffu, ce.w, 1);
-                float kr = __shfl_down_sync(0xffffffffu, ce.x, 1);
-                if (lane == 0 || k0 == 0) kl = sc[orow + kml];
-                if (lane == 31 || k0 + 4 == n2) kr = sc[orow + kpr];
-                const float2 cc[2] = {make_float2(ce.x, ce.y), make_float2(ce.z, ce.w)};
-                const float2 nb[2][6] = {
-                    {make_float2(ip.x, ip.y), make_float2(im.x, im.y), make_float2(jp.x, jp.y),
-                     make_float2(jm.x, jm.y), make_float2(ce.y, ce.z), make_float2(kl, ce.x)},
-                    {make_float2(ip.z, ip.w), make_float2(im.z, im.w), make_float2(jp.z, jp.w),
-                     make_float2(jm.z, jm.w), make_float2(ce.w, kr), make_float2(ce.y, ce.z)}};
+            for (int f = 0; f < NF; ++f) {
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    float2 acc;
-                    if (c == 0) {  // dh = sum (hi_n - hi_c)
-                        acc = v_sub(nb[h][0], cc[h]);
+                for (int c = 0; c < 2; ++c) {
+                    const float* sc = blk(pc.stage, f, c);
+                    const float4 ce = *reinterpret_cast<const float4*>(sc + orow + k0);
+                    const float4 jm = *reinterpret_cast<const float4*>(sc + urow + k0);
+                    const float4 jp = *reinterpret_cast<const float4*>(sc + drow + k0);
+                    const float4 im = *reinterpret_cast<const float4*>(blk(pm.stage, f, c) + orow + k0);
+                    const float4 ip = *reinterpret_cast<const float4*>(blk(pp.stage, f, c) + orow + k0);
+                    float kl = __shfl_up_sync(0xffffffffu, ce.w, 1);
+                    float kr = __shfl_down_sync(0xffffffffu, ce.x, 1);
+                    if (lane == 0 || k0 == 0) kl = sc[orow + kml];
+                    if (lane == 31 || k0 + 4 == n2) kr = sc[orow + kpr];
+                    const float2 cc[2] = {make_float2(ce.x, ce.y), make_float2(ce.z, ce.w)};
+                    const float2 nb[2][6] = {
+                        {make_float2(ip.x, ip.y), make_float2(im.x, im.y), make_float2(jp.x, jp.y),
+                         make_float2(jm.x, jm.y), make_float2(ce.y, ce.z), make_float2(kl, ce.x)},
+                        {make_float2(ip.z, ip.w), make_float2(im.z, im.w), make_float2(jp.z, jp.w),
+                         make_float2(jm.z, jm.w), make_float2(ce.w, kr), make_float2(ce.y, ce.z)}};
 #pragma unroll
-                        for (int n = 1; n < 6; ++n) acc = v_add(acc, v_sub(nb[h][n], cc[h]));
-                    } else {       // dl = fma(-6, lo_c, sum lo_n)
-                        acc = nb[h][0];
+                    for (int h = 0; h < 2; ++h) {
+                        float2 acc;
+                        if (c == 0) {  // dh = sum (hi_n - hi_c)
+                            acc = v_sub(nb[h][0], cc[h]);
 #pragma unroll
-                        for (int n = 1; n < 6; ++n) acc = v_add(acc, nb[h][n]);
-                        acc = v_fma(vs<float2>(-6.0f), cc[h], acc);
+                            for (int n = 1; n < 6; ++n) acc = v_add(acc, v_sub(nb[h][n], cc[h]));
+                        } else {       // dl = fma(-6, lo_c, sum lo_n)
+                            acc = nb[h][0];
+#pragma unroll
+                            for (int n = 1; n < 6; ++n) acc = v_add(acc, nb[h][n]);
+                            acc = v_fma(vs<float2>(-6.0f), cc[h], acc);
+                        }
+                        dsum[h][f][c] = acc;
+                        cen[h][f][c] = cc[h];
                     }
-                    dsum[h][c] = acc;
-                    cen[h][c] = cc[h];
                 }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[pm.stage]);  // plane i-1 is no longer read
-            float4 vh4 = make_float4(0.f, 0.f, 0.f, 0.f), vl4 = vh4;
-            if constexpr (MODE != kOD) {
-                vh4 = *reinterpret_cast<const float4*>(pif + rowoff);
-                vl4 = *reinterpret_cast<const float4*>(pif + N + rowoff);
-            }
-            const float vhv[4] = {vh4.x, vh4.y, vh4.z, vh4.w};
-            const float vlv[4] = {vl4.x, vl4.y, vl4.z, vl4.w};
-            float ah[4], al[4], bh[4], bl[4];
+            float ah[NF][4], al[NF][4], bh[NF][4], bl[NF][4];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 uint64_t site;
                 if constexpr (WIDE) site = (uint64_t)(rowoff + 2 * h);
                 else site = (uint32_t)rowoff + (uint32_t)(2 * h);
-                float2 z = make_float2(0.0f, 0.0f);
-                if (noisy)
-                    z = gauss_cos_f2(noise_key(site, p.step, kPass2Mul, p.seed),
-                                     noise_key(site + 1, p.step, kPass2Mul, p.seed));
-                const float2 x = v_add(cen[h][0], cen[h][1]);
-                float2 vp;
-                if (p.v.vkind == TIPT_VP_POLY) {
-                    const float2 d = v_fma(v_mul(v_mul(vs<float2>((float)p.v.c3), x), x), x,
-                                           v_mul(vs<float2>((float)p.v.c1), x));
-                    vp = p.v.c2 != 0.0 ? v_fma(v_mul(vs<float2>((float)p.v.c2), x), x, d) : d;
+                const uint64_t ka = noise_key(site, p.step, kPass2Mul, p.seed);
+                const uint64_t kb = noise_key(site + 1, p.step, kPass2Mul, p.seed);
+                float2 z[NF], vp[NF];
+                if constexpr (CPLX) {
+                    z[0] = z[1] = make_float2(0.0f, 0.0f);
+                    if (noisy) gauss_pair_f2(ka, kb, z[0], z[1]);
+                    complex_force_v<float2>(p.v, s_tab, tminf, dinvf,
+                                            v_add(cen[h][0][0], cen[h][0][1]),
+                                            v_add(cen[h][1][0], cen[h][1][1]), vp[0], vp[1]);
                 } else {
-                    vp = lerp_table_f32<float2>(s_tab, v_mul(v_sub(x, vs<float2>(tminf)),
-                                                             vs<float2>(dinvf)), last);
+                    z[0] = noisy ? gauss_cos_f2(ka, kb) : make_float2(0.0f, 0.0f);
+                    const float2 x = v_add(cen[h][0][0], cen[h][0][1]);
+                    if (p.v.vkind == TIPT_VP_POLY) {
+                        const float2 d = v_fma(v_mul(v_mul(vs<float2>((float)p.v.c3), x), x), x,
+                                               v_mul(vs<float2>((float)p.v.c1), x));
+                        vp[0] = p.v.c2 != 0.0 ? v_fma(v_mul(vs<float2>((float)p.v.c2), x), x, d) : d;
+                    } else {
+                        vp[0] = lerp_table_f32<float2>(
+                            s_tab, v_mul(v_sub(x, vs<float2>(tminf)), vs<float2>(dinvf)), last);
+                    }
                 }
-                alt_real_site_f32c<MODE>(p, cen[h][0].x, cen[h][1].x, dsum[h][0].x, dsum[h][1].x,
-                                         vp.x, z.x, vhv[2 * h], vlv[2 * h], ah[2 * h], al[2 * h],
-                                         bh[2 * h], bl[2 * h]);
-                alt_real_site_f32c<MODE>(p, cen[h][0].y, cen[h][1].y, dsum[h][0].y, dsum[h][1].y,
-                                         vp.y, z.y, vhv[2 * h + 1], vlv[2 * h + 1], ah[2 * h + 1],
-                                         al[2 * h + 1], bh[2 * h + 1], bl[2 * h + 1]);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    float vh[2] = {0.0f, 0.0f}, vl[2] = {0.0f, 0.0f};
+                    if constexpr (MODE != kOD) {
+                        const float* pif = static_cast<const float*>(p.f[NF + f]);
+                        const float2 a = *reinterpret_cast<const float2*>(pif + rowoff + 2 * h);
+                        const float2 b = *reinterpret_cast<const float2*>(pif + N + rowoff + 2 * h);
+                        vh[0] = a.x; vh[1] = a.y; vl[0] = b.x; vl[1] = b.y;
+                    }
+                    alt_real_site_f32c<MODE>(p, cen[h][f][0].x, cen[h][f][1].x, dsum[h][f][0].x,
+                                             dsum[h][f][1].x, vp[f].x, z[f].x, vh[0], vl[0],
+                                             ah[f][2 * h], al[f][2 * h], bh[f][2 * h], bl[f][2 * h]);
+                    alt_real_site_f32c<MODE>(p, cen[h][f][0].y, cen[h][f][1].y, dsum[h][f][0].y,
+                                             dsum[h][f][1].y, vp[f].y, z[f].y, vh[1], vl[1],
+                                             ah[f][2 * h + 1], al[f][2 * h + 1], bh[f][2 * h + 1],
+                                             bl[f][2 * h + 1]);
+                }
             }
-            if constexpr (MODE != kBA2) {
-                *reinterpret_cast<float4*>(o0 + rowoff) = make_float4(ah[0], ah[1], ah[2], ah[3]);
-                *reinterpret_cast<float4*>(o0 + N + rowoff) = make_float4(al[0], al[1], al[2], al[3]);
-            }
-            if constexpr (MODE != kOD) {
-                *reinterpret_cast<float4*>(o1 + rowoff) = make_float4(bh[0], bh[1], bh[2], bh[3]);
-                *reinterpret_cast<float4*>(o1 + N + rowoff) = make_float4(bl[0], bl[1], bl[2], bl[3]);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                if constexpr (MODE != kBA2) {
+                    float* o = static_cast<float*>(p.o[f]);
+                    *reinterpret_cast<float4*>(o + rowoff) = make_float4(ah[f][0], ah[f][1], ah[f][2], ah[f][3]);
+                    *reinterpret_cast<float4*>(o + N + rowoff) = make_float4(al[f][0], al[f][1], al[f][2], al[f][3]);
+                }
+                if constexpr (MODE != kOD) {
+                    float* o = static_cast<float*>(p.o[NF + f]);
+                    *reinterpret_cast<float4*>(o + rowoff) = make_float4(bh[f][0], bh[f][1], bh[f][2], bh[f][3]);
+                    *reinterpret_cast<float4*>(o + N + rowoff) = make_float4(bl[f][0], bl[f][1], bl[f][2], bl[f][3]);
+                }
             }
             pm = pc;
             pc = pp;
@@ -1174,30 +1197,34 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
     return fail(TIPT_ERR_STORAGE, "marching kernel takes F32C or F64");
 }
 
-// The real-field alternative integrators on the marching ring: compensated
-// FP32, polynomial V' or a table staged in shared memory, n2 % 4 == 0.
-static bool alt_geometry(const AltParams& p, MarchGeom& g, int64_t& smem) {
+// The alternative integrators on the marching ring: compensated FP32,
+// polynomial V' or a table staged in shared memory, n2 % 4 == 0; the complex
+// field without Z_N (its force runs in FP64 on the generic kernel).
+static bool alt_geometry(const AltParams& p, bool cplx, MarchGeom& g, int64_t& smem) {
     if (p.v.vkind != TIPT_VP_POLY && !p.v.table_in_smem) return false;
+    if (cplx && p.v.zn_active > 0.5 && p.v.zn_n > 0.5) return false;
     const int64_t tb = p.v.vkind == TIPT_VP_POLY ? 0 : (int64_t)p.v.npts * 4;
-    return geometry_dims(p.n1, p.n2, p.n0, 4, 2, tb, g, smem);
+    return geometry_dims(p.n1, p.n2, p.n0, 4, cplx ? 4 : 2, tb, g, smem);
 }
 
-bool alt_march_supported(const AltParams& p) {
-    uintptr_t a = reinterpret_cast<uintptr_t>(p.f[0]) | reinterpret_cast<uintptr_t>(p.f[1]) |
-                  reinterpret_cast<uintptr_t>(p.o[0]) | reinterpret_cast<uintptr_t>(p.o[1]);
+bool alt_march_supported(const AltParams& p, bool cplx) {
+    uintptr_t a = 0;
+    for (int q = 0; q < (cplx ? 4 : 2); ++q)
+        a |= reinterpret_cast<uintptr_t>(p.f[q]) | reinterpret_cast<uintptr_t>(p.o[q]);
     if (a % 16) return false;
     MarchGeom g;
     int64_t smem;
-    return alt_geometry(p, g, smem);
+    return alt_geometry(p, cplx, g, smem);
 }
 
-template <int MODE>
+template <int MODE, bool CPLX>
 static int launch_alt_march_k(const AltParams& p, cudaStream_t st) {
     MarchGeom g;
     int64_t smem;
-    if (!alt_geometry(p, g, smem)) return fail(TIPT_ERR_UNSUPPORTED, "integrator march geometry");
+    if (!alt_geometry(p, CPLX, g, smem))
+        return fail(TIPT_ERR_UNSUPPORTED, "integrator march geometry");
     const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
-    auto kern = wide ? alt_march_f32c<MODE, true> : alt_march_f32c<MODE, false>;
+    auto kern = wide ? alt_march_f32c<MODE, CPLX, true> : alt_march_f32c<MODE, CPLX, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess)
@@ -1216,11 +1243,18 @@ static int launch_alt_march_k(const AltParams& p, cudaStream_t st) {
     return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "integrator march launch");
 }
 
-int launch_alt_march(int mode, const AltParams& p, cudaStream_t st) {
+int launch_alt_march(int mode, bool cplx, const AltParams& p, cudaStream_t st) {
+    if (cplx) {
+        switch (mode) {
+            case kOD: return launch_alt_march_k<kOD, true>(p, st);
+            case kBA1: return launch_alt_march_k<kBA1, true>(p, st);
+            default: return launch_alt_march_k<kBA2, true>(p, st);
+        }
+    }
     switch (mode) {
-        case kOD: return launch_alt_march_k<kOD>(p, st);
-        case kBA1: return launch_alt_march_k<kBA1>(p, st);
-        default: return launch_alt_march_k<kBA2>(p, st);
+        case kOD: return launch_alt_march_k<kOD, false>(p, st);
+        case kBA1: return launch_alt_march_k<kBA1, false>(p, st);
+        default: return launch_alt_march_k<kBA2, false>(p, st);
     }
 }
 

@@ -8,10 +8,11 @@ namespace tipt {
 bool march_supported(int storage, const RealStageParams& p);
 int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cudaStream_t st);
 
-// Real-field overdamped / BAOAB passes (mode kOD, kBA1, kBA2), compensated FP32.
+// Overdamped / BAOAB passes (mode kOD, kBA1, kBA2) of the real or complex
+// field, compensated FP32.
 struct AltParams;
-bool alt_march_supported(const AltParams& p);
-int launch_alt_march(int mode, const AltParams& p, cudaStream_t st);
+bool alt_march_supported(const AltParams& p, bool cplx);
+int launch_alt_march(int mode, bool cplx, const AltParams& p, cudaStream_t st);
 
 // Complex field, compensated FP32, Z_N off, V'(rho) polynomial or staged in shared memory.
 bool complex_march_supported(const ComplexStageParams& p);

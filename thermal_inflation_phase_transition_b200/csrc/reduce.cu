@@ -254,6 +254,110 @@ __global__ void __launch_bounds__(kRedThreads) obs_march_kernel(ObsParams p) {
     }
 }
 
+// Compensated-FP32 form of the marching reduction: the per-site terms in FP32
+// -- a value as hi + lo, a neighbour difference as (hi_n - hi_c) + (lo_n - lo_c)
+// (the hi difference is exact for close neighbours) -- summed over the
+// thread's four sites in FP32 and added to the FP64 accumulators once per
+// plane (a term's relative error is about 6e-8; min and max are FP32 values of
+// hi + lo).  The threshold test compares the pair with the threshold split
+// into hi + lo, so it is exact.
+__global__ void __launch_bounds__(kRedThreads) obs_march_f32c_kernel(ObsParams p) {
+    const int n0 = p.n0, n1 = p.n1, n2 = p.n2;
+    const int64_t n12 = (int64_t)n1 * n2;
+    const int64_t N = (int64_t)n0 * n12;
+    const int tpr = n2 >> 2;
+    const int64_t cols = (int64_t)n1 * tpr;
+    const int64_t col = (int64_t)blockIdx.x * kRedThreads + threadIdx.x;
+    ObsAcc a;
+    acc_init(a);
+    if (col < cols) {
+        const float* phi = static_cast<const float*>(p.phi);
+        const float* pi = static_cast<const float*>(p.pi);
+        const int j = (int)(col / tpr);
+        const int k0 = 4 * (int)(col - (int64_t)j * tpr);
+        const int64_t rj = (int64_t)j * n2 + k0;
+        const int64_t rjp = (int64_t)(j + 1 < n1 ? j + 1 : 0) * n2 + k0;
+        const int64_t rkp = (int64_t)j * n2 + (k0 + 4 < n2 ? k0 + 4 : 0);
+        const int i0 = p.i_begin + blockIdx.y * kObsPlanes;
+        const int ni = min(kObsPlanes, p.i_end - i0);
+        const float qa = (float)(0.25 * p.lam), qb = (float)(-0.5 * p.m2);
+        const float th = (float)p.thr, tl = (float)(p.thr - (double)th);
+        auto ld4 = [&](const float* f, int64_t o, float v[4]) {
+            const float4 x = __ldg(reinterpret_cast<const float4*>(f + o));
+            v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+        };
+        float ch[4], cl[4];
+        ld4(phi, (int64_t)i0 * n12 + rj, ch);
+        ld4(phi, N + (int64_t)i0 * n12 + rj, cl);
+        for (int q = 0; q < ni; ++q) {
+            const int i = i0 + q;
+            const int64_t pc = (int64_t)i * n12;
+            const int64_t pnx = (int64_t)(i + 1 < n0 ? i + 1 : 0) * n12;
+            float nh[4], nl[4], jh[4], jl[4], vh[4] = {0, 0, 0, 0}, vl[4] = {0, 0, 0, 0};
+            ld4(phi, pnx + rj, nh);
+            ld4(phi, N + pnx + rj, nl);
+            ld4(phi, pc + rjp, jh);
+            ld4(phi, N + pc + rjp, jl);
+            if (pi) {
+                ld4(pi, pc + rj, vh);
+                ld4(pi, N + pc + rj, vl);
+            }
+            const float kh = __ldg(phi + pc + rkp), kl = __ldg(phi + N + pc + rkp);
+            float gs = 0.0f, ps = 0.0f, s1 = 0.0f, s2 = 0.0f, sq = 0.0f;
+            float mn = INFINITY, mx = -INFINITY;
+            int above = 0, bad = 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float c = __fadd_rn(ch[u], cl[u]);
+                // forward differences, R:2303-2308
+                const float fx = __fadd_rn(__fsub_rn(nh[u], ch[u]), __fsub_rn(nl[u], cl[u]));
+                const float fy = __fadd_rn(__fsub_rn(jh[u], ch[u]), __fsub_rn(jl[u], cl[u]));
+                const float fz = __fadd_rn(__fsub_rn(u < 3 ? ch[u + 1] : kh, ch[u]),
+                                           __fsub_rn(u < 3 ? cl[u + 1] : kl, cl[u]));
+                gs = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, __fmaf_rn(fz, fz, gs)));
+                const float c2 = __fmul_rn(c, c);
+                ps = __fmaf_rn(__fmaf_rn(qa, c2, qb), c2, ps);
+                s1 = __fadd_rn(s1, c);
+                s2 = __fadd_rn(s2, c2);
+                const float v = __fadd_rn(vh[u], vl[u]);
+                sq = __fmaf_rn(v, v, sq);
+                above += (ch[u] > th || (ch[u] == th && cl[u] > tl)) ? 1 : 0;
+                bad += (isfinite(c) && isfinite(v)) ? 0 : 1;
+                mn = fminf(mn, c);
+                mx = fmaxf(mx, c);
+            }
+            a.grad += (double)gs;
+            a.pot += (double)ps * p.inv_mu2;
+            a.s1 += (double)s1;
+            a.s2 += (double)s2;
+            a.sq += (double)sq;
+            a.above += (double)above;
+            a.nonfinite += (double)bad;
+            a.mn = fmin(a.mn, (double)mn);
+            a.mx = fmax(a.mx, (double)mx);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                ch[u] = nh[u];
+                cl[u] = nl[u];
+            }
+        }
+    }
+    a = block_reduce(a);
+    if (threadIdx.x == 0) {
+        double* o = p.partials + ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * kObs;
+        o[0] = 0.0;
+        o[1] = a.grad;
+        o[2] = a.pot;
+        o[3] = a.s1;
+        o[4] = a.s2;
+        o[5] = a.sq;
+        o[6] = a.above;
+        o[7] = a.mn;
+        o[8] = a.mx;
+        o[9] = a.nonfinite;
+    }
+}
+
 __global__ void __launch_bounds__(kRedThreads) obs_final_kernel(ObsParams p, int G, double inv_n) {
     ObsAcc a;
     acc_init(a);
@@ -347,7 +451,7 @@ int launch_observables(int storage, const void* phi, const void* pi, int n0, int
         switch (storage) {
             case TIPT_F64: obs_march_kernel<TIPT_F64><<<grid, kRedThreads, 0, st>>>(p); break;
             case TIPT_F32: obs_march_kernel<TIPT_F32><<<grid, kRedThreads, 0, st>>>(p); break;
-            default: obs_march_kernel<TIPT_F32C><<<grid, kRedThreads, 0, st>>>(p); break;
+            default: obs_march_f32c_kernel<<<grid, kRedThreads, 0, st>>>(p); break;
         }
     } else {
         switch (storage) {

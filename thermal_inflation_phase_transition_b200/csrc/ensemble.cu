@@ -75,6 +75,77 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
         p.c3 = rp.c3;
         const uint32_t n12 = (uint32_t)rp.n1 * (uint32_t)rp.n2;
         const F32CConst kc = f32c_const(p);
+        if constexpr (S == TIPT_F32C) {
+            // Site pairs (s, s + 1) with s even share i and j when n2 is even: one
+            // 8-byte load per field plane and neighbour, the stencil sums and the
+            // update in the lanes of the packed FP32x2 instructions (bitwise the
+            // one-site arithmetic, as in the marching kernel).
+            if ((rp.n2 & 1) == 0 && ((ch.begin | ch.count | rp.offset) & 1) == 0) {
+                const float* phi = static_cast<const float*>(e.phi);
+                const float* pi = static_cast<const float*>(e.pi);
+                float* po = static_cast<float*>(e.phi_out);
+                float* vo = static_cast<float*>(e.pi_out);
+                const int64_t N = e.n_total;
+                for (int t = threadIdx.x; 2 * t < ch.count; t += blockDim.x) {
+                    const uint32_t s = (uint32_t)(ch.begin + 2 * t);
+                    const uint32_t q = fdiv(s, rp.m2);
+                    const uint32_t k = s - q * (uint32_t)rp.n2;
+                    const uint32_t i = fdiv(q, rp.m1);
+                    const uint32_t j = q - i * (uint32_t)rp.n1;
+                    const int64_t g = rp.offset + s;
+                    const int64_t o4[4] = {
+                        (i + 1 < (uint32_t)rp.n0) ? (int64_t)n12 : -(int64_t)(rp.n0 - 1) * n12,
+                        (i > 0) ? -(int64_t)n12 : (int64_t)(rp.n0 - 1) * n12,
+                        (j + 1 < (uint32_t)rp.n1) ? rp.n2 : -(int64_t)(rp.n1 - 1) * rp.n2,
+                        (j > 0) ? -(int64_t)rp.n2 : (int64_t)(rp.n1 - 1) * rp.n2};
+                    const int64_t gkr = g + ((k + 2 < (uint32_t)rp.n2) ? 2 : 2 - (int64_t)rp.n2);
+                    const int64_t gkl = g + ((k > 0) ? -1 : (int64_t)(rp.n2 - 1));
+                    const float* base[4] = {phi, phi + N, pi, pi + N};  // phi hi, lo, pi hi, lo
+                    float2 dsum[4], cen[4];
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) {
+                        const float* b = base[f];
+                        const float2 cc = __ldg(reinterpret_cast<const float2*>(b + g));
+                        float2 nb[6];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            nb[u] = __ldg(reinterpret_cast<const float2*>(b + g + o4[u]));
+                        nb[4] = make_float2(cc.y, __ldg(b + gkr));  // k+1
+                        nb[5] = make_float2(__ldg(b + gkl), cc.x);  // k-1
+                        float2 acc;
+                        if ((f & 1) == 0) {  // hi: sum (hi_n - hi_c)
+                            acc = v_sub(nb[0], cc);
+#pragma unroll
+                            for (int n = 1; n < 6; ++n) acc = v_add(acc, v_sub(nb[n], cc));
+                        } else {             // lo: fma(-6, lo_c, sum lo_n)
+                            acc = nb[0];
+#pragma unroll
+                            for (int n = 1; n < 6; ++n) acc = v_add(acc, nb[n]);
+                            acc = v_fma(vs<float2>(-6.0f), cc, acc);
+                        }
+                        dsum[f] = acc;
+                        cen[f] = cc;
+                    }
+                    F32CIn<float2> x;
+                    x.dh_phi = dsum[0];
+                    x.dl_phi = dsum[1];
+                    x.dh_pi = dsum[2];
+                    x.dl_pi = dsum[3];
+                    x.phh = cen[0];
+                    x.phl = cen[1];
+                    x.pih = cen[2];
+                    x.pil = cen[3];
+                    float2 a, b, cc, d;
+                    update_f32c<float2>(p, kc, nullptr, x, site_kick_f32c2(p, kc, (uint64_t)s), a, b,
+                                        cc, d);
+                    *reinterpret_cast<float2*>(po + g) = a;
+                    *reinterpret_cast<float2*>(po + N + g) = b;
+                    *reinterpret_cast<float2*>(vo + g) = cc;
+                    *reinterpret_cast<float2*>(vo + N + g) = d;
+                }
+                continue;
+            }
+        }
         for (int t = threadIdx.x; t < ch.count; t += blockDim.x) {
             const uint32_t s = (uint32_t)(ch.begin + t);
             const uint32_t q = fdiv(s, rp.m2);

@@ -112,3 +112,25 @@ def test_gamma_mle_censoring():
     assert n == 3
     assert abs(g - 3 / (8.0 * 0.5 * (10 + 20 + 100 + 100))) < 1e-15
     assert abs(rel - 1 / 3 ** 0.5) < 1e-15
+
+
+def test_slab_entries_reject_bad_ranges():
+    """The slab step and slab observables check the plane range before any launch."""
+    lib = L.lib()
+    buf = (C.c_double * 4096)()
+    p = C.cast(buf, C.c_void_p)
+    # nz = 1 (2-D lattices are one GPU's work)
+    assert lib.tipt_rk2_step_table_slab(L.TIPT_F64, p, p, p, p, 4, 4, 1, 0, 8, _sp(), _vs(),
+                                        None) == 1
+    # planes [6, 10) outside an 8-plane lattice
+    assert lib.tipt_rk2_step_table_slab(L.TIPT_F64, p, p, p, p, 4, 4, 4, 6, 8, _sp(), _vs(),
+                                        None) == 1
+    assert b"outside" in lib.tipt_last_error()
+    # site count below the slab's
+    out = (C.c_double * 10)()
+    assert lib.tipt_observables_slab(L.TIPT_F64, p, None, 4, 4, 4, 10, 1.0, 1.0, 0.0, 0.0, 1.0,
+                                     1.0, C.cast(out, C.c_void_p), p, 8 * 4096, None) == 1
+    # workspace too small
+    assert lib.tipt_observables_slab(L.TIPT_F64, p, None, 4, 4, 4, 512, 1.0, 1.0, 0.0, 0.0, 1.0,
+                                     1.0, C.cast(out, C.c_void_p), p, 8, None) == 1
+    assert b"workspace" in lib.tipt_last_error()

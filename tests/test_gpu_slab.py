@@ -96,3 +96,53 @@ def test_slab_rejects_bad_ranges():
         L.call("tipt_rk2_step_table_slab", L.TIPT_F64, phi.data_ptr(), pi.data_ptr(),
                phi.data_ptr(), pi.data_ptr(), 6, 4, 8, 3, 8,
                RF.step_params(0.05, 1, 1, 1, 1), vs, None)
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_slab_far_planes_use_64bit_site_keys(storage):
+    """A slab whose lattice-wide site indices pass 2^32 runs the kernels' 64-bit
+    noise-key path: the step equals the oracle step with the noise keyed by the
+    lattice-wide index, and the marching and generic kernels agree bit for bit."""
+    from oracle import oracle as O
+    n1, n2, nxl = 16, 32, 4
+    i_lo = (1 << 32) // (n1 * n2) + 5
+    nxg = i_lo + nxl + 10
+    ns, step, seed = 0.3, 7, 2
+    rng = np.random.default_rng(31)
+    shape = (nxl + 2, n1, n2)
+    phi0, pi0 = rng.normal(0.6, 0.5, shape), rng.normal(0.0, 0.3, shape)
+    keys = np.array([O.noise_key(((i_lo - 1 + q) * n1 + j) * n2 + k, step, O.K_PASS2, seed)
+                     for q in range(nxl + 2) for j in range(n1) for k in range(n2)],
+                    dtype=np.uint64)
+    noise = (ns * O.hash_pair(keys)[2]).reshape(shape)
+    tab, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.0), 0.0, 3.0, 1024)
+    a, b = phi0.copy(), pi0.copy()
+    O.rk2_step_table(a, b, 0.05, 1.0, 1.0, 1.0, noise, np.empty(shape), np.empty(shape), 1.0,
+                     tab, tmin, dinv, 1024)
+    vs, _t = _vs()
+    outs = []
+    for policy in (0, 1):
+        L.set_kernel_policy(policy)
+        try:
+            phi = torch.from_numpy(phi0).to(DEV)
+            pi = torch.from_numpy(pi0).to(DEV)
+            if storage == "f32c":
+                phi, pi = RF.to_f32c(phi), RF.to_f32c(pi)
+            po, vo = torch.zeros_like(phi), torch.zeros_like(pi)
+            sp = RF.step_params(0.05, 1.0, 1.0, 1.0, 1.0, ns, step, seed)
+            L.call("tipt_rk2_step_table_slab", L.TIPT_F32C if storage == "f32c" else L.TIPT_F64,
+                   phi.data_ptr(), pi.data_ptr(), po.data_ptr(), vo.data_ptr(), nxl, n1, n2,
+                   i_lo, nxg, sp, vs, None)
+            torch.cuda.synchronize()
+        finally:
+            L.set_kernel_policy(0)
+        outs.append((po, vo))
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+    po, vo = outs[0]
+    if storage == "f32c":
+        po, vo = RF.from_f32c(po), RF.from_f32c(vo)
+    got_phi, got_pi = po.cpu().numpy()[1:-1], vo.cpu().numpy()[1:-1]
+    tol = 1e-12 if storage == "f64" else 2e-6
+    np.testing.assert_allclose(got_phi, a[1:-1], rtol=0, atol=tol * np.abs(a).max())
+    np.testing.assert_allclose(got_pi, b[1:-1], rtol=0, atol=tol * np.abs(b).max())
+    assert L.device_status() == 0

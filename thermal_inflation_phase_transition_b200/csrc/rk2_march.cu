@@ -484,13 +484,10 @@ __global__ void __maxnreg__(kMarchRegs)
                     const float4 jp = *reinterpret_cast<const float4*>(sc + drow + k0);
                     const float4 im = *reinterpret_cast<const float4*>(blk(pm.stage, f, c) + orow + k0);
                     const float4 ip = *reinterpret_cast<const float4*>(blk(pp.stage, f, c) + orow + k0);
-                    // k-1 of site 0 and k+1 of site 3 are the neighbouring lanes' end
-                    // values (shuffles); shared-memory reads only at warp and row ends,
-                    // which keeps the four-site stride off conflicting banks
-                    float kl = __shfl_up_sync(0xffffffffu, ce.w, 1);
-                    float kr = __shfl_down_sync(0xffffffffu, ce.x, 1);
-                    if (lane == 0 || k0 == 0) kl = sc[orow + kml];
-                    if (lane == 31 || k0 + 4 == n2) kr = sc[orow + kpr];
+                    // k-1 of site 0 and k+1 of site 3 (scalar reads: fewer instructions
+                    // than lane shuffles, which this issue-bound kernel prefers to the
+                    // 4-way bank conflict they remove)
+                    const float kl = sc[orow + kml], kr = sc[orow + kpr];
                     // site pairs (0,1) and (2,3): centre and the six neighbours
                     const float2 cc[2] = {make_float2(ce.x, ce.y), make_float2(ce.z, ce.w)};
                     const float2 nb[2][6] = {

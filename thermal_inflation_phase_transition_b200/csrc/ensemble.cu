@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
         p.c2 = rp.c2;
         p.c3 = rp.c3;
         const uint32_t n12 = (uint32_t)rp.n1 * (uint32_t)rp.n2;
+        set_f32c_pairs(p);
         const F32CConst kc = f32c_const(p);
         if constexpr (S == TIPT_F32C) {
             // Site pairs (s, s + 1) with s even share i and j when n2 is even: one

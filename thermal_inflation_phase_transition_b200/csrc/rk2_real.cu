@@ -167,6 +167,7 @@ int launch_real_stage(int storage, RealStageParams p, cudaStream_t st) {
         return fail(TIPT_ERR_UNSUPPORTED, "2-D V' table row of %d points exceeds %lld bytes of "
                     "shared memory", p.npts, (long long)kMaxTableSmem);
     const int64_t smem = p.table_in_smem ? tb : 0;
+    set_f32c_pairs(p);
     const bool march = g_kernel_policy != 1 && march_supported(storage, p);
     if (g_kernel_policy == 2 && !march)
         return fail(TIPT_ERR_UNSUPPORTED, "marching kernel does not cover this shape/storage");

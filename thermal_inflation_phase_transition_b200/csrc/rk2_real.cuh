@@ -42,6 +42,12 @@ struct RealStageParams {
     long long offset;
     long long sched_len;  // steps beyond the schedule reuse its last entry
     double ns_mult;
+    // FP32 constants of the compensated storage as lane pairs (x = y), rounded
+    // from the FP64 parameters on the host (set_f32c_pairs): the packed FP32x2
+    // instructions then read them from the parameter bank.
+    struct {
+        float2 h1, h2h, h2l, inv_dx2, inv_a2, eta, inv_mu2, c1, c2, c3, tmin, dinv;
+    } k2;
     // Planes computed: [i_begin, i_end) of the n0 planes (all planes, periodic
     // in i, when i_end = 0); the noise key's site is the array index plus
     // site_offset (a slab of a larger lattice keys by the global index).
@@ -115,6 +121,30 @@ struct F32CConst {
     float ns;                      // hash noise amplitude
 };
 
+// Fills RealStageParams::k2 from the FP64 parameters (host or device).
+__host__ __device__ inline void set_f32c_pairs(RealStageParams& p) {
+    auto pr = [](float x) { return make_float2(x, x); };
+    const float h2h = (float)p.h2;
+    p.k2.h1 = pr((float)p.h1);
+    p.k2.h2h = pr(h2h);
+    p.k2.h2l = pr((float)(p.h2 - (double)h2h));
+    p.k2.inv_dx2 = pr((float)p.inv_dx2);
+    p.k2.inv_a2 = pr((float)p.inv_a2);
+    p.k2.eta = pr((float)p.eta);
+    p.k2.inv_mu2 = pr((float)p.inv_mu2);
+    p.k2.c1 = pr((float)p.c1);
+    p.k2.c2 = pr((float)p.c2);
+    p.k2.c3 = pr((float)p.c3);
+    p.k2.tmin = pr((float)p.tmin);
+    p.k2.dinv = pr((float)p.dinv);
+}
+
+// A lane-pair constant as a lane vector.
+__device__ __forceinline__ float kv(float2 c, float) { return c.x; }
+__device__ __forceinline__ float2 kv(float2 c, float2) { return c; }
+template <typename V>
+__device__ __forceinline__ V kvec(float2 c) { return kv(c, V{}); }
+
 __device__ __forceinline__ F32CConst f32c_const(const RealStageParams& p) {
     F32CConst k;
     k.h1 = (float)p.h1;
@@ -139,8 +169,8 @@ __device__ __forceinline__ V vprime_v(const RealStageParams& p, const F32CConst&
                                       const float* s_tab, V x) {
     constexpr int NL = sizeof(V) / sizeof(float);
     if (p.vkind == TIPT_VP_POLY) {
-        const V d = v_fma(v_mul(v_mul(vs<V>(kc.c3), x), x), x, v_mul(vs<V>(kc.c1), x));
-        return p.c2 != 0.0 ? v_fma(v_mul(vs<V>(kc.c2), x), x, d) : d;
+        const V d = v_fma(v_mul(v_mul(kvec<V>(p.k2.c3), x), x), x, v_mul(kvec<V>(p.k2.c1), x));
+        return p.c2 != 0.0 ? v_fma(v_mul(kvec<V>(p.k2.c2), x), x, d) : d;
     }
     if (!p.table_in_smem) {
         V r;
@@ -150,7 +180,8 @@ __device__ __forceinline__ V vprime_v(const RealStageParams& p, const F32CConst&
                                                  (double)vlane(x, l)));
         return r;
     }
-    return lerp_table_f32<V>(s_tab, v_mul(v_sub(x, vs<V>(kc.tmin)), vs<V>(kc.dinv)), kc.last);
+    return lerp_table_f32<V>(s_tab, v_mul(v_sub(x, kvec<V>(p.k2.tmin)), kvec<V>(p.k2.dinv)),
+                             kc.last);
 }
 
 // Noise increment for one site (FP64): array value * nfac, or ns_eff * z.
@@ -237,11 +268,12 @@ template <typename V>
 __device__ __forceinline__ void update_f32c(const RealStageParams& p, const F32CConst& kc,
                                             const float* s_tab, const F32CIn<V>& x, V kick,
                                             V& phh, V& phl, V& pih, V& pil) {
-    const V h1 = vs<V>(kc.h1);
-    const V h2h = vs<V>(kc.h2h);
-    const V h2l = vs<V>(kc.h2l);
-    const V inv_dx2 = vs<V>(kc.inv_dx2);
-    const V inv_a2 = vs<V>(kc.inv_a2), eta = vs<V>(kc.eta), inv_mu2 = vs<V>(kc.inv_mu2);
+    const V h1 = kvec<V>(p.k2.h1);
+    const V h2h = kvec<V>(p.k2.h2h);
+    const V h2l = kvec<V>(p.k2.h2l);
+    const V inv_dx2 = kvec<V>(p.k2.inv_dx2);
+    const V inv_a2 = kvec<V>(p.k2.inv_a2), eta = kvec<V>(p.k2.eta),
+            inv_mu2 = kvec<V>(p.k2.inv_mu2);
     const V lap = v_mul(v_add(x.dh_phi, x.dl_phi), inv_dx2);
     const V lapv = v_mul(v_add(x.dh_pi, x.dl_pi), inv_dx2);
     const V lap2 = v_fma(h1, lapv, lap);  // Laplacian of phi + h1 pi

@@ -167,23 +167,18 @@ __global__ void __launch_bounds__(kRedThreads) obs_partial_kernel(ObsParams p) {
 // shape only.
 constexpr int kObsPlanes = 64;
 
+// Four consecutive sites as FP64 (F64 and F32 storages; compensated FP32 has
+// its own kernel below).
 template <int S>
-__device__ __forceinline__ void load4(const void* f, int64_t s, int64_t N, double v[4]) {
+__device__ __forceinline__ void load4(const void* f, int64_t s, double v[4]) {
     if constexpr (S == TIPT_F64) {
         const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(f) + s);
         const double2 a = __ldg(q), b = __ldg(q + 1);
         v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-    } else if constexpr (S == TIPT_F32) {
+    } else {
+        static_assert(S == TIPT_F32, "F64 or F32 storage");
         const float4 a = __ldg(reinterpret_cast<const float4*>(static_cast<const float*>(f) + s));
         v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-    } else {
-        const float* g = static_cast<const float*>(f);
-        const float4 h = __ldg(reinterpret_cast<const float4*>(g + s));
-        const float4 l = __ldg(reinterpret_cast<const float4*>(g + N + s));
-        v[0] = (double)h.x + (double)l.x;
-        v[1] = (double)h.y + (double)l.y;
-        v[2] = (double)h.z + (double)l.z;
-        v[3] = (double)h.w + (double)l.w;
     }
 }
 
@@ -206,14 +201,14 @@ __global__ void __launch_bounds__(kRedThreads) obs_march_kernel(ObsParams p) {
         const int i0 = p.i_begin + blockIdx.y * kObsPlanes;
         const int ni = min(kObsPlanes, p.i_end - i0);
         double ph[4], pn[4], pv[4], jp[4], kp;
-        load4<S>(p.phi, (int64_t)i0 * n12 + rj, N, ph);
+        load4<S>(p.phi, (int64_t)i0 * n12 + rj, ph);
         for (int q = 0; q < ni; ++q) {
             const int i = i0 + q;
             const int64_t pc = (int64_t)i * n12;
             const int64_t pnx = (int64_t)(i + 1 < n0 ? i + 1 : 0) * n12;
-            load4<S>(p.phi, pnx + rj, N, pn);
-            load4<S>(p.phi, pc + rjp, N, jp);
-            if (p.pi) load4<S>(p.pi, pc + rj, N, pv);
+            load4<S>(p.phi, pnx + rj, pn);
+            load4<S>(p.phi, pc + rjp, jp);
+            if (p.pi) load4<S>(p.pi, pc + rj, pv);
             else pv[0] = pv[1] = pv[2] = pv[3] = 0.0;
             kp = load_val<S>(p.phi, pc + rkp, N);
 #pragma unroll

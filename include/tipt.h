@@ -137,6 +137,16 @@ int tipt_rk2_step_table_slab(int storage, const void* phi, const void* pi, void*
                              int64_t nx_global, const tipt_step_params* sp,
                              const tipt_vsource* vp, void* stream);
 
+/* tipt_rk2_step_table_slab for the array planes [plane_begin, plane_end) of
+ * [1, nx_local + 1) only: the interior planes 2 .. nx_local - 1 read no ghost
+ * plane and can run while the halo exchange is in flight, the two edge planes
+ * after it.  No reference counterpart. */
+int tipt_rk2_step_table_slab_planes(int storage, const void* phi, const void* pi, void* phi_out,
+                                    void* pi_out, int64_t nx_local, int64_t ny, int64_t nz,
+                                    int64_t i_lo, int64_t nx_global, int64_t plane_begin,
+                                    int64_t plane_end, const tipt_step_params* sp,
+                                    const tipt_vsource* vp, void* stream);
+
 /* rk2_step_table with the per-step scalars read on the device, for step loops
  * captured once into a CUDA graph and replayed (the reference's host loop
  * R:3619-3768 recomputes them each step on the host).  The step index is

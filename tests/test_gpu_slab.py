@@ -146,3 +146,35 @@ def test_slab_far_planes_use_64bit_site_keys(storage):
     np.testing.assert_allclose(got_phi, a[1:-1], rtol=0, atol=tol * np.abs(a).max())
     np.testing.assert_allclose(got_pi, b[1:-1], rtol=0, atol=tol * np.abs(b).max())
     assert L.device_status() == 0
+
+
+@pytest.mark.parametrize("storage", ["f32c", "f64"])
+@pytest.mark.parametrize("shape", [(16, 8, 64), (3, 4, 32), (2, 4, 16)])
+def test_overlapped_slab_step_equals_plain(storage, shape):
+    """One rank: the exchange on the side stream with the interior planes stepped
+    meanwhile and the edge planes after it gives the plain step's bits, which are
+    the single-lattice step's."""
+    vs, _t = _vs()
+    phi, pi = _state(shape, storage, 6)
+    a, b = phi.clone(), pi.clone()
+    ao, bo = torch.empty_like(a), torch.empty_like(b)
+    for n in range(3):
+        RF.rk2_step_table_into(a, b, ao, bo, 0.05, 1.0, 1.0, 1.0, 1.0, vs, noise_scale=0.3,
+                               noise_step=n, seed=4)
+        a, ao = ao, a
+        b, bo = bo, b
+    sl = Slab(shape, rank=0, world=1)
+    res = []
+    for overlap in (False, True):
+        x, y = sl.scatter(phi), sl.scatter(pi)
+        xo, yo = torch.empty_like(x), torch.empty_like(y)
+        for n in range(3):
+            sl.step(x, y, xo, yo, 0.05, 1.0, 1.0, 1.0, 1.0, vs, noise_scale=0.3, noise_step=n,
+                    seed=4, overlap=overlap)
+            x, xo = xo, x
+            y, yo = yo, y
+        torch.cuda.synchronize()
+        res.append((sl.interior(x).contiguous(), sl.interior(y).contiguous()))
+    assert torch.equal(res[0][0], res[1][0]) and torch.equal(res[0][1], res[1][1])
+    assert torch.equal(res[1][0], a) and torch.equal(res[1][1], b)
+    assert L.device_status() == 0

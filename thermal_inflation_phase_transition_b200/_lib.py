@@ -79,6 +79,8 @@ _SIGS = {
                                   C.POINTER(VSource), _p, _i64, _p, _i64, _p],
     "tipt_rk2_step_table_slab": [_i, _p, _p, _p, _p, _i64, _i64, _i64, _i64, _i64,
                                  C.POINTER(StepParams), C.POINTER(VSource), _p],
+    "tipt_rk2_step_table_slab_planes": [_i, _p, _p, _p, _p, _i64, _i64, _i64, _i64, _i64, _i64,
+                                        _i64, C.POINTER(StepParams), C.POINTER(VSource), _p],
     "tipt_counter_add": [_p, _i64, _p],
     "tipt_ensemble_step": [_i, _p, _p, _p, _p, _i64, _p, _p, C.c_int32, _p,
                            C.POINTER(StepParams), _p, _i64, _p],

@@ -204,15 +204,19 @@ int tipt_rk2_step_table(int storage, const void* phi, const void* pi, void* phi_
     return launch_real_stage(storage, p, (cudaStream_t)stream);
 }
 
-int tipt_rk2_step_table_slab(int storage, const void* phi, const void* pi, void* phi_out,
-                             void* pi_out, int64_t nx_local, int64_t ny, int64_t nz, int64_t i_lo,
-                             int64_t nx_global, const tipt_step_params* sp,
-                             const tipt_vsource* vp, void* stream) {
+int tipt_rk2_step_table_slab_planes(int storage, const void* phi, const void* pi, void* phi_out,
+                                    void* pi_out, int64_t nx_local, int64_t ny, int64_t nz,
+                                    int64_t i_lo, int64_t nx_global, int64_t plane_begin,
+                                    int64_t plane_end, const tipt_step_params* sp,
+                                    const tipt_vsource* vp, void* stream) {
     int rc;
     if (nx_local < 1 || nz < 2) return fail(TIPT_ERR_ARG, "slab needs nx_local >= 1 and nz >= 2");
     if (i_lo < 0 || i_lo + nx_local > nx_global)
         return fail(TIPT_ERR_ARG, "slab planes [%lld, %lld) outside the %lld-plane lattice",
                     (long long)i_lo, (long long)(i_lo + nx_local), (long long)nx_global);
+    if (plane_begin < 1 || plane_end > nx_local + 1 || plane_begin >= plane_end)
+        return fail(TIPT_ERR_ARG, "array planes [%lld, %lld) not inside [1, %lld)",
+                    (long long)plane_begin, (long long)plane_end, (long long)(nx_local + 1));
     if ((rc = check_state(storage, phi, pi, phi_out, pi_out, nx_local + 2, ny, nz))) return rc;
     if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
     if ((rc = check_vsource(vp, "vp"))) return rc;
@@ -223,10 +227,18 @@ int tipt_rk2_step_table_slab(int storage, const void* phi, const void* pi, void*
     p.nfac = 1.0;
     p.ns_eff = sp->noise_scale;
     p.mul = kPass2Mul;
-    p.i_begin = 1;
-    p.i_end = (int)nx_local + 1;
+    p.i_begin = (int)plane_begin;
+    p.i_end = (int)plane_end;
     p.site_offset = (long long)(i_lo - 1) * ny * nz;  // array plane 1 = lattice plane i_lo
     return launch_real_stage(storage, p, (cudaStream_t)stream);
+}
+
+int tipt_rk2_step_table_slab(int storage, const void* phi, const void* pi, void* phi_out,
+                             void* pi_out, int64_t nx_local, int64_t ny, int64_t nz, int64_t i_lo,
+                             int64_t nx_global, const tipt_step_params* sp,
+                             const tipt_vsource* vp, void* stream) {
+    return tipt_rk2_step_table_slab_planes(storage, phi, pi, phi_out, pi_out, nx_local, ny, nz,
+                                           i_lo, nx_global, 1, nx_local + 1, sp, vp, stream);
 }
 
 int tipt_rk2_step_table_sched(int storage, const void* phi, const void* pi, void* phi_out,

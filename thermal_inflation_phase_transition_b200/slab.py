@@ -146,29 +146,56 @@ class Slab:
 
     # ------------------------------------------------------------- step ---
     def step(self, phi, pi, phi_out, pi_out, dt, dx, eta_eff, mu, inv_a2, vsource, *,
-             noise_scale=0.0, noise_step=0, seed=0, stream=None, stepper=None):
+             noise_scale=0.0, noise_step=0, seed=0, stream=None, stepper=None, overlap=True):
         """Halo exchange of (phi, pi), then one midpoint step of the local planes
         into (phi_out, pi_out) (rk2_step_table, R:1875-1966, hash noise).
-        `stepper`, if given, replaces the library call with the same arguments
-        (the CPU tests pass the oracle)."""
-        self.exchange(phi, pi)
+
+        With ``overlap`` (and at least three local planes) the exchange runs on a
+        second stream while the interior planes 2 .. nx_local - 1, which read no
+        ghost plane, are stepped; the two edge planes follow the exchange.  The
+        result is the same either way.  `stepper`, if given, replaces the library
+        call with the same arguments after a plain exchange (the CPU tests pass
+        the oracle)."""
+        kw = dict(noise_scale=noise_scale, noise_step=noise_step, seed=seed)
         if stepper is not None:
+            self.exchange(phi, pi)
             return stepper(self, phi, pi, phi_out, pi_out, dt, dx, eta_eff, mu, inv_a2, vsource,
                            noise_scale, noise_step, seed)
-        self.step_local(phi, pi, phi_out, pi_out, dt, dx, eta_eff, mu, inv_a2, vsource,
-                        noise_scale=noise_scale, noise_step=noise_step, seed=seed, stream=stream)
+        args = (phi, pi, phi_out, pi_out, dt, dx, eta_eff, mu, inv_a2, vsource)
+        n = self.nx_local
+        if not overlap or n < 3:
+            self.exchange(phi, pi)
+            self.step_local(*args, stream=stream, **kw)
+            return
+        main = torch.cuda.current_stream(phi.device) if stream is None else stream
+        if getattr(self, "_comm", None) is None:
+            self._comm = torch.cuda.Stream(device=phi.device)
+        ready = torch.cuda.Event()
+        ready.record(main)                      # the inputs are complete on the main stream
+        self._comm.wait_event(ready)
+        with torch.cuda.stream(self._comm):
+            self.exchange(phi, pi)
+        done = torch.cuda.Event()
+        done.record(self._comm)
+        self.step_local(*args, stream=main, planes=(2, n), **kw)      # interior planes
+        main.wait_event(done)
+        self.step_local(*args, stream=main, planes=(1, 2), **kw)      # edge planes
+        self.step_local(*args, stream=main, planes=(n, n + 1), **kw)
 
     def step_local(self, phi, pi, phi_out, pi_out, dt, dx, eta_eff, mu, inv_a2, vsource, *,
-                   noise_scale=0.0, noise_step=0, seed=0, stream=None):
-        """The step of the local planes alone (ghost planes already filled)."""
+                   noise_scale=0.0, noise_step=0, seed=0, stream=None, planes=None):
+        """The step of the local planes alone (ghost planes already filled);
+        ``planes = (b, e)`` restricts it to the array planes [b, e) of
+        [1, nx_local + 1)."""
         need_cuda(phi, pi, phi_out, pi_out, names=["phi", "pi", "phi_out", "pi_out"])
         nxl, ny, nz = dims_of(phi)
         if (nxl, ny, nz) != self.local_shape:
             raise ValueError(f"local fields must be {self.local_shape}, got {(nxl, ny, nz)}")
+        b, e = planes if planes is not None else (1, self.nx_local + 1)
         sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
-        L.call("tipt_rk2_step_table_slab", storage_of(phi), ptr(phi), ptr(pi), ptr(phi_out),
-               ptr(pi_out), self.nx_local, ny, nz, self.i_lo, self.shape[0], sp, vsource,
-               stream_handle(stream))
+        L.call("tipt_rk2_step_table_slab_planes", storage_of(phi), ptr(phi), ptr(pi),
+               ptr(phi_out), ptr(pi_out), self.nx_local, ny, nz, self.i_lo, self.shape[0], int(b),
+               int(e), sp, vsource, stream_handle(stream))
 
     # ------------------------------------------------------ observables ---
     def observables(self, phi, pi=None, *, dx=1.0, inv_a2=1.0, lam=0.0, mphi=0.0, mu=1.0,

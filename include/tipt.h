@@ -48,8 +48,12 @@ enum { TIPT_F64 = 0, TIPT_F32 = 1, TIPT_F32C = 2 };
 enum {
     TIPT_VP_TABLE = 0,   /* 1-D uniform FP64 table: table[npts] */
     TIPT_VP_TABLE2D = 1, /* 2-D FP64 table [nT][npts]; rows blended at T, then lerped in phi */
-    TIPT_VP_POLY = 2     /* V'(x) = c1 x + c2 x^2 + c3 x^3 (zero-coupling inline V', R:2228) */
+    TIPT_VP_POLY = 2,    /* V'(x) = c1 x + c2 x^2 + c3 x^3 (zero-coupling inline V', R:2228) */
+    TIPT_VP_THERMAL = 3  /* the thermal one-loop V' evaluated per site at T (R:2201-2266
+                            _vprime_inline): `thermal` points to its couplings and splines */
 };
+
+struct tipt_thermal;
 
 typedef struct {
     int32_t kind;          /* TIPT_VP_* */
@@ -59,8 +63,9 @@ typedef struct {
     int32_t nT;            /* 2-D: rows along T (>= 2) */
     int32_t pad_;
     double T_min, T_dinv;  /* 2-D: T origin and 1/spacing */
-    double T;              /* 2-D: temperature at which rows are blended */
+    double T;              /* 2-D: temperature at which rows are blended; thermal: T */
     double c1, c2, c3;     /* polynomial coefficients */
+    const struct tipt_thermal* thermal; /* TIPT_VP_THERMAL: host pointer, read at the call */
 } tipt_vsource;
 
 /* Per-step scalars of the host loop (R:3674-3768): dt, dx, eta_eff, mu and
@@ -335,7 +340,7 @@ int tipt_complex_baoab_step_table(int storage, const void* phi1, const void* phi
  * cf dJ_F(u_f) du_f/dphi), u_b = sqrt(mB^2 + gb^2 phi^2 / 2 + (gb^2/4 + 2 gg^2/3) T^2) / T,
  * u_f = sqrt(gf^2 phi^2 / 2 + gfg^2 T^2 / 6) / T, dJ from cubic splines on a
  * uniform u grid. */
-typedef struct {
+typedef struct tipt_thermal {
     double lam, mphi, boson_mass_sq;
     double boson_coupling, boson_gauge_coupling, fermion_coupling, fermion_gauge_coupling;
     double coeff_b, coeff_f;  /* the reference's _POT_COEFFS */

@@ -72,3 +72,52 @@ def test_thermal_table_drives_the_stepper():
                        init_sigma=100.0, graph_steps=10)
     obs = sim.run(20)
     assert np.isfinite(obs).all() and obs[-1, 9] == 0
+
+
+# ------------------------------------------ rk2_fused_single_pass, thermal V' ---
+def _single_pass_run(g, tag, storage, policy=0):
+    from thermal_inflation_phase_transition_b200 import _lib as L
+    from thermal_inflation_phase_transition_b200 import real_field as RF
+    from thermal_inflation_phase_transition_b200.thermal import ThermalPotential
+    tp = ThermalPotential(splines=(g["cb"], g["cf"]), n_y=g["u"].size, ymax=float(g["u"][-1]),
+                          pot_coeffs=tuple(g["pot_coeffs"]))
+    phi = torch.from_numpy(g[f"{tag}_phi0"]).cuda()
+    pi = torch.from_numpy(g[f"{tag}_pi0"]).cuda()
+    if storage == "f32c":
+        phi, pi = RF.to_f32c(phi), RF.to_f32c(pi)
+    tmp = [torch.empty_like(phi), torch.empty_like(pi)]
+    keys = ("lam", "mphi", "bosonMassSquared", "bosonCoupling", "bosonGaugeCoupling",
+            "fermionCoupling", "fermionGaugeCoupling")
+    L.set_kernel_policy(policy)
+    try:
+        for n in range(5):
+            RF.rk2_fused_single_pass(phi, pi, float(g["dt"]), float(g["dx"]), float(g["eta"]),
+                                     float(g["T"]), float(g["T_mid"]), float(g["mu"]),
+                                     *[float(g[k]) for k in keys], float(g["ns"]), n, *tmp,
+                                     float(g["inv_a2"]), splines=tp)
+        torch.cuda.synchronize()
+    finally:
+        L.set_kernel_policy(0)
+    if storage == "f32c":
+        return RF.from_f32c(phi).cpu().numpy(), RF.from_f32c(pi).cpu().numpy(), phi, pi
+    return phi.cpu().numpy(), pi.cpu().numpy(), phi, pi
+
+
+@pytest.mark.parametrize("tag", ["3d", "odd"])
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_fused_single_pass_thermal_vs_reference(golden, tag, storage):
+    """rk2_fused_single_pass with the thermal inline V' (nonzero couplings, the
+    reference's dJ splines) against the reference kernel's five-step trajectory."""
+    g = golden("thermal_inline.npz")
+    phi, pi, _, _ = _single_pass_run(g, tag, storage)
+    tol = 1e-11 if storage == "f64" else 2e-6
+    for got, key in ((phi, f"{tag}_phi5"), (pi, f"{tag}_pi5")):
+        ref = g[key]
+        assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), (key, np.abs(got - ref).max())
+
+
+def test_fused_single_pass_thermal_marching_equals_generic(golden):
+    g = golden("thermal_inline.npz")
+    a = _single_pass_run(g, "3d", "f32c", policy=1)
+    b = _single_pass_run(g, "3d", "f32c", policy=0)
+    assert torch.equal(a[2], b[2]) and torch.equal(a[3], b[3])

@@ -23,3 +23,20 @@ def test_spline_reproduces_a_cubic_exactly():
 
 def test_counterterm_cut():
     assert abs(counterterm_x_cut(0.5, 2.0) - np.pi) < 1e-15
+
+
+def test_inline_vprime_oracle_matches_reference(golden):
+    """The oracle's restatement of _vprime_inline (R:2201-2266) against the reference
+    kernel's values at sample fields (both signs, the argument clamps, phi = 0) and
+    three temperatures."""
+    from oracle.thermal import vprime_inline
+    g = golden("thermal_inline.npz")
+    keys = ("lam", "mphi", "bosonMassSquared", "bosonCoupling", "bosonGaugeCoupling",
+            "fermionCoupling", "fermionGaugeCoupling")
+    kw = {k: float(g[k]) for k in keys}
+    u = g["u"]
+    for a, T in enumerate(g["Ts"]):
+        got = vprime_inline(g["phs"], float(T), g["cb"], g["cf"], float(u[0]),
+                            float(u[1] - u[0]), pot_coeffs=tuple(g["pot_coeffs"]), **kw)
+        want = g["vprime_inline"][a]
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())

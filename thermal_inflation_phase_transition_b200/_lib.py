@@ -12,7 +12,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libtipt.so")
 
 TIPT_F64, TIPT_F32, TIPT_F32C = 0, 1, 2
-VP_TABLE, VP_TABLE2D, VP_POLY = 0, 1, 2
+VP_TABLE, VP_TABLE2D, VP_POLY, VP_THERMAL = 0, 1, 2, 3
 K_PASS2 = 73856093
 K_PASS4 = 19349669
 
@@ -27,7 +27,8 @@ class VSource(C.Structure):
     _fields_ = [("kind", C.c_int32), ("npts", C.c_int32), ("table", C.c_void_p),
                 ("tmin", C.c_double), ("dinv", C.c_double), ("nT", C.c_int32),
                 ("pad_", C.c_int32), ("T_min", C.c_double), ("T_dinv", C.c_double),
-                ("T", C.c_double), ("c1", C.c_double), ("c2", C.c_double), ("c3", C.c_double)]
+                ("T", C.c_double), ("c1", C.c_double), ("c2", C.c_double), ("c3", C.c_double),
+                ("thermal", C.c_void_p)]
 
 
 class StepParams(C.Structure):

@@ -66,6 +66,15 @@ bool overlap(const void* a, const void* b, int64_t n) {
 int check_vsource(const tipt_vsource* vp, const char* name) {
     if (!vp) return fail(TIPT_ERR_ARG, "%s is NULL", name);
     if (vp->kind == TIPT_VP_POLY) return TIPT_OK;
+    if (vp->kind == TIPT_VP_THERMAL) {
+        const tipt_thermal* t = vp->thermal;
+        if (!t) return fail(TIPT_ERR_ARG, "%s: thermal parameters are NULL", name);
+        if (t->nseg < 1 || !(t->h > 0.0)) return fail(TIPT_ERR_ARG, "%s: bad spline grid", name);
+        if (!t->spline || reinterpret_cast<uintptr_t>(t->spline) % 8)
+            return fail(TIPT_ERR_ALIGN, "%s: spline is NULL or misaligned", name);
+        if (!(vp->T > 0.0)) return fail(TIPT_ERR_ARG, "%s: T must be > 0", name);
+        return TIPT_OK;
+    }
     if (vp->kind != TIPT_VP_TABLE && vp->kind != TIPT_VP_TABLE2D)
         return fail(TIPT_ERR_ARG, "%s: unknown V' source kind %d", name, vp->kind);
     if (!vp->table) return fail(TIPT_ERR_ARG, "%s: table is NULL", name);
@@ -89,6 +98,7 @@ static void fill_vsource(RealStageParams& p, const tipt_vsource* vp) {
     p.c2 = vp->c2;
     p.c3 = vp->c3;
     p.table_in_smem = 0;
+    if (vp->kind == TIPT_VP_THERMAL) p.th = thermal_site(*vp->thermal, vp->T);
 }
 
 static RealStageParams stage_params(const void* phi, const void* pi, void* phi_out,
@@ -250,6 +260,8 @@ int tipt_rk2_step_table_sched(int storage, const void* phi, const void* pi, void
     if ((rc = check_state(storage, phi, pi, phi_out, pi_out, nx, ny, nz))) return rc;
     if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
     if ((rc = check_vsource(vp, "vp"))) return rc;
+    if (vp->kind == TIPT_VP_THERMAL)
+        return fail(TIPT_ERR_UNSUPPORTED, "scheduled steps take a table or a polynomial V'");
     if ((rc = check_ptr(sched, 8, "sched")) || (rc = check_ptr(counter, 8, "counter"))) return rc;
     if (sched_len < 1 || offset < 0) return fail(TIPT_ERR_ARG, "bad schedule length or offset");
     RealStageParams p = stage_params(phi, pi, phi_out, pi_out, nx, ny, nz, sp, vp);

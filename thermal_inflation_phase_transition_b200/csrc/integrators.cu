@@ -337,7 +337,7 @@ static int alt_setup(int storage, const void* const* in, int n_in, void* const* 
     }
     if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
     if ((rc = check_vsource(vp, "vp"))) return rc;
-    if (vp->kind == TIPT_VP_TABLE2D)
+    if (vp->kind == TIPT_VP_TABLE2D || vp->kind == TIPT_VP_THERMAL)
         return fail(TIPT_ERR_UNSUPPORTED, "these integrators take a 1-D V' table or a polynomial");
     if (!(sp->dt > 0.0) || !(sp->eta_eff > 0.0))
         return fail(TIPT_ERR_ARG, "dt and eta_eff (gamma) must be > 0");

@@ -243,6 +243,8 @@ extern "C" int tipt_complex_rk2_step_table(int storage, const void* phi1, const 
     }
     if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
     if ((rc = check_vsource(vp, "vp"))) return rc;
+    if (vp->kind == TIPT_VP_THERMAL)
+        return fail(TIPT_ERR_UNSUPPORTED, "the complex field takes a V'(rho) table or a polynomial");
     if (vp->kind == TIPT_VP_TABLE2D)
         return fail(TIPT_ERR_UNSUPPORTED, "complex field takes a 1-D V'(rho) table");
     if ((noise1 == nullptr) != (noise2 == nullptr))

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
 
 // Bytes of shared memory the V' row needs for storage S (0 if polynomial).
 static int64_t table_smem_bytes(int S, const RealStageParams& p) {
-    if (p.vkind == TIPT_VP_POLY) return 0;
+    if (p.vkind == TIPT_VP_POLY || p.vkind == TIPT_VP_THERMAL) return 0;
     return (int64_t)p.npts * (S == TIPT_F32C ? 4 : 8);
 }
 

@@ -9,6 +9,7 @@
 // reference passes fuse into one launch with a radius-1 halo and no scratch.
 #pragma once
 
+#include "thermal_inline.cuh"
 #include "tipt_device.cuh"
 
 namespace tipt {
@@ -53,6 +54,7 @@ struct RealStageParams {
     // site_offset (a slab of a larger lattice keys by the global index).
     int i_begin, i_end;
     long long site_offset;
+    ThermalSite th;  // TIPT_VP_THERMAL: the inline thermal V' at T
 };
 
 // Resolve the per-step scalars of a scheduled launch (no-op otherwise).
@@ -102,6 +104,7 @@ __device__ __forceinline__ void stage_table(const RealStageParams& p, TT* s_tab)
 // V'(x) in FP64 from the staged row, the global 1-D table, or the polynomial.
 __device__ __forceinline__ double vprime_d(const RealStageParams& p, const double* s_tab, double x) {
     if (p.vkind == TIPT_VP_POLY) return poly_vprime<double>(p.c1, p.c2, p.c3, x);
+    if (p.vkind == TIPT_VP_THERMAL) return thermal_vprime_inline(p.th, x);
     const double* t = p.table_in_smem ? s_tab : p.table;
     return lerp_table<double>(t, p.tmin, p.dinv, p.npts - 2, x);
 }
@@ -171,6 +174,13 @@ __device__ __forceinline__ V vprime_v(const RealStageParams& p, const F32CConst&
     if (p.vkind == TIPT_VP_POLY) {
         const V d = v_fma(v_mul(v_mul(kvec<V>(p.k2.c3), x), x), x, v_mul(kvec<V>(p.k2.c1), x));
         return p.c2 != 0.0 ? v_fma(v_mul(kvec<V>(p.k2.c2), x), x, d) : d;
+    }
+    if (p.vkind == TIPT_VP_THERMAL) {  // FP64 per lane from the FP32 value
+        V r;
+#pragma unroll
+        for (int l = 0; l < NL; ++l)
+            vset(r, l, (float)thermal_vprime_inline(p.th, (double)vlane(x, l)));
+        return r;
     }
     if (!p.table_in_smem) {
         V r;

@@ -119,24 +119,32 @@ def rk2_fused_table(phi, pi, dt, dx, eta_eff, mu, noise, phi_tmp, pi_tmp, inv_a2
 def rk2_fused_single_pass(phi, pi, dt, dx, eta_eff, T, T_mid, mu, lam, mphi, bosonMassSquared,
                           bosonCoupling, bosonGaugeCoupling, fermionCoupling,
                           fermionGaugeCoupling, noise_scale, noise_seed, phi_tmp, pi_tmp,
-                          inv_a2, *, seed=0):
+                          inv_a2, *, seed=0, splines=None):
     """R:2339 rk2_fused_single_pass: 4-pass RK2 with inline V' and inline hash noise.
 
     ``noise_seed`` is the reference's name for the step counter (R:3742).  The
-    inline V' here covers zero thermal couplings, where R:2228 reduces it to
-    lam*phi^3 - mphi^2*phi; the thermal dJ spline terms are not built yet."""
-    if any(float(c) != 0.0 for c in (bosonCoupling, bosonGaugeCoupling, fermionCoupling,
-                                     fermionGaugeCoupling)):
-        raise NotImplementedError("inline thermal dJ terms (nonzero couplings) are not built; "
-                                  "tabulate V' and use rk2_fused_table")
+    inline V' is the reference's _vprime_inline (R:2201-2266) evaluated per site at T
+    in the first half and T_mid in the second; its dJ splines are those of
+    ``splines`` (a thermal.ThermalPotential), by default the reference script's
+    module-level splines (thermal.default_potential).  With all four couplings zero
+    it reduces to lam phi^3 - mphi^2 phi (R:2228), evaluated as a polynomial."""
     st = storage_of(phi)
     need_cuda(phi, pi, phi_tmp, pi_tmp, names=["phi", "pi", "phi_tmp", "pi_tmp"])
     same_layout(phi, pi, phi_tmp, pi_tmp, names=["pi", "phi_tmp", "pi_tmp"])
     nx, ny, nz = dims_of(phi)
-    v = poly_source(-float(mphi) * float(mphi), 0.0, float(lam))
     sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_seed, seed)
+    if all(float(c) == 0.0 for c in (bosonCoupling, bosonGaugeCoupling, fermionCoupling,
+                                     fermionGaugeCoupling)) and splines is None:
+        va = vb = poly_source(-float(mphi) * float(mphi), 0.0, float(lam))
+    else:
+        from .thermal import default_potential
+        tp = splines if splines is not None else default_potential(phi.device)
+        kw = dict(lam=lam, mphi=mphi, bosonMassSquared=bosonMassSquared,
+                  bosonCoupling=bosonCoupling, bosonGaugeCoupling=bosonGaugeCoupling,
+                  fermionCoupling=fermionCoupling, fermionGaugeCoupling=fermionGaugeCoupling)
+        va, vb = tp.source(T, **kw), tp.source(T_mid, **kw)
     L.call("tipt_rk2_fused_table", st, ptr(phi), ptr(pi), ptr(phi), ptr(pi), ptr(phi_tmp),
-           ptr(pi_tmp), nx, ny, nz, sp, v, v, None, stream_handle())
+           ptr(pi_tmp), nx, ny, nz, sp, va, vb, None, stream_handle())
 
 
 def _vsource_1d(vp_table, vp_tmin, vp_dinv, vp_npts, vpoly):

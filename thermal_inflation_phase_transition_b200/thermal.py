@@ -14,6 +14,7 @@ the table runs.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import numpy as np
@@ -22,7 +23,8 @@ import torch
 from . import _lib as L
 from ._common import dims_of, need_cuda, ptr, storage_of, stream_handle
 
-__all__ = ["dj_grid", "not_a_knot_spline", "ThermalPotential", "counterterm_x_cut"]
+__all__ = ["dj_grid", "not_a_knot_spline", "ThermalPotential", "counterterm_x_cut",
+           "default_potential"]
 
 YMAX = 100.0
 N_Y = 256
@@ -104,6 +106,24 @@ class ThermalPotential:
                                 float(pot_coeffs[1]), float(self.u[0]),
                                 float(self.u[1] - self.u[0]), n_y - 1, 0, self._spl.data_ptr())
 
+    def source(self, T, *, lam=None, mphi=None, bosonMassSquared=None, bosonCoupling=None,
+               bosonGaugeCoupling=None, fermionCoupling=None, fermionGaugeCoupling=None):
+        """V' source of the steppers that evaluates this potential per site at T, as the
+        reference's inline V' (R:2201-2266 _vprime_inline); couplings default to this
+        object's.  The returned structure keeps its parameters alive."""
+        q = self.params
+        pick = lambda v, d: float(d if v is None else v)  # noqa: E731
+        th = L.Thermal(pick(lam, q.lam), pick(mphi, q.mphi), pick(bosonMassSquared, q.boson_mass_sq),
+                       pick(bosonCoupling, q.boson_coupling),
+                       pick(bosonGaugeCoupling, q.boson_gauge_coupling),
+                       pick(fermionCoupling, q.fermion_coupling),
+                       pick(fermionGaugeCoupling, q.fermion_gauge_coupling), q.coeff_b, q.coeff_f,
+                       q.x_min, q.h, q.nseg, 0, self._spl.data_ptr())
+        vs = L.VSource(L.VP_THERMAL, 0, None, 0.0, 0.0, 0, 0, 0.0, 0.0, float(T), 0.0, 0.0, 0.0,
+                       C.addressof(th))
+        vs._keep = (th, self._spl)
+        return vs
+
     def vprime_field(self, phi, T, out=None):
         """R:1435 Vprime_field(out, phi, T, ...): V' per site (FP64; into ``out`` with
         phi's dtype when given, as the reference's out array)."""
@@ -137,3 +157,16 @@ class ThermalPotential:
         return Table2D(np.ascontiguousarray(v), float(phi_lo),
                        1.0 / ((phi_hi - phi_lo) / (nphi - 1)), float(T_lo),
                        1.0 / ((T_hi - T_lo) / (nT - 1)))
+
+
+_DEFAULT = {}
+
+
+def default_potential(device="cuda"):
+    """The reference script's module-level splines (R:432-455: dJ_B, dJ_F on the
+    256-point grid, no counterterm), built once per device on the GPU."""
+    dev = torch.device(device)
+    key = (dev.type, dev.index if dev.index is not None else torch.cuda.current_device())
+    if key not in _DEFAULT:
+        _DEFAULT[key] = ThermalPotential(device=dev)
+    return _DEFAULT[key]

@@ -10,7 +10,9 @@ h_y, inv_hy, xhi_clamp, nseg) of the AST-extracted real-field kernels, which
 are run unmodified:
 * ``_vprime_inline`` (R:2201-2266) at sample fields and temperatures;
 * five steps of ``rk2_fused_single_pass`` (R:2339-2647) with the script's
-  default couplings (R:642-643, R:744-748) on two lattices.
+  default couplings (R:642-643, R:744-748) on two lattices;
+* five steps of ``rk2_step_inline`` (R:2654-2822) on the same lattices, its noise
+  array filled with the reference's hash and Box-Muller (make_golden.noise).
 """
 from __future__ import annotations
 
@@ -22,6 +24,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
+import make_golden  # noqa: E402
 import ref_extract  # noqa: E402
 
 
@@ -70,6 +73,17 @@ def main():
                                        c["fermionGaugeCoupling"], ns, np.uint64(n),
                                        np.empty_like(phi), np.empty_like(pi), inv_a2)
         out[f"{tag}_phi5"], out[f"{tag}_pi5"] = phi, pi
+        # rk2_step_inline from the same initial state, noise array at the pass-2 multiplier
+        phi, pi = out[f"{tag}_phi0"].copy(), out[f"{tag}_pi0"].copy()
+        for n in range(5):
+            nf = make_golden.noise(shape, n, make_golden.K_PASS2, ns)
+            out[f"{tag}_noise{n}"] = nf
+            R["rk2_step_inline"](phi, pi, dt, dx, eta, T, mu, c["lam"], c["mphi"],
+                                 c["bosonMassSquared"], c["bosonCoupling"],
+                                 c["bosonGaugeCoupling"], c["fermionCoupling"],
+                                 c["fermionGaugeCoupling"], nf, np.empty_like(phi),
+                                 np.empty_like(pi), inv_a2)
+        out[f"{tag}_inline_phi5"], out[f"{tag}_inline_pi5"] = phi, pi
     np.savez_compressed(os.path.join(HERE, "thermal_inline.npz"), u=u, cb=cb, cf=cf,
                         pot_coeffs=np.array(pot), phs=phs, Ts=Ts, vprime_inline=vin, dt=dt,
                         dx=dx, eta=eta, mu=mu, inv_a2=inv_a2, T=T, T_mid=Tm, ns=ns,

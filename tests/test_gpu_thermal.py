@@ -121,3 +121,35 @@ def test_fused_single_pass_thermal_marching_equals_generic(golden):
     a = _single_pass_run(g, "3d", "f32c", policy=1)
     b = _single_pass_run(g, "3d", "f32c", policy=0)
     assert torch.equal(a[2], b[2]) and torch.equal(a[3], b[3])
+
+
+@pytest.mark.parametrize("tag", ["3d", "odd"])
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_step_inline_thermal_vs_reference(golden, tag, storage):
+    """rk2_step_inline (R:2654-2822: the midpoint step with the thermal V' inline),
+    driven by the reference's noise arrays, against the reference kernel."""
+    from thermal_inflation_phase_transition_b200 import real_field as RF
+    from thermal_inflation_phase_transition_b200.thermal import ThermalPotential
+    g = golden("thermal_inline.npz")
+    tp = ThermalPotential(splines=(g["cb"], g["cf"]), n_y=g["u"].size, ymax=float(g["u"][-1]),
+                          pot_coeffs=tuple(g["pot_coeffs"]))
+    phi = torch.from_numpy(g[f"{tag}_phi0"]).cuda()
+    pi = torch.from_numpy(g[f"{tag}_pi0"]).cuda()
+    if storage == "f32c":
+        phi, pi = RF.to_f32c(phi), RF.to_f32c(pi)
+    tmp = [torch.empty_like(phi), torch.empty_like(pi)]
+    keys = ("lam", "mphi", "bosonMassSquared", "bosonCoupling", "bosonGaugeCoupling",
+            "fermionCoupling", "fermionGaugeCoupling")
+    for n in range(5):
+        RF.rk2_step_inline(phi, pi, float(g["dt"]), float(g["dx"]), float(g["eta"]),
+                           float(g["T"]), float(g["mu"]), *[float(g[k]) for k in keys],
+                           torch.from_numpy(g[f"{tag}_noise{n}"]).cuda(), *tmp,
+                           float(g["inv_a2"]), splines=tp)
+    torch.cuda.synchronize()
+    if storage == "f32c":
+        phi, pi = RF.from_f32c(phi), RF.from_f32c(pi)
+    tol = 1e-11 if storage == "f64" else 2e-6
+    for got, key in ((phi, f"{tag}_inline_phi5"), (pi, f"{tag}_inline_pi5")):
+        ref = g[key]
+        got = got.cpu().numpy()
+        assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), (key, np.abs(got - ref).max())

@@ -83,6 +83,32 @@ def rk2_step_table(phi, pi, dt, dx, eta_eff, mu, noise, phi_tmp, pi_tmp, inv_a2,
     swap_storage(pi, pi_tmp)
 
 
+def rk2_step_inline(phi, pi, dt, dx, eta_eff, T, mu, lam_val, mphi_val, bosonMassSquared,
+                    bosonCoupling, bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling,
+                    noise, phi_tmp, pi_tmp, inv_a2, *, splines=None, noise_scale=0.0,
+                    noise_step=0, seed=0):
+    """R:2654 rk2_step_inline: rk2_step_table's midpoint step with the thermal V'
+    evaluated inline per site at T (R:2201-2266 _vprime_inline) instead of a table;
+    phi and pi are updated in place.  ``noise`` is the reference's noise array (or
+    None for inline hash noise with the keywords); the dJ splines come from
+    ``splines`` (a thermal.ThermalPotential), by default the reference script's."""
+    from .thermal import default_potential
+    st = storage_of(phi)
+    need_cuda(phi, pi, phi_tmp, pi_tmp, names=["phi", "pi", "phi_tmp", "pi_tmp"])
+    same_layout(phi, pi, phi_tmp, pi_tmp, names=["pi", "phi_tmp", "pi_tmp"])
+    _noise_check(noise, phi, st)
+    nx, ny, nz = dims_of(phi)
+    tp = splines if splines is not None else default_potential(phi.device)
+    vs = tp.source(T, lam=lam_val, mphi=mphi_val, bosonMassSquared=bosonMassSquared,
+                   bosonCoupling=bosonCoupling, bosonGaugeCoupling=bosonGaugeCoupling,
+                   fermionCoupling=fermionCoupling, fermionGaugeCoupling=fermionGaugeCoupling)
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
+    L.call("tipt_rk2_step_table", st, ptr(phi), ptr(pi), ptr(phi_tmp), ptr(pi_tmp), nx, ny, nz,
+           sp, vs, ptr(noise), stream_handle())
+    swap_storage(phi, phi_tmp)
+    swap_storage(pi, pi_tmp)
+
+
 def rk2_step_table_into(phi, pi, phi_out, pi_out, dt, dx, eta_eff, mu, inv_a2, vsource, *,
                         noise=None, noise_scale=0.0, noise_step=0, seed=0, stream=None):
     """Ping-pong form of rk2_step_table: (phi, pi) -> (phi_out, pi_out), no swap.

@@ -209,6 +209,21 @@ int tipt_complex_rk2_step_table(int storage, const void* phi1, const void* phi2,
                                 const tipt_vsource* vp, const tipt_complex_terms* ct,
                                 const void* noise1, const void* noise2, void* stream);
 
+/* Complex rk2_fused_table (C:1789-2064): two dt/2 midpoint halves, the first
+ * with vp_T, the second with vp_Tm; array noise adds 0.5*noise_a in each half.
+ * With noise1 == noise2 == NULL the halves use the inline hash pairs of the
+ * complex rk2_fused_single_pass (C:2765-3132): 0.5*ns*(z1, z2) at multiplier
+ * 73856093, then 19349669.  vp_T / vp_Tm may be TIPT_VP_THERMAL (the inline
+ * V'(rho) of C:2605-2680).  mid1..mid4 hold the state between the halves (the
+ * reference's phi1_tmp .. pi2_tmp); the outputs may be the inputs. */
+int tipt_complex_rk2_fused_table(int storage, const void* phi1, const void* phi2,
+                                 const void* pi1, const void* pi2, void* phi1_out,
+                                 void* phi2_out, void* pi1_out, void* pi2_out, void* mid1,
+                                 void* mid2, void* mid3, void* mid4, int64_t nx, int64_t ny,
+                                 int64_t nz, const tipt_step_params* sp, const tipt_vsource* vp_T,
+                                 const tipt_vsource* vp_Tm, const tipt_complex_terms* ct,
+                                 const void* noise1, const void* noise2, void* stream);
+
 /* compute_winding_number (C:2683-2744; tools/winding.py:15-64) on the FP64
  * value of the stored fields (the reference casts to FP64, C:4627-4629).
  * Outputs (each may be NULL):

@@ -40,3 +40,72 @@ def test_inline_vprime_oracle_matches_reference(golden):
                             float(u[1] - u[0]), pot_coeffs=tuple(g["pot_coeffs"]), **kw)
         want = g["vprime_inline"][a]
         np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
+
+
+_COUPLINGS = ("lam", "mphi", "bosonMassSquared", "bosonCoupling", "bosonGaugeCoupling",
+              "fermionCoupling", "fermionGaugeCoupling")
+
+
+def _state(g, key, n):
+    return [g[f"{key}_{f}_{n}"].copy() for f in ("phi1", "phi2", "pi1", "pi2")]
+
+
+def _close(got, g, key, suffix, rtol):
+    for a, f in zip(got, ("phi1", "phi2", "pi1", "pi2")):
+        want = g[f"{key}_{f}{suffix}"]
+        assert np.abs(a - want).max() <= rtol * np.abs(want).max(), (key, f)
+
+
+def test_complex_fused_table_oracle_matches_reference(golden):
+    """oracle.complex_steps.rk2_fused_table against five steps of the reference's
+    complex rk2_fused_table (C:1789-2064), U(1) and Z_4, noise arrays."""
+    from oracle import oracle as O
+    from oracle.complex_steps import rk2_fused_table
+    g = golden("complex_thermal.npz")
+    p = {k: g[f"ft_{k}"] for k in ("dt", "dx", "eta", "mu", "inv_a2", "ns")}
+    tabs = [g[f"ft_{k}"] for k in ("table_T", "tmin_T", "dinv_T", "npts_T", "table_Tm", "tmin_Tm",
+                                  "dinv_Tm", "npts_Tm")]
+    tabs = [t if t.ndim else t.item() for t in tabs]
+    for zn_tag, zn in (("u1", (0.0, 0.0, 0.0)), ("z4", tuple(g["ft_zn_z4"]))):
+        for tag in ("3d", "odd"):
+            key = f"ft_{zn_tag}_{tag}"
+            s = _state(g, key, 0)
+            shape = s[0].shape
+            for n in range(5):
+                n1 = O.noise_field(shape, n, O.K_PASS2, 0, float(p["ns"]), 0)
+                n2 = O.noise_field(shape, n, O.K_PASS2, 0, float(p["ns"]), 1)
+                rk2_fused_table(s, float(p["dt"]), float(p["dx"]), float(p["eta"]), float(p["mu"]),
+                                n1, n2, float(p["inv_a2"]), *tabs, zn=zn)
+            _close(s, g, key, "_5", 1e-12)
+
+
+def test_complex_thermal_oracle_matches_reference(golden):
+    """oracle.complex_steps rk2_fused_single_pass / rk2_step_inline against five
+    steps of the reference's complex kernels (C:2765-3132, C:3140-) with the
+    inline thermal V'(rho) and the complex script's pot_coeffs (2, -1)."""
+    from oracle import oracle as O
+    from oracle.complex_steps import rk2_fused_single_pass, rk2_step_inline
+    g = golden("complex_thermal.npz")
+    th = golden("thermal.npz")
+    u, cb, cf = th["u"], th["cb"], th["cf"]
+    x_min, h = float(u[0]), float(u[1] - u[0])
+    c = {k: float(g[f"th_{k}"]) for k in _COUPLINGS}
+    pot = tuple(g["th_pot_coeffs"])
+    dt, dx, eta, mu, inv_a2, T, Tm, ns = (float(g[f"th_{k}"]) for k in
+                                          ("dt", "dx", "eta", "mu", "inv_a2", "T", "T_mid", "ns"))
+    for tag in ("3d", "odd"):
+        key = f"th_{tag}"
+        s = _state(g, key, 0)
+        for n in range(5):
+            rk2_fused_single_pass(s, dt, dx, eta, T, Tm, mu, c, ns, n, inv_a2, cb, cf, x_min, h,
+                                  pot)
+        _close(s, g, key, "_5", 1e-12)
+        s = _state(g, key, 0)
+        shape = s[0].shape
+        for n in range(5):
+            n1 = O.noise_field(shape, n, O.K_PASS2, 0, ns, 0)
+            n2 = O.noise_field(shape, n, O.K_PASS2, 0, ns, 1)
+            rk2_step_inline(s, dt, dx, eta, T, mu, c, n1, n2, inv_a2, cb, cf, x_min, h, pot)
+        for a, f in zip(s, ("phi1", "phi2", "pi1", "pi2")):
+            want = g[f"{key}_inline_{f}_5"]
+            assert np.abs(a - want).max() <= 1e-12 * np.abs(want).max(), (key, f)

@@ -93,6 +93,9 @@ _SIGS = {
     "tipt_complex_rk2_step_table": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
                                     C.POINTER(StepParams), C.POINTER(VSource),
                                     C.POINTER(ComplexTerms), _p, _p, _p],
+    "tipt_complex_rk2_fused_table": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64,
+                                     _i64, _i64, C.POINTER(StepParams), C.POINTER(VSource),
+                                     C.POINTER(VSource), C.POINTER(ComplexTerms), _p, _p, _p],
     "tipt_compute_winding_number": [_i, _p, _p, _i64, _i64, _i64, _p, _p, _p, _i64, _p, _p],
     "tipt_observables_workspace_size": [_i64, _i64, _i64],
     "tipt_observables": [_i, _p, _p, _i64, _i64, _i64, _d, _d, _d, _d, _d, _d, _p, _p, _i64,

@@ -47,6 +47,99 @@ def rk2_step_table(phi1, phi2, pi1, pi2, dt, dx, eta_eff, mu, noise1, noise2, ph
         swap_storage(a, b)
 
 
+def _check_noise_pair(noise1, noise2, st, phi1):
+    if (noise1 is None) != (noise2 is None):
+        raise ValueError("give both noise1 and noise2, or neither")
+    if noise1 is not None:
+        need_cuda(noise1, noise2, names=["noise1", "noise2"])
+        want = torch.float32 if st == L.TIPT_F32 else torch.float64
+        for n in (noise1, noise2):
+            if n.dtype != want or tuple(n.shape) != dims_of(phi1):
+                raise ValueError(f"noise arrays must be {want} with shape {dims_of(phi1)}")
+
+
+def _fused(state, tmp, dt, dx, eta_eff, mu, inv_a2, va, vb, zn, eps4, noise1, noise2,
+           noise_scale, noise_step, seed):
+    """Two dt/2 halves in place: state -> tmp (first half) -> state (second half)."""
+    st = storage_of(state[0])
+    names = ("phi1", "phi2", "pi1", "pi2", "phi1_tmp", "phi2_tmp", "pi1_tmp", "pi2_tmp")
+    need_cuda(*state, *tmp, names=names)
+    same_layout(state[0], *state[1:], *tmp, names=names[1:])
+    _check_noise_pair(noise1, noise2, st, state[0])
+    nx, ny, nz = dims_of(state[0])
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
+    ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
+    L.call("tipt_complex_rk2_fused_table", st, *[ptr(a) for a in state],
+           *[ptr(a) for a in state], *[ptr(a) for a in tmp], nx, ny, nz, sp, va, vb, ct,
+           ptr(noise1), ptr(noise2), stream_handle())
+
+
+def rk2_fused_table(phi1, phi2, pi1, pi2, dt, dx, eta_eff, mu, noise1, noise2, phi1_tmp,
+                    phi2_tmp, pi1_tmp, pi2_tmp, inv_a2, vp_table_T, vp_tmin_T, vp_dinv_T,
+                    vp_npts_T, vp_table_Tm, vp_tmin_Tm, vp_dinv_Tm, vp_npts_Tm, *,
+                    zn=(0.0, 0.0, 0.0), eps4=0.0, noise_scale=0.0, noise_step=0, seed=0):
+    """C:1789 rk2_fused_table (complex): two dt/2 halves with the V'(rho) tables at T
+    and T_mid, 0.5*noise in each half, in place; noise1 = noise2 = None selects the
+    inline hash pairs (keywords)."""
+    va = table_source(vp_table_T, vp_tmin_T, vp_dinv_T, vp_npts_T)
+    vb = table_source(vp_table_Tm, vp_tmin_Tm, vp_dinv_Tm, vp_npts_Tm)
+    _fused((phi1, phi2, pi1, pi2), (phi1_tmp, phi2_tmp, pi1_tmp, pi2_tmp), dt, dx, eta_eff, mu,
+           inv_a2, va, vb, zn, eps4, noise1, noise2, noise_scale, noise_step, seed)
+
+
+def _thermal_kw(lam, mphi, bosonMassSquared, bosonCoupling, bosonGaugeCoupling, fermionCoupling,
+                fermionGaugeCoupling):
+    return dict(lam=lam, mphi=mphi, bosonMassSquared=bosonMassSquared,
+                bosonCoupling=bosonCoupling, bosonGaugeCoupling=bosonGaugeCoupling,
+                fermionCoupling=fermionCoupling, fermionGaugeCoupling=fermionGaugeCoupling)
+
+
+def rk2_fused_single_pass(phi1, phi2, pi1, pi2, dt, dx, eta_eff, T, T_mid, mu, lam, mphi,
+                          bosonMassSquared, bosonCoupling, bosonGaugeCoupling, fermionCoupling,
+                          fermionGaugeCoupling, noise_scale, noise_seed, phi1_tmp, phi2_tmp,
+                          pi1_tmp, pi2_tmp, inv_a2, *, zn=(0.0, 0.0, 0.0), eps4=0.0,
+                          splines=None, seed=0):
+    """C:2765 rk2_fused_single_pass (complex): two dt/2 halves with the inline V'(rho)
+    (C:2605-2680 _vprime_complex_inline) at T, then T_mid, and one inline hash pair per
+    site per half (multipliers 73856093, 19349669; ``noise_seed`` is the step counter),
+    in place.  The dJ splines come from ``splines`` (a thermal.ThermalPotential), by
+    default the complex script's (its _POT_COEFFS = (2, -1), C:215)."""
+    from .thermal import default_potential
+    tp = splines if splines is not None else default_potential(phi1.device, (2.0, -1.0))
+    kw = _thermal_kw(lam, mphi, bosonMassSquared, bosonCoupling, bosonGaugeCoupling,
+                     fermionCoupling, fermionGaugeCoupling)
+    _fused((phi1, phi2, pi1, pi2), (phi1_tmp, phi2_tmp, pi1_tmp, pi2_tmp), dt, dx, eta_eff, mu,
+           inv_a2, tp.source(T, **kw), tp.source(T_mid, **kw), zn, eps4, None, None,
+           noise_scale, noise_seed, seed)
+
+
+def rk2_step_inline(phi1, phi2, pi1, pi2, dt, dx, eta_eff, T, mu, lam_val, mphi_val,
+                    bosonMassSquared, bosonCoupling, bosonGaugeCoupling, fermionCoupling,
+                    fermionGaugeCoupling, noise1, noise2, phi1_tmp, phi2_tmp, pi1_tmp, pi2_tmp,
+                    inv_a2, *, zn=(0.0, 0.0, 0.0), eps4=0.0, splines=None, noise_scale=0.0,
+                    noise_step=0, seed=0):
+    """C:3140 rk2_step_inline (complex): rk2_step_table's midpoint step with the inline
+    V'(rho) at T, in place (storage exchange with the *_tmp tensors); noise arrays as
+    the reference passes them, or None for the inline hash pair (keywords)."""
+    from .thermal import default_potential
+    st = storage_of(phi1)
+    arrs = (phi1, phi2, pi1, pi2, phi1_tmp, phi2_tmp, pi1_tmp, pi2_tmp)
+    names = ("phi1", "phi2", "pi1", "pi2", "phi1_tmp", "phi2_tmp", "pi1_tmp", "pi2_tmp")
+    need_cuda(*arrs, names=names)
+    same_layout(phi1, *arrs[1:], names=names[1:])
+    _check_noise_pair(noise1, noise2, st, phi1)
+    tp = splines if splines is not None else default_potential(phi1.device, (2.0, -1.0))
+    vs = tp.source(T, **_thermal_kw(lam_val, mphi_val, bosonMassSquared, bosonCoupling,
+                                    bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling))
+    nx, ny, nz = dims_of(phi1)
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
+    ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
+    L.call("tipt_complex_rk2_step_table", st, *[ptr(a) for a in arrs], nx, ny, nz, sp, vs, ct,
+           ptr(noise1), ptr(noise2), stream_handle())
+    for a, b in ((phi1, phi1_tmp), (phi2, phi2_tmp), (pi1, pi1_tmp), (pi2, pi2_tmp)):
+        swap_storage(a, b)
+
+
 def rk2_step_table_into(state, out, dt, dx, eta_eff, mu, inv_a2, vsource, *, zn=(0.0, 0.0, 0.0),
                         eps4=0.0, noise_scale=0.0, noise_step=0, seed=0, stream=None):
     """Ping-pong form: state=(phi1, phi2, pi1, pi2) -> out=(phi1', phi2', pi1', pi2')."""

@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
                     x.pih = cen[2];
                     x.pil = cen[3];
                     float2 a, b, cc, d;
-                    update_f32c<float2>(p, kc, nullptr, x, site_kick_f32c2(p, kc, (uint64_t)s), a, b,
+                    update_f32c<float2, false>(p, kc, nullptr, x, site_kick_f32c2(p, kc, (uint64_t)s), a, b,
                                         cc, d);
                     *reinterpret_cast<float2*>(po + g) = a;
                     *reinterpret_cast<float2*>(po + N + g) = b;
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
                     pv[u] = __ldg(pi + idx[u]);
                 }
                 double a, b;
-                update_f64(p, nullptr, ph, pv, site_noise<double>(p, (uint64_t)s), a, b);
+                update_f64<false>(p, nullptr, ph, pv, site_noise<double>(p, (uint64_t)s), a, b);
                 static_cast<double*>(e.phi_out)[g] = a;
                 static_cast<double*>(e.pi_out)[g] = b;
             } else {
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
                 x.pih = vh[0];
                 x.pil = vl[0];
                 float a, b, cc, d;
-                update_f32c<float>(p, kc, nullptr, x, site_kick_f32c(p, kc, (uint64_t)s), a, b,
+                update_f32c<float, false>(p, kc, nullptr, x, site_kick_f32c(p, kc, (uint64_t)s), a, b,
                                    cc, d);
                 float* po = static_cast<float*>(e.phi_out);
                 float* vo = static_cast<float*>(e.pi_out);

@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(256) alt_complex_kernel(AltParams p) {
                 c[a] = (double)q[0];
             }
             double d1, d2;
-            complex_force<double>(p.v, dtab, p.v.tmin, p.v.dinv, c[0], c[1], d1, d2);
+            complex_force<double, false>(p.v, dtab, p.v.tmin, p.v.dinv, c[0], c[1], d1, d2);
             const double F[2] = {force_d(p, lap[0], d1), force_d(p, lap[1], d2)};
             double z[2] = {0.0, 0.0};
             if (noisy) gauss_pair(key, z[0], z[1]);
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(256) alt_complex_kernel(AltParams p) {
                                        __fadd_rn(ch[0], cl[0]), __fadd_rn(ch[1], cl[1]), d1, d2);
             } else {
                 double e1, e2;
-                complex_force<double>(p.v, p.v.table, p.v.tmin, p.v.dinv,
+                complex_force<double, false>(p.v, p.v.table, p.v.tmin, p.v.dinv,
                                       (double)ch[0] + (double)cl[0], (double)ch[1] + (double)cl[1],
                                       e1, e2);
                 d1 = (float)e1;

@@ -26,7 +26,7 @@ __device__ __forceinline__ void complex_noise(const ComplexStageParams& p, uint6
     }
 }
 
-template <int S>
+template <int S, bool TH>
 __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using TT = typename std::conditional<S == TIPT_F32C, float, double>::type;
@@ -68,11 +68,11 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
                 lapt[f] = (pt[f][1] + pt[f][2] + pt[f][3] + pt[f][4] + pt[f][5] + pt[f][6] - 6.0 * pt[f][0]) * p.inv_dx2;
             }
             double d1, d2;
-            complex_force<double>(p, dtab, p.tmin, p.dinv, a[0][0], a[1][0], d1, d2);
+            complex_force<double, TH>(p, dtab, p.tmin, p.dinv, a[0][0], a[1][0], d1, d2);
             double k1a = p.inv_a2 * lap[0] - p.eta * a[2][0] - d1 * p.inv_mu2;
             double k1b = p.inv_a2 * lap[1] - p.eta * a[3][0] - d2 * p.inv_mu2;
             double pta = a[2][0] + p.h1 * k1a, ptb = a[3][0] + p.h1 * k1b;
-            complex_force<double>(p, dtab, p.tmin, p.dinv, pt[0][0], pt[1][0], d1, d2);
+            complex_force<double, TH>(p, dtab, p.tmin, p.dinv, pt[0][0], pt[1][0], d1, d2);
             double k2a = p.inv_a2 * lapt[0] - p.eta * pta - d1 * p.inv_mu2;
             double k2b = p.inv_a2 * lapt[1] - p.eta * ptb - d2 * p.inv_mu2;
             complex_noise<double>(p, (uint64_t)s, n1, n2);
@@ -102,12 +102,12 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
                 lapt[f] = ((double)s6b - 6.0 * (double)pt[f][0]) * p.inv_dx2;
             }
             double d1, d2;
-            complex_force<double>(p, dtab, p.tmin, p.dinv, a[0][0], a[1][0], d1, d2);
+            complex_force<double, TH>(p, dtab, p.tmin, p.dinv, a[0][0], a[1][0], d1, d2);
             double k1a = p.inv_a2 * lap[0] - p.eta * (double)a[2][0] - d1 * p.inv_mu2;
             double k1b = p.inv_a2 * lap[1] - p.eta * (double)a[3][0] - d2 * p.inv_mu2;
             float pta = __double2float_rn((double)a[2][0] + p.h1 * k1a);
             float ptb = __double2float_rn((double)a[3][0] + p.h1 * k1b);
-            complex_force<double>(p, dtab, p.tmin, p.dinv, pt[0][0], pt[1][0], d1, d2);
+            complex_force<double, TH>(p, dtab, p.tmin, p.dinv, pt[0][0], pt[1][0], d1, d2);
             double k2a = p.inv_a2 * lapt[0] - p.eta * (double)pta - d1 * p.inv_mu2;
             double k2b = p.inv_a2 * lapt[1] - p.eta * (double)ptb - d2 * p.inv_mu2;
             complex_noise<float>(p, (uint64_t)s, n1, n2);
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
                         q2d = (double)hi[1][0] + ((double)lo[1][0] + (double)h1 * ((double)hi[3][0] + (double)lo[3][0]));
                     }
                     double e1, e2;
-                    complex_force<double>(p, p.table, p.tmin, p.dinv, q1d, q2d, e1, e2);
+                    complex_force<double, TH>(p, p.table, p.tmin, p.dinv, q1d, q2d, e1, e2);
                     d1 = (float)e1;
                     d2 = (float)e2;
                 }
@@ -180,7 +180,8 @@ constexpr int64_t kMaxTableSmemC = 96 * 1024;
 
 template <int S>
 static int launch_complex_generic(ComplexStageParams p, int64_t smem, cudaStream_t st) {
-    auto kern = complex_stage_generic<S>;
+    auto kern = p.vkind == TIPT_VP_THERMAL ? complex_stage_generic<S, true>
+                                           : complex_stage_generic<S, false>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -196,7 +197,8 @@ static int launch_complex_generic(ComplexStageParams p, int64_t smem, cudaStream
 }
 
 int launch_complex_stage(int storage, ComplexStageParams p, cudaStream_t st) {
-    int64_t tb = p.vkind == TIPT_VP_POLY ? 0 : (int64_t)p.npts * (storage == TIPT_F32C ? 4 : 8);
+    const bool no_table = p.vkind == TIPT_VP_POLY || p.vkind == TIPT_VP_THERMAL;
+    int64_t tb = no_table ? 0 : (int64_t)p.npts * (storage == TIPT_F32C ? 4 : 8);
     p.table_in_smem = (tb > 0 && tb <= kMaxTableSmemC) ? 1 : 0;
     const int64_t smem = p.table_in_smem ? tb : 0;
     if (storage == TIPT_F32C && kernel_policy() != 1) {
@@ -217,13 +219,14 @@ int launch_complex_stage(int storage, ComplexStageParams p, cudaStream_t st) {
 
 using namespace tipt;
 
-extern "C" int tipt_complex_rk2_step_table(int storage, const void* phi1, const void* phi2,
-                                           const void* pi1, const void* pi2, void* phi1_out,
-                                           void* phi2_out, void* pi1_out, void* pi2_out,
-                                           int64_t nx, int64_t ny, int64_t nz,
-                                           const tipt_step_params* sp, const tipt_vsource* vp,
-                                           const tipt_complex_terms* ct, const void* noise1,
-                                           const void* noise2, void* stream) {
+// Checks a complex stage call and fills its parameters (one midpoint stage of
+// size dt with the pass-2 hash multiplier; callers adjust the half steps).
+static int complex_stage_call(int storage, const void* phi1, const void* phi2, const void* pi1,
+                              const void* pi2, void* phi1_out, void* phi2_out, void* pi1_out,
+                              void* pi2_out, int64_t nx, int64_t ny, int64_t nz,
+                              const tipt_step_params* sp, const tipt_vsource* vp,
+                              const tipt_complex_terms* ct, const void* noise1,
+                              const void* noise2, ComplexStageParams& p) {
     int rc;
     if ((rc = check_state(storage, phi1, phi2, phi1_out, phi2_out, nx, ny, nz)) ||
         (rc = check_state(storage, pi1, pi2, pi1_out, pi2_out, nx, ny, nz)))
@@ -243,8 +246,6 @@ extern "C" int tipt_complex_rk2_step_table(int storage, const void* phi1, const 
     }
     if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
     if ((rc = check_vsource(vp, "vp"))) return rc;
-    if (vp->kind == TIPT_VP_THERMAL)
-        return fail(TIPT_ERR_UNSUPPORTED, "the complex field takes a V'(rho) table or a polynomial");
     if (vp->kind == TIPT_VP_TABLE2D)
         return fail(TIPT_ERR_UNSUPPORTED, "complex field takes a 1-D V'(rho) table");
     if ((noise1 == nullptr) != (noise2 == nullptr))
@@ -252,7 +253,6 @@ extern "C" int tipt_complex_rk2_step_table(int storage, const void* phi1, const 
     if (noise1 && ((rc = check_ptr(noise1, storage == TIPT_F32 ? 4 : 8, "noise1")) ||
                    (rc = check_ptr(noise2, storage == TIPT_F32 ? 4 : 8, "noise2"))))
         return rc;
-    ComplexStageParams p;
     memset(&p, 0, sizeof(p));
     p.f[0] = phi1;
     p.f[1] = phi2;
@@ -292,5 +292,49 @@ extern "C" int tipt_complex_rk2_step_table(int storage, const void* phi1, const 
     p.c1 = vp->c1;
     p.c2 = vp->c2;
     p.c3 = vp->c3;
+    if (vp->kind == TIPT_VP_THERMAL) p.th = thermal_site(*vp->thermal, vp->T);
+    return TIPT_OK;
+}
+
+
+extern "C" int tipt_complex_rk2_step_table(int storage, const void* phi1, const void* phi2,
+                                           const void* pi1, const void* pi2, void* phi1_out,
+                                           void* phi2_out, void* pi1_out, void* pi2_out, int64_t nx,
+                                           int64_t ny, int64_t nz, const tipt_step_params* sp,
+                                           const tipt_vsource* vp,
+                                           const tipt_complex_terms* ct, const void* noise1,
+                                           const void* noise2, void* stream) {
+    ComplexStageParams p;
+    int rc = complex_stage_call(storage, phi1, phi2, pi1, pi2, phi1_out, phi2_out, pi1_out,
+                                pi2_out, nx, ny, nz, sp, vp, ct, noise1, noise2, p);
+    if (rc) return rc;
     return launch_complex_stage(storage, p, (cudaStream_t)stream);
+}
+
+extern "C" int tipt_complex_rk2_fused_table(int storage, const void* phi1, const void* phi2,
+                                            const void* pi1, const void* pi2, void* phi1_out,
+                                            void* phi2_out, void* pi1_out, void* pi2_out,
+                                            void* mid1, void* mid2, void* mid3, void* mid4,
+                                            int64_t nx, int64_t ny, int64_t nz,
+                                            const tipt_step_params* sp,
+                                            const tipt_vsource* vp_T, const tipt_vsource* vp_Tm,
+                                            const tipt_complex_terms* ct, const void* noise1,
+                                            const void* noise2, void* stream) {
+    ComplexStageParams a, b;
+    int rc = complex_stage_call(storage, phi1, phi2, pi1, pi2, mid1, mid2, mid3, mid4, nx, ny, nz,
+                                sp, vp_T, ct, noise1, noise2, a);
+    if (rc) return rc;
+    rc = complex_stage_call(storage, mid1, mid2, mid3, mid4, phi1_out, phi2_out, pi1_out, pi2_out,
+                            nx, ny, nz, sp, vp_Tm, ct, noise1, noise2, b);
+    if (rc) return rc;
+    // first half at T (C:1829-1946), pass-2 multiplier; second at T_mid
+    // (C:1948-2064), pass-4 multiplier; 0.5 noise (array or hash) in each
+    for (ComplexStageParams* q : {&a, &b}) {
+        q->h1 = q->h2 = 0.5 * sp->dt;
+        q->nfac = 0.5;
+        q->ns_eff = 0.5 * sp->noise_scale;
+    }
+    b.mul = kPass4Mul;
+    if ((rc = launch_complex_stage(storage, a, (cudaStream_t)stream))) return rc;
+    return launch_complex_stage(storage, b, (cudaStream_t)stream);
 }

@@ -24,21 +24,31 @@ struct ComplexStageParams {
     double tmin, dinv;
     double c1, c2, c3;
     int table_in_smem;
+    ThermalSite th;  // TIPT_VP_THERMAL: the inline thermal V'(rho) at T
 };
 
 // C:2137-2158 projection + Z_N (reference form), then eps*Re(Phi^4) whose
 // gradient is 4 eps (p1^3 - 3 p1 p2^2, 3 p1^2 p2 - p2^3).  FP64 (and the
 // reference float32 mode's FP64 arithmetic).
-template <typename R>
+// TH = false compiles the thermal branch out (callers that never take it).
+template <typename R, bool TH = true>
 __device__ __forceinline__ void complex_force(const ComplexStageParams& p, const R* tab, R tmin,
                                               R dinv, R p1, R p2, R& d1, R& d2) {
     R rho = sqrt(p1 * p1 + p2 * p2);
     R rho_safe = rho > R(1e-30) ? rho : R(1e-30);
-    R dvdr;
-    if (p.vkind == TIPT_VP_POLY) dvdr = poly_vprime<R>((R)p.c1, (R)p.c2, (R)p.c3, rho);
-    else dvdr = lerp_table<R>(tab, tmin, dinv, p.npts - 2, rho);
-    R a = dvdr * p1 / rho_safe;
-    R b = dvdr * p2 / rho_safe;
+    R dvdr, a, b;
+    if (TH && p.vkind == TIPT_VP_THERMAL) {
+        // C:2605-2680 _vprime_complex_inline: V'(rho_safe) times phi_a * (1 / rho_safe)
+        dvdr = (R)thermal_vprime_inline(p.th, (double)rho_safe);
+        const R inv_rho = R(1) / rho_safe;
+        a = dvdr * p1 * inv_rho;
+        b = dvdr * p2 * inv_rho;
+    } else {
+        if (p.vkind == TIPT_VP_POLY) dvdr = poly_vprime<R>((R)p.c1, (R)p.c2, (R)p.c3, rho);
+        else dvdr = lerp_table<R>(tab, tmin, dinv, p.npts - 2, rho);
+        a = dvdr * p1 / rho_safe;
+        b = dvdr * p2 / rho_safe;
+    }
     if (p.zn_active > 0.5 && p.zn_n > 0.5 && rho > R(1e-20)) {
         R th = atan2(p2, p1);
         R sn = sin((R)p.zn_n * th);

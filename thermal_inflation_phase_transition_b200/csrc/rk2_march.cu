@@ -362,7 +362,7 @@ __global__ void __maxnreg__(kMarchRegs)
 // 16-byte vector per plane and neighbour) and evaluates them as two site
 // pairs in the lanes of the packed FP32x2 instructions; the stencil sums run
 // in the order of the generic kernel, so results are bitwise identical.
-template <bool WIDE>
+template <bool WIDE, bool TH>
 __global__ void __maxnreg__(kMarchRegs)
     rk2_stage_march_f32c(RealStageParams p_in, MarchGeom g) {
     RealStageParams p = p_in;
@@ -526,7 +526,7 @@ __global__ void __maxnreg__(kMarchRegs)
                 uint64_t site;
                 if constexpr (WIDE) site = (uint64_t)(rowoff + p.site_offset + 2 * h);
                 else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)(2 * h);
-                update_f32c<float2>(p, kc, s_tab, in[h], site_kick_f32c2(p, kc, site), o[h][0],
+                update_f32c<float2, TH>(p, kc, s_tab, in[h], site_kick_f32c2(p, kc, site), o[h][0],
                                     o[h][1], o[h][2], o[h][3]);
             }
             *reinterpret_cast<float4*>(phi_out + rowoff) = make_float4(o[0][0].x, o[0][0].y, o[1][0].x, o[1][0].y);
@@ -1185,9 +1185,12 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
     // 64-bit noise-key sites when an index (array + offset) can exceed 32 bits
     const bool wide = (int64_t)p.n0 * p.n1 * p.n2 + (p.site_offset > 0 ? p.site_offset : 0) >
                       0xFFFFFFFFll;
+    if (storage == TIPT_F32C && p.vkind == TIPT_VP_THERMAL)
+        return wide ? launch_march_k(rk2_stage_march_f32c<true, true>, p, g, smem, st)
+                    : launch_march_k(rk2_stage_march_f32c<false, true>, p, g, smem, st);
     if (storage == TIPT_F32C)
-        return wide ? launch_march_k(rk2_stage_march_f32c<true>, p, g, smem, st)
-                    : launch_march_k(rk2_stage_march_f32c<false>, p, g, smem, st);
+        return wide ? launch_march_k(rk2_stage_march_f32c<true, false>, p, g, smem, st)
+                    : launch_march_k(rk2_stage_march_f32c<false, false>, p, g, smem, st);
     if (storage == TIPT_F64)
         return wide ? launch_march_k(rk2_stage_march<TIPT_F64, true>, p, g, smem, st)
                     : launch_march_k(rk2_stage_march<TIPT_F64, false>, p, g, smem, st);

@@ -10,7 +10,7 @@
 
 namespace tipt {
 
-template <int S>
+template <int S, bool TH>
 __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
     RealStageParams p = p_in;
     resolve_schedule(p);
@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
                 pv[q] = __ldg(pi + idx[q]);
             }
             double a, b;
-            update_f64(p, reinterpret_cast<const double*>(s_tab), ph, pv,
+            update_f64<TH>(p, reinterpret_cast<const double*>(s_tab), ph, pv,
                        site_noise<double>(p, (uint64_t)(s + p.site_offset)), a, b);
             static_cast<double*>(p.phi_out)[s] = a;
             static_cast<double*>(p.pi_out)[s] = b;
@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
                 pv[q] = __ldg(pi + idx[q]);
             }
             float a, b;
-            update_f32(p, reinterpret_cast<const double*>(s_tab), ph, pv,
+            update_f32<TH>(p, reinterpret_cast<const double*>(s_tab), ph, pv,
                        site_noise<float>(p, (uint64_t)(s + p.site_offset)), a, b);
             static_cast<float*>(p.phi_out)[s] = a;
             static_cast<float*>(p.pi_out)[s] = b;
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
             x.pih = vh[0];
             x.pil = vl[0];
             float a, b, c, d;
-            update_f32c<float>(p, kc, reinterpret_cast<const float*>(s_tab), x,
+            update_f32c<float, TH>(p, kc, reinterpret_cast<const float*>(s_tab), x,
                                site_kick_f32c(p, kc, (uint64_t)(s + p.site_offset)), a, b, c, d);
             float* po = static_cast<float*>(p.phi_out);
             float* vo = static_cast<float*>(p.pi_out);
@@ -115,7 +115,7 @@ int num_sms() {
 
 template <int S>
 static int launch_generic(RealStageParams p, int64_t smem, cudaStream_t st) {
-    auto kern = rk2_stage_generic<S>;
+    auto kern = p.vkind == TIPT_VP_THERMAL ? rk2_stage_generic<S, true> : rk2_stage_generic<S, false>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);

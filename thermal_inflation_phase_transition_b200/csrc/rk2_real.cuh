@@ -102,9 +102,11 @@ __device__ __forceinline__ void stage_table(const RealStageParams& p, TT* s_tab)
 }
 
 // V'(x) in FP64 from the staged row, the global 1-D table, or the polynomial.
+// TH = false compiles the thermal branch out (see vprime_v).
+template <bool TH = true>
 __device__ __forceinline__ double vprime_d(const RealStageParams& p, const double* s_tab, double x) {
     if (p.vkind == TIPT_VP_POLY) return poly_vprime<double>(p.c1, p.c2, p.c3, x);
-    if (p.vkind == TIPT_VP_THERMAL) return thermal_vprime_inline(p.th, x);
+    if (TH && p.vkind == TIPT_VP_THERMAL) return thermal_vprime_inline(p.th, x);
     const double* t = p.table_in_smem ? s_tab : p.table;
     return lerp_table<double>(t, p.tmin, p.dinv, p.npts - 2, x);
 }
@@ -167,7 +169,9 @@ __device__ __forceinline__ F32CConst f32c_const(const RealStageParams& p) {
     return k;
 }
 
-template <typename V>
+// TH = false compiles the thermal branch out (kernels launched only for the
+// polynomial and table sources keep their register budget).
+template <typename V, bool TH = true>
 __device__ __forceinline__ V vprime_v(const RealStageParams& p, const F32CConst& kc,
                                       const float* s_tab, V x) {
     constexpr int NL = sizeof(V) / sizeof(float);
@@ -175,7 +179,7 @@ __device__ __forceinline__ V vprime_v(const RealStageParams& p, const F32CConst&
         const V d = v_fma(v_mul(v_mul(kvec<V>(p.k2.c3), x), x), x, v_mul(kvec<V>(p.k2.c1), x));
         return p.c2 != 0.0 ? v_fma(v_mul(kvec<V>(p.k2.c2), x), x, d) : d;
     }
-    if (p.vkind == TIPT_VP_THERMAL) {  // FP64 per lane from the FP32 value
+    if (TH && p.vkind == TIPT_VP_THERMAL) {  // FP64 per lane from the FP32 value
         V r;
 #pragma unroll
         for (int l = 0; l < NL; ++l)
@@ -213,6 +217,7 @@ __device__ __forceinline__ double force_d(const RealStageParams& p, double lap, 
     // inv_a2*lap - eta*pi - V'/mu^2
     return __dsub_rn(__dsub_rn(__dmul_rn(p.inv_a2, lap), __dmul_rn(p.eta, pv)), __dmul_rn(dv, p.inv_mu2));
 }
+template <bool TH = true>
 __device__ __forceinline__ void update_f64(const RealStageParams& p, const double* s_tab,
                                            const double ph[7], const double pv[7], double noise,
                                            double& phi_new, double& pi_new) {
@@ -222,9 +227,9 @@ __device__ __forceinline__ void update_f64(const RealStageParams& p, const doubl
 #pragma unroll
     for (int q = 0; q < 7; ++q) pt[q] = __fma_rn(p.h1, pv[q], ph[q]);
     const double lap2 = __dmul_rn(__fma_rn(-6.0, pt[0], sum6_d(pt)), p.inv_dx2);
-    const double k1 = force_d(p, lap, pv[0], vprime_d(p, s_tab, c));
+    const double k1 = force_d(p, lap, pv[0], vprime_d<TH>(p, s_tab, c));
     const double pit = __fma_rn(p.h1, k1, pv[0]);
-    const double k2 = force_d(p, lap2, pit, vprime_d(p, s_tab, pt[0]));
+    const double k2 = force_d(p, lap2, pit, vprime_d<TH>(p, s_tab, pt[0]));
     phi_new = __fma_rn(p.h2, pit, c);
     pi_new = __dadd_rn(pv[0], __fma_rn(p.h2, k2, noise));
 }
@@ -233,6 +238,7 @@ __device__ __forceinline__ void update_f64(const RealStageParams& p, const doubl
 // The reference's float32 mode (USE_FLOAT32, R:348): float32 neighbour sums,
 // FP64 for the rest, float32 stores -- including the stored midpoint state
 // phi~, pi~ that pass 2 reads (R:1932-1933).
+template <bool TH = true>
 __device__ __forceinline__ void update_f32(const RealStageParams& p, const double* s_tab,
                                            const float ph[7], const float pv[7], double noise,
                                            float& phi_new, float& pi_new) {
@@ -244,10 +250,10 @@ __device__ __forceinline__ void update_f32(const RealStageParams& p, const doubl
     for (int q = 0; q < 7; ++q) pt[q] = __double2float_rn((double)ph[q] + p.h1 * (double)pv[q]);
     float s6b = pt[1] + pt[2] + pt[3] + pt[4] + pt[5] + pt[6];
     double lap2 = ((double)s6b - 6.0 * (double)pt[0]) * p.inv_dx2;
-    double k1 = p.inv_a2 * lap - p.eta * (double)pv[0] - vprime_d(p, s_tab, (double)c) * p.inv_mu2;
+    double k1 = p.inv_a2 * lap - p.eta * (double)pv[0] - vprime_d<TH>(p, s_tab, (double)c) * p.inv_mu2;
     float pit = __double2float_rn((double)pv[0] + p.h1 * k1);
     double k2 = p.inv_a2 * lap2 - p.eta * (double)pit -
-                vprime_d(p, s_tab, (double)pt[0]) * p.inv_mu2;
+                vprime_d<TH>(p, s_tab, (double)pt[0]) * p.inv_mu2;
     phi_new = __double2float_rn((double)c + p.h2 * (double)pit);
     pi_new = __double2float_rn((double)pv[0] + (p.h2 * k2 + noise));
 }
@@ -274,7 +280,7 @@ __device__ __forceinline__ V force_v(V inv_a2, V eta, V inv_mu2, V lap, V pv, V 
     return v_sub(v_sub(v_mul(inv_a2, lap), v_mul(eta, pv)), v_mul(dv, inv_mu2));
 }
 
-template <typename V>
+template <typename V, bool TH = true>
 __device__ __forceinline__ void update_f32c(const RealStageParams& p, const F32CConst& kc,
                                             const float* s_tab, const F32CIn<V>& x, V kick,
                                             V& phh, V& phl, V& pih, V& pil) {
@@ -289,14 +295,14 @@ __device__ __forceinline__ void update_f32c(const RealStageParams& p, const F32C
     const V lap2 = v_fma(h1, lapv, lap);  // Laplacian of phi + h1 pi
     const V phc = v_add(x.phh, x.phl);
     const V pvc = v_add(x.pih, x.pil);
-    const V k1 = force_v(inv_a2, eta, inv_mu2, lap, pvc, vprime_v<V>(p, kc, s_tab, phc));
+    const V k1 = force_v(inv_a2, eta, inv_mu2, lap, pvc, vprime_v<V, TH>(p, kc, s_tab, phc));
     // pi~ = pi + h1 k1 as {t_hi, t_lo}
     V t_hi, t_e;
     two_sum(x.pih, v_mul(h1, k1), t_hi, t_e);
     const V t_lo = v_add(x.pil, t_e);
     const V pit = v_add(t_hi, t_lo);
     const V pht = v_add(x.phh, v_fma(h1, pvc, x.phl));
-    const V k2 = force_v(inv_a2, eta, inv_mu2, lap2, pit, vprime_v<V>(p, kc, s_tab, pht));
+    const V k2 = force_v(inv_a2, eta, inv_mu2, lap2, pit, vprime_v<V, TH>(p, kc, s_tab, pht));
     // phi + h2 pi~ with the product's rounding error kept
     const V d_hi = v_mul(h2h, t_hi);
     const V d_lo = v_add(v_fma(h2h, t_hi, v_neg(d_hi)), v_fma(h2h, t_lo, v_mul(h2l, t_hi)));

@@ -162,11 +162,13 @@ class ThermalPotential:
 _DEFAULT = {}
 
 
-def default_potential(device="cuda"):
+def default_potential(device="cuda", pot_coeffs=(1.0, 1.0)):
     """The reference script's module-level splines (R:432-455: dJ_B, dJ_F on the
-    256-point grid, no counterterm), built once per device on the GPU."""
+    256-point grid, no counterterm) with its _POT_COEFFS (real script (1, 1),
+    complex script (2, -1), C:215), built once per device on the GPU."""
     dev = torch.device(device)
-    key = (dev.type, dev.index if dev.index is not None else torch.cuda.current_device())
+    key = (dev.type, dev.index if dev.index is not None else torch.cuda.current_device(),
+           tuple(float(c) for c in pot_coeffs))
     if key not in _DEFAULT:
-        _DEFAULT[key] = ThermalPotential(device=dev)
+        _DEFAULT[key] = ThermalPotential(device=dev, pot_coeffs=pot_coeffs)
     return _DEFAULT[key]

@@ -360,7 +360,13 @@ typedef struct tipt_thermal {
     double boson_coupling, boson_gauge_coupling, fermion_coupling, fermion_gauge_coupling;
     double coeff_b, coeff_f;  /* the reference's _POT_COEFFS */
     double x_min, h;          /* spline grid: u_i = x_min + i h, i = 0..nseg */
-    int32_t nseg, pad_;
+    int32_t nseg;
+    int32_t form;             /* steppers' per-site V' (TIPT_VP_THERMAL): 0 = the inline form
+                                 _vprime_inline (R:2201-2266: x clamped to
+                                 x_min + h nseg - 1e-12, segment (x - x_min) * (1/h)),
+                                 1 = the Vprime_field form (R:1435-1485 with
+                                 cubic_eval_uniform R:1415-1426: clamped only above
+                                 x_min + h nseg, segment (x - x_min) / h) */
     const double* spline;     /* device [8][nseg]: dx^3, dx^2, dx, 1 coefficients of dJ_B, then dJ_F */
 } tipt_thermal;
 
@@ -379,6 +385,22 @@ int tipt_thermal_vprime_field(int storage, const void* phi, double T, const tipt
  * phi_i = linspace(phi_lo, phi_hi, nphi), T_j from the device array Ts. */
 int tipt_thermal_vprime_table(double phi_lo, double phi_hi, int32_t nphi, const double* Ts,
                               int32_t nT, const tipt_thermal* tp, double* out, void* stream);
+
+/* R:1364-1385 laplacian_periodic(out, a, dx): the periodic 7-point Laplacian
+ * (a[ip] + a[im] + a[jp] + a[jm] + a[kp] + a[km] - 6 a) / dx^2 into out, which
+ * has a's storage (F32: float32 neighbour sum, the rest in FP64, as the
+ * reference on float32 arrays; F32C: FP64 from hi + lo, stored as a {hi, lo}
+ * pair).  out must not overlap a. */
+int tipt_laplacian_periodic(int storage, const void* a, void* out, int64_t nx, int64_t ny,
+                            int64_t nz, double dx, void* stream);
+
+/* R:1415-1426 cubic_eval_uniform(x, x_min, h, nseg, c0, c1, c2, c3) at the n
+ * device points x: segment trunc((x - x_min) / h) clamped to [0, nseg - 1],
+ * Horner in dx = x - (x_min + i h) with the device coefficient arrays c0 (dx^3)
+ * .. c3 (1), FP64, into out[n]. */
+int tipt_cubic_eval_uniform(const double* x, int64_t n, double x_min, double h, int32_t nseg,
+                            const double* c0, const double* c1, const double* c2,
+                            const double* c3, double* out, void* stream);
 
 /* ------------------------------------------------------------ labelling
  * Connected components of |field| > threshold (face neighbours, open or

@@ -83,7 +83,7 @@ def load_real(pot_coeffs=(1.0, 1.0), splines: dict | None = None) -> dict:
         ["_hash_rng_pair", "rk2_step_table", "rk2_fused_table", "rk2_fused_single_pass",
          "rk2_step_inline", "_vprime_inline", "compute_energy_densities", "laplacian_periodic",
          "baoab_step_table", "overdamped_euler_step_table", "cubic_eval_uniform",
-         "Vprime_field"],
+         "Vprime_field", "rk2_step", "rk2_step_fused"],
         ["RK2_INLINE_TILE_J", "RK2_INLINE_TILE_K", "RK2_NF_TILE_J", "RK2_NF_TILE_K",
          "BAOAB_TILE_J", "BAOAB_TILE_K", "OVERDAMPED_TILE_J", "OVERDAMPED_TILE_K"],
         g,

@@ -109,3 +109,38 @@ def test_complex_thermal_oracle_matches_reference(golden):
         for a, f in zip(s, ("phi1", "phi2", "pi1", "pi2")):
             want = g[f"{key}_inline_{f}_5"]
             assert np.abs(a - want).max() <= 1e-12 * np.abs(want).max(), (key, f)
+
+
+def test_unfused_oracle_matches_reference(golden):
+    """oracle.thermal laplacian / cubic_eval_uniform / rk2_step / rk2_step_fused
+    against the reference's kernels (R:1364-1656), FP64 arrays."""
+    from oracle import oracle as O
+    from oracle import thermal as OT
+    g = golden("unfused.npz")
+    th = golden("thermal.npz")
+    u, cb, cf = th["u"], th["cb"], th["cf"]
+    x_min, h = float(u[0]), float(u[1] - u[0])
+    got = OT.cubic_eval_uniform(g["cubic_x"], x_min, h, cb.shape[1], *cb)
+    np.testing.assert_allclose(got, g["cubic_out"], rtol=1e-14, atol=0)
+    for tag in ("3d", "odd", "2d"):
+        lap = OT.laplacian(g[f"lap_{tag}_f64_in"], float(g["lap_dx"]))
+        ref = g[f"lap_{tag}_f64_out"]
+        assert np.abs(lap - ref).max() <= 1e-13 * np.abs(ref).max()
+    c = {k: float(g[k]) for k in _COUPLINGS}
+    dt, dx, eta, mu, inv_a2, T, Tm, ns = (float(g[k]) for k in
+                                          ("dt", "dx", "eta", "mu", "inv_a2", "T", "T_mid", "ns"))
+    for tag in ("3d", "odd", "2d"):
+        for name in ("rk2_step", "rk2_step_fused"):
+            key = f"{name}_{tag}_f64"
+            phi, pi = g[f"{key}_phi0"], g[f"{key}_pi0"]
+            for n in range(5):
+                nf = O.noise_field(phi.shape, n, O.K_PASS2, 0, ns, 0)
+                if name == "rk2_step":
+                    phi, pi = OT.rk2_step(phi, pi, dt, dx, eta, T, mu, c, nf, inv_a2, cb, cf,
+                                          x_min, h)
+                else:
+                    phi, pi = OT.rk2_step_fused(phi, pi, dt, dx, eta, T, Tm, mu, c, nf, inv_a2,
+                                                cb, cf, x_min, h)
+            for a, f in ((phi, "phi5"), (pi, "pi5")):
+                ref = g[f"{key}_{f}"]
+                assert np.abs(a - ref).max() <= 1e-12 * np.abs(ref).max(), (key, f)

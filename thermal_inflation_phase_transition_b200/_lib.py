@@ -42,7 +42,7 @@ class Thermal(C.Structure):
                 ("boson_coupling", C.c_double), ("boson_gauge_coupling", C.c_double),
                 ("fermion_coupling", C.c_double), ("fermion_gauge_coupling", C.c_double),
                 ("coeff_b", C.c_double), ("coeff_f", C.c_double), ("x_min", C.c_double),
-                ("h", C.c_double), ("nseg", C.c_int32), ("pad_", C.c_int32),
+                ("h", C.c_double), ("nseg", C.c_int32), ("form", C.c_int32),
                 ("spline", C.c_void_p)]
 
 
@@ -115,6 +115,8 @@ _SIGS = {
     "tipt_thermal_dj": [_i, _p, C.c_int32, _p, _p, _d, _p, _p],
     "tipt_thermal_vprime_field": [_i, _p, _d, C.POINTER(Thermal), _p, _i64, _i64, _i64, _p],
     "tipt_thermal_vprime_table": [_d, _d, C.c_int32, _p, C.c_int32, C.POINTER(Thermal), _p, _p],
+    "tipt_laplacian_periodic": [_i, _p, _p, _i64, _i64, _i64, _d, _p],
+    "tipt_cubic_eval_uniform": [_p, _i64, _d, _d, C.c_int32, _p, _p, _p, _p, _p, _p],
     "tipt_label_workspace_size": [_i64, _i64, _i64],
     "tipt_label_components": [_i, _p, _d, _i64, _i64, _i64, _i, _p, _p, _p, _i64, _p],
     "tipt_label_stats": [_i, _p, _p, _i64, _i64, _i64, C.c_int32, _p, _p, _p, _p, _p, _p],

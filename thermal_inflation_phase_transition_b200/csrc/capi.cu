@@ -73,6 +73,8 @@ int check_vsource(const tipt_vsource* vp, const char* name) {
         if (!t->spline || reinterpret_cast<uintptr_t>(t->spline) % 8)
             return fail(TIPT_ERR_ALIGN, "%s: spline is NULL or misaligned", name);
         if (!(vp->T > 0.0)) return fail(TIPT_ERR_ARG, "%s: T must be > 0", name);
+        if (t->form != 0 && t->form != 1)
+            return fail(TIPT_ERR_ARG, "%s: thermal form must be 0 (inline) or 1 (field)", name);
         return TIPT_OK;
     }
     if (vp->kind != TIPT_VP_TABLE && vp->kind != TIPT_VP_TABLE2D)

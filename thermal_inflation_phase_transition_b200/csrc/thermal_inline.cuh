@@ -1,10 +1,14 @@
 // The thermal one-loop V' evaluated per site, as the reference's inline form
-// _vprime_inline (R:2201-2266) that rk2_fused_single_pass (R:2339-2647) calls:
+// _vprime_inline (R:2201-2266) that rk2_fused_single_pass (R:2339-2647) calls
+// or (form 1) as Vprime_field (R:1435-1485) that rk2_step / rk2_step_fused call:
 //   V' = lam phi^3 - mphi^2 phi + T^4/(2 pi^2) (cb dJ_B(x_b) dx_b/dphi + cf dJ_F(x_f) dx_f/dphi),
 //   x_b = sqrt(mB^2 + gb^2 phi^2/2 + (gb^2/4 + 2 gg^2/3) T^2) / T,
 //   x_f = sqrt(gf^2 phi^2/2 + gfg^2 T^2/6) / T,
-// dJ from the cubic splines on the uniform grid x_min + i h (x clamped to
-// [x_min, xhi], segment trunc((x - x_min) / h) clamped to [0, nseg-1]).
+// dJ from the cubic splines on the uniform grid x_min + i h: inline form x
+// clamped to [x_min, xhi], xhi = x_min + h nseg - 1e-12, segment
+// trunc((x - x_min) * (1/h)); field form x below x_min raised to x_min, x above
+// x_min + h nseg lowered to x_min + h nseg - 1e-12, segment trunc((x - x_min) / h);
+// the segment clamped to [0, nseg-1] in both.
 // FP64, in the reference's order of operations.
 #pragma once
 
@@ -16,8 +20,9 @@ namespace tipt {
 struct ThermalSite {
     const double* spline;  // [8][nseg]: dx^3, dx^2, dx, 1 coefficients of dJ_B, then dJ_F
     int nseg;
+    int field_form;        // 1: the Vprime_field / cubic_eval_uniform clamp and segment rule
     double lam, mphi_sq, bms, gb2, gf2, gfg2, coef_b, coeff_b, coeff_f;
-    double x_min, h, inv_hy, xhi;
+    double x_min, h, inv_hy, xhi, xtop;
     double T, T2, pref;
 };
 
@@ -39,6 +44,8 @@ inline ThermalSite thermal_site(const tipt_thermal& t, double T) {
     s.h = t.h;
     s.inv_hy = 1.0 / t.h;                       // R:452
     s.xhi = t.x_min + t.h * t.nseg - 1e-12;     // R:453
+    s.xtop = t.x_min + t.h * t.nseg;            // R:1467-1468
+    s.field_form = t.form == 1;
     s.T = T;
     s.T2 = T * T;
     s.pref = s.T2 * s.T2 / (2.0 * 3.141592653589793 * 3.141592653589793);
@@ -48,9 +55,16 @@ inline ThermalSite thermal_site(const tipt_thermal& t, double T) {
 __device__ __forceinline__ double thermal_dj(const double* c, const ThermalSite& s, double x) {
     const int nseg = s.nseg;
     double xc = x;
-    if (xc < s.x_min) xc = s.x_min;
-    else if (xc > s.xhi) xc = s.xhi;
-    int si = (int)((xc - s.x_min) * s.inv_hy);
+    int si;
+    if (s.field_form) {  // R:1464-1473, R:1418-1424
+        if (xc < s.x_min) xc = s.x_min;
+        else if (xc > s.xtop) xc = s.xtop - 1e-12;
+        si = (int)((xc - s.x_min) / s.h);
+    } else {             // R:2238-2248
+        if (xc < s.x_min) xc = s.x_min;
+        else if (xc > s.xhi) xc = s.xhi;
+        si = (int)((xc - s.x_min) * s.inv_hy);
+    }
     si = si < 0 ? 0 : (si >= nseg ? nseg - 1 : si);
     const double d = xc - (s.x_min + si * s.h);
     return ((c[si] * d + c[nseg + si]) * d + c[2 * nseg + si]) * d + c[3 * nseg + si];

@@ -173,6 +173,107 @@ def rk2_fused_single_pass(phi, pi, dt, dx, eta_eff, T, T_mid, mu, lam, mphi, bos
            ptr(pi_tmp), nx, ny, nz, sp, va, vb, None, stream_handle())
 
 
+def laplacian_periodic(out, a, dx):
+    """R:1364 laplacian_periodic: out = periodic 7-point Laplacian of a (out has a's
+    storage; a float32 pair of planes is evaluated in FP64 and stored as hi/lo)."""
+    need_cuda(out, a, names=["out", "a"])
+    same_layout(a, out, names=["out"])
+    L.call("tipt_laplacian_periodic", storage_of(a), ptr(a), ptr(out), *dims_of(a), float(dx),
+           stream_handle())
+    return out
+
+
+def cubic_eval_uniform(x, x_min, h, nseg, c0, c1, c2, c3):
+    """R:1415 cubic_eval_uniform at the points x (a float64 CUDA tensor of any shape;
+    a Python number gives a Python float): segment trunc((x - x_min) / h) clamped
+    to [0, nseg - 1], Horner in x - x_i.  c0 .. c3 are float64 CUDA tensors."""
+    scalar = not isinstance(x, torch.Tensor)
+    dev = c0.device
+    xt = torch.tensor([float(x)], dtype=torch.float64, device=dev) if scalar else x
+    need_cuda(xt, c0, c1, c2, c3, names=["x", "c0", "c1", "c2", "c3"])
+    for c in (xt, c0, c1, c2, c3):
+        if c.dtype != torch.float64 or not c.is_contiguous():
+            raise ValueError("cubic_eval_uniform takes contiguous float64 tensors")
+    if min(c.numel() for c in (c0, c1, c2, c3)) < int(nseg):
+        raise ValueError("coefficient arrays are shorter than nseg")
+    out = torch.empty_like(xt)
+    L.call("tipt_cubic_eval_uniform", ptr(xt), xt.numel(), float(x_min), float(h), int(nseg),
+           ptr(c0), ptr(c1), ptr(c2), ptr(c3), ptr(out), stream_handle())
+    return float(out.item()) if scalar else out
+
+
+def Vprime_field(out, phi, T, lam, mphi, bosonMassSquared, bosonCoupling, bosonGaugeCoupling,
+                 fermionCoupling, fermionGaugeCoupling, *, splines=None):
+    """R:1435 Vprime_field: out = V'(phi, T) per site (FP64 arithmetic; out float64,
+    or float32 as the reference's float32 arrays).  The dJ splines come from
+    ``splines`` (a thermal.ThermalPotential), by default the reference script's."""
+    from .thermal import ThermalPotential, default_potential
+    need_cuda(out, phi, names=["out", "phi"])
+    if tuple(out.shape) != dims_of(phi) or out.dtype not in (torch.float64, torch.float32):
+        raise ValueError(f"out must be float64/float32 with shape {dims_of(phi)}")
+    tp = splines if splines is not None else default_potential(phi.device)
+    q = tp.params
+    th = L.Thermal(float(lam), float(mphi), float(bosonMassSquared), float(bosonCoupling),
+                   float(bosonGaugeCoupling), float(fermionCoupling), float(fermionGaugeCoupling),
+                   q.coeff_b, q.coeff_f, q.x_min, q.h, q.nseg, 1, q.spline)
+    o = out if out.dtype == torch.float64 and out.is_contiguous() else \
+        torch.empty(dims_of(phi), dtype=torch.float64, device=phi.device)
+    L.call("tipt_thermal_vprime_field", storage_of(phi), ptr(phi), float(T), th, ptr(o),
+           *dims_of(phi), stream_handle())
+    if o is not out:
+        out.copy_(o)
+    return out
+
+
+def _thermal_pair(phi, T_list, lam, mphi, bosonMassSquared, bosonCoupling, bosonGaugeCoupling,
+                  fermionCoupling, fermionGaugeCoupling, splines):
+    from .thermal import default_potential
+    tp = splines if splines is not None else default_potential(phi.device)
+    kw = dict(lam=lam, mphi=mphi, bosonMassSquared=bosonMassSquared, bosonCoupling=bosonCoupling,
+              bosonGaugeCoupling=bosonGaugeCoupling, fermionCoupling=fermionCoupling,
+              fermionGaugeCoupling=fermionGaugeCoupling, form="field")
+    return [tp.source(T, **kw) for T in T_list]
+
+
+def rk2_step(phi, pi, dt, dx, eta_eff, T, mu, lam, mphi, bosonMassSquared, bosonCoupling,
+             bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling, noise, lap, Vp,
+             phi_mid_buf, pi_mid_buf, inv_a2, *, splines=None):
+    """R:1489 rk2_step: the un-fused midpoint step (laplacian_periodic and
+    Vprime_field at phi, then at the midpoint; phi += dt pi~, pi += dt k~ + noise),
+    in place, as one fused launch with V' in the Vprime_field form.  ``lap`` and
+    ``Vp`` are the reference's scratch arrays and are not written;
+    ``phi_mid_buf`` / ``pi_mid_buf`` exchange storage with phi / pi."""
+    st = storage_of(phi)
+    need_cuda(phi, pi, phi_mid_buf, pi_mid_buf, names=["phi", "pi", "phi_mid_buf", "pi_mid_buf"])
+    same_layout(phi, pi, phi_mid_buf, pi_mid_buf, names=["pi", "phi_mid_buf", "pi_mid_buf"])
+    _noise_check(noise, phi, st)
+    (vs,) = _thermal_pair(phi, [T], lam, mphi, bosonMassSquared, bosonCoupling,
+                          bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling, splines)
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2)
+    L.call("tipt_rk2_step_table", st, ptr(phi), ptr(pi), ptr(phi_mid_buf), ptr(pi_mid_buf),
+           *dims_of(phi), sp, vs, ptr(noise), stream_handle())
+    swap_storage(phi, phi_mid_buf)
+    swap_storage(pi, pi_mid_buf)
+
+
+def rk2_step_fused(phi, pi, dt, dx, eta_eff, T, T_mid, mu, lam, mphi, bosonMassSquared,
+                   bosonCoupling, bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling,
+                   noise, lap, Vp, phi_mid_buf, pi_mid_buf, inv_a2, *, splines=None):
+    """R:1553 rk2_step_fused: two dt/2 midpoint halves with V' (Vprime_field form)
+    at T, then T_mid, and 0.5 * noise in each half, in place (two launches; the
+    state between the halves lives in phi_mid_buf / pi_mid_buf).  ``lap`` and
+    ``Vp`` are the reference's scratch arrays and are not written."""
+    st = storage_of(phi)
+    need_cuda(phi, pi, phi_mid_buf, pi_mid_buf, names=["phi", "pi", "phi_mid_buf", "pi_mid_buf"])
+    same_layout(phi, pi, phi_mid_buf, pi_mid_buf, names=["pi", "phi_mid_buf", "pi_mid_buf"])
+    _noise_check(noise, phi, st)
+    va, vb = _thermal_pair(phi, [T, T_mid], lam, mphi, bosonMassSquared, bosonCoupling,
+                           bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling, splines)
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2)
+    L.call("tipt_rk2_fused_table", st, ptr(phi), ptr(pi), ptr(phi), ptr(pi), ptr(phi_mid_buf),
+           ptr(pi_mid_buf), *dims_of(phi), sp, va, vb, ptr(noise), stream_handle())
+
+
 def _vsource_1d(vp_table, vp_tmin, vp_dinv, vp_npts, vpoly):
     if vpoly is not None:
         return poly_source(*[float(c) for c in vpoly])

@@ -107,10 +107,15 @@ class ThermalPotential:
                                 float(self.u[1] - self.u[0]), n_y - 1, 0, self._spl.data_ptr())
 
     def source(self, T, *, lam=None, mphi=None, bosonMassSquared=None, bosonCoupling=None,
-               bosonGaugeCoupling=None, fermionCoupling=None, fermionGaugeCoupling=None):
+               bosonGaugeCoupling=None, fermionCoupling=None, fermionGaugeCoupling=None,
+               form="inline"):
         """V' source of the steppers that evaluates this potential per site at T, as the
-        reference's inline V' (R:2201-2266 _vprime_inline); couplings default to this
-        object's.  The returned structure keeps its parameters alive."""
+        reference's inline V' (R:2201-2266 _vprime_inline, ``form="inline"``) or as its
+        Vprime_field (R:1435-1485, ``form="field"``, the V' of rk2_step /
+        rk2_step_fused); couplings default to this object's.  The returned structure
+        keeps its parameters alive."""
+        if form not in ("inline", "field"):
+            raise ValueError("form must be 'inline' or 'field'")
         q = self.params
         pick = lambda v, d: float(d if v is None else v)  # noqa: E731
         th = L.Thermal(pick(lam, q.lam), pick(mphi, q.mphi), pick(bosonMassSquared, q.boson_mass_sq),
@@ -118,7 +123,7 @@ class ThermalPotential:
                        pick(bosonGaugeCoupling, q.boson_gauge_coupling),
                        pick(fermionCoupling, q.fermion_coupling),
                        pick(fermionGaugeCoupling, q.fermion_gauge_coupling), q.coeff_b, q.coeff_f,
-                       q.x_min, q.h, q.nseg, 0, self._spl.data_ptr())
+                       q.x_min, q.h, q.nseg, 1 if form == "field" else 0, self._spl.data_ptr())
         vs = L.VSource(L.VP_THERMAL, 0, None, 0.0, 0.0, 0, 0, 0.0, 0.0, float(T), 0.0, 0.0, 0.0,
                        C.addressof(th))
         vs._keep = (th, self._spl)

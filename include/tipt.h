@@ -166,6 +166,16 @@ int tipt_rk2_step_table_sched(int storage, const void* phi, const void* pi, void
                               const double* sched, int64_t sched_len, const uint64_t* counter,
                               int64_t offset, void* stream);
 
+/* tipt_rk2_step_table_sched on an expanding background (the reference's
+ * HUBBLE_EXPANSION loop, R:3621-3636): sched holds sched_len rows
+ * (T, ns, eta_eff, inv_a2), and a step reads its eta_eff = eta + 3H/mu and
+ * inv_a2 = 1/a^2 from its row in place of sp->eta_eff and sp->inv_a2. */
+int tipt_rk2_step_table_sched4(int storage, const void* phi, const void* pi, void* phi_out,
+                               void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                               const tipt_step_params* sp, const tipt_vsource* vp,
+                               const double* sched, int64_t sched_len, const uint64_t* counter,
+                               int64_t offset, void* stream);
+
 /* *counter += k on the stream (one-thread kernel; graph-capturable). */
 int tipt_counter_add(uint64_t* counter, int64_t k, void* stream);
 

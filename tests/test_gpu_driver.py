@@ -52,3 +52,52 @@ def test_f32c_driver_tracks_fp64_cooling(shape):
     k = D.OBS_INDEX["phi2_mean"]
     rel = np.abs(r32[:, k] - r64[:, k]) / r64[:, k]
     assert rel.max() < 1e-6, rel.max()
+
+
+def _expanding_schedule(n):
+    """(T, ns, eta_eff, inv_a2) rows with every column varying step to step."""
+    s = np.empty((n, 4))
+    k = np.arange(n)
+    s[:, 0] = 1.04 - 0.002 * k
+    s[:, 1] = 0.3 + 0.01 * np.sin(k)
+    s[:, 2] = 1.0 + 0.05 * k
+    s[:, 3] = 1.0 / (1.0 + 0.03 * k) ** 2
+    return s
+
+
+def test_expanding_schedule_vs_oracle():
+    """Per-step eta_eff and inv_a2 from a 4-column schedule (the reference's
+    expanding loop, R:3621-3636), 20 graph-replayed steps against the oracle's
+    rk2_step_table called with each step's scalars."""
+    from oracle import oracle as O
+    shape = (12, 10, 8)
+    sched = _expanding_schedule(20)
+    tab = D.Table1D.build(D.toy_vprime, 1.02, -0.5, 3.0, 4096)
+    rng = np.random.default_rng(4)
+    phi0, pi0 = rng.normal(0.6, 0.5, shape), rng.normal(0.0, 0.3, shape)
+    sim = D.Simulation(shape, storage="f64", dt=0.05, dx=1.0, eta=9.0, mu=1.0, inv_a2=9.0,
+                       table=tab, schedule=sched, seed=3, phi0=phi0, pi0=pi0, graph_steps=10)
+    sim.run(20, observe=False)
+    phi, pi = phi0.copy(), pi0.copy()
+    for n in range(20):
+        T, ns, eta_eff, inv_a2 = sched[n]
+        O.rk2_step_table(phi, pi, 0.05, 1.0, eta_eff, 1.0, None, np.empty(shape),
+                         np.empty(shape), inv_a2, tab.values, tab.tmin, tab.dinv,
+                         tab.values.size, noise_scale=ns, noise_step=n, noise_seed=3)
+    g_phi, g_pi = sim.fields()
+    assert np.abs(g_phi.cpu().numpy() - phi).max() <= 1e-12 * np.abs(phi).max()
+    assert np.abs(g_pi.cpu().numpy() - pi).max() <= 1e-12 * np.abs(pi).max()
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_expanding_graphs_equal_eager(storage):
+    tab = D.Table2D.build(D.toy_vprime, 0.0, 3.0, 4096, 0.97, 1.06, 64)
+    sched = _expanding_schedule(50)
+    kw = dict(storage=storage, table=tab, schedule=sched, seed=1, init_seed=3, graph_steps=20)
+    a = D.Simulation((16, 12, 32), **kw)
+    b = D.Simulation((16, 12, 32), **kw)
+    oa = a.run(50)
+    ob = b.run(50, use_graphs=False)
+    assert np.array_equal(oa, ob)
+    for x, y in zip(a.fields(), b.fields()):
+        assert torch.equal(x, y)

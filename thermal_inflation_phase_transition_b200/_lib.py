@@ -78,6 +78,8 @@ _SIGS = {
                              _p],
     "tipt_rk2_step_table_sched": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
                                   C.POINTER(VSource), _p, _i64, _p, _i64, _p],
+    "tipt_rk2_step_table_sched4": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
+                                  C.POINTER(VSource), _p, _i64, _p, _i64, _p],
     "tipt_rk2_step_table_slab": [_i, _p, _p, _p, _p, _i64, _i64, _i64, _i64, _i64,
                                  C.POINTER(StepParams), C.POINTER(VSource), _p],
     "tipt_rk2_step_table_slab_planes": [_i, _p, _p, _p, _p, _i64, _i64, _i64, _i64, _i64, _i64,

@@ -253,11 +253,11 @@ int tipt_rk2_step_table_slab(int storage, const void* phi, const void* pi, void*
                                            i_lo, nx_global, 1, nx_local + 1, sp, vp, stream);
 }
 
-int tipt_rk2_step_table_sched(int storage, const void* phi, const void* pi, void* phi_out,
-                              void* pi_out, int64_t nx, int64_t ny, int64_t nz,
-                              const tipt_step_params* sp, const tipt_vsource* vp,
-                              const double* sched, int64_t sched_len, const uint64_t* counter,
-                              int64_t offset, void* stream) {
+static int step_table_sched(int storage, const void* phi, const void* pi, void* phi_out,
+                            void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                            const tipt_step_params* sp, const tipt_vsource* vp,
+                            const double* sched, int cols, int64_t sched_len,
+                            const uint64_t* counter, int64_t offset, void* stream) {
     int rc;
     if ((rc = check_state(storage, phi, pi, phi_out, pi_out, nx, ny, nz))) return rc;
     if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
@@ -277,8 +277,27 @@ int tipt_rk2_step_table_sched(int storage, const void* phi, const void* pi, void
     p.ctr = reinterpret_cast<const unsigned long long*>(counter);
     p.offset = offset;
     p.sched_len = sched_len;
+    p.sched_cols = cols;
     p.ns_mult = 1.0;
     return launch_real_stage(storage, p, (cudaStream_t)stream);
+}
+
+int tipt_rk2_step_table_sched(int storage, const void* phi, const void* pi, void* phi_out,
+                              void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                              const tipt_step_params* sp, const tipt_vsource* vp,
+                              const double* sched, int64_t sched_len, const uint64_t* counter,
+                              int64_t offset, void* stream) {
+    return step_table_sched(storage, phi, pi, phi_out, pi_out, nx, ny, nz, sp, vp, sched, 2,
+                            sched_len, counter, offset, stream);
+}
+
+int tipt_rk2_step_table_sched4(int storage, const void* phi, const void* pi, void* phi_out,
+                               void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                               const tipt_step_params* sp, const tipt_vsource* vp,
+                               const double* sched, int64_t sched_len, const uint64_t* counter,
+                               int64_t offset, void* stream) {
+    return step_table_sched(storage, phi, pi, phi_out, pi_out, nx, ny, nz, sp, vp, sched, 4,
+                            sched_len, counter, offset, stream);
 }
 
 __global__ void counter_add_kernel(unsigned long long* c, long long k) { *c += (unsigned long long)k; }

@@ -36,13 +36,17 @@ struct RealStageParams {
     double c1, c2, c3;
     int table_in_smem;   // 1: stage (and blend) the row into dynamic smem
     // Device-resident schedule (for graph-captured step loops): when sched is
-    // set, the step is s = *ctr + offset, T = sched[2s], the noise amplitude
-    // is ns_mult * sched[2s+1] and the hash step is step + s.
+    // set, the step is s = *ctr + offset, row e = min(s, sched_len - 1) of
+    // sched_cols doubles gives T = sched[cols e], the noise amplitude
+    // ns_mult * sched[cols e + 1] and, with 4 columns (an expanding
+    // background), eta_eff = sched[4e + 2] and inv_a2 = sched[4e + 3]; the hash
+    // step is step + s.
     const double* sched;
     const unsigned long long* ctr;
     long long offset;
     long long sched_len;  // steps beyond the schedule reuse its last entry
     double ns_mult;
+    int sched_cols;       // 2 (T, ns) or 4 (T, ns, eta_eff, inv_a2)
     // FP32 constants of the compensated storage as lane pairs (x = y), rounded
     // from the FP64 parameters on the host (set_f32c_pairs): the packed FP32x2
     // instructions then read them from the parameter bank.
@@ -62,8 +66,15 @@ __device__ __forceinline__ void resolve_schedule(RealStageParams& p) {
     if (!p.sched) return;
     const unsigned long long s = *p.ctr + (unsigned long long)p.offset;
     const unsigned long long e = s < (unsigned long long)p.sched_len ? s : p.sched_len - 1;
-    p.T = p.sched[2 * e];
-    p.ns_eff = p.ns_mult * p.sched[2 * e + 1];
+    const double* row = p.sched + (p.sched_cols == 4 ? 4 * e : 2 * e);
+    p.T = row[0];
+    p.ns_eff = p.ns_mult * row[1];
+    if (p.sched_cols == 4) {
+        p.eta = row[2];
+        p.inv_a2 = row[3];
+        p.k2.eta = make_float2((float)p.eta, (float)p.eta);
+        p.k2.inv_a2 = make_float2((float)p.inv_a2, (float)p.inv_a2);
+    }
     p.step += s;
 }
 

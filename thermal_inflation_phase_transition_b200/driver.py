@@ -27,7 +27,14 @@ from .observables import OBS_INDEX, OBS_NAMES, workspace_bytes
 from .real_field import to_f32c
 
 __all__ = ["Table1D", "Table2D", "Simulation", "constant_temperature", "linear_cooling",
-           "toy_vprime", "OBS_NAMES", "OBS_INDEX"]
+           "hubble_expansion", "hubble_param", "toy_vprime", "OBS_NAMES", "OBS_INDEX",
+           "G_STAR", "M_PL", "DEL_V"]
+
+# The reference's expanding background (R:424-427): SM relativistic degrees of
+# freedom, reduced Planck mass (GeV), vacuum energy of the inflation background (GeV^4).
+G_STAR = 106.75
+M_PL = 2.4e18
+DEL_V = 1e36 / 4
 
 
 def toy_vprime(phi, T, D=0.1, E=0.05, lam=0.1, T0=1.0):
@@ -90,12 +97,48 @@ def linear_cooling(T_start, T_end, n_cool, n_steps, *, dt, eta=1.0, dx_phys=1.0,
     return np.ascontiguousarray(np.stack([T, ns], axis=1), np.float64)
 
 
+def hubble_param(T, g_star=G_STAR, m_pl=M_PL, del_v=DEL_V):
+    """H(T) = sqrt((T^4 g* pi^2 / 30 + del_V) / (3 M_pl^2)) in GeV (R:706-710, the
+    form the step loop evaluates, R:3625)."""
+    T4 = T * T * T * T
+    return math.sqrt((T4 * (g_star * math.pi ** 2 / 30.0) + del_v) * (1.0 / (3.0 * m_pl ** 2)))
+
+
+def hubble_expansion(T0, n_steps, *, dt, eta, mu, dx_phys=1.0, scale_factor=True, noise=True,
+                     a0=1.0, g_star=G_STAR, m_pl=M_PL, del_v=DEL_V):
+    """(n_steps, 4) schedule of (T, ns, eta_eff, inv_a2) on the reference's expanding
+    background (R:3621-3636, noise amplitude R:3714-3718): at step n, T = T0 / a,
+    H = H(T), eta_eff = eta + 3H/mu and inv_a2 = 1/a^2 (eta_eff = eta, inv_a2 =
+    inv_a3 = 1 when ``scale_factor`` is False, the reference's --no_scale_factor),
+    ns = sqrt(2 eta_eff T dt inv_a3 / (mu^2 dx_phys^3)); then a += a H dt / mu.
+    Returns the schedule and the scale factor after the last step."""
+    out = np.empty((n_steps, 4), np.float64)
+    chig = g_star * math.pi ** 2 / 30.0
+    inv3 = 1.0 / (3.0 * m_pl ** 2)
+    a = float(a0)
+    for n in range(n_steps):
+        T = T0 / a
+        T4 = T * T * T * T
+        H = math.sqrt((T4 * chig + del_v) * inv3)
+        if scale_factor:
+            eta_eff, inv_a2, inv_a3 = eta + 3.0 * H / mu, 1.0 / (a * a), 1.0 / (a * a * a)
+        else:
+            eta_eff, inv_a2, inv_a3 = eta, 1.0, 1.0
+        ns = math.sqrt(2.0 * eta_eff * T * dt * inv_a3 / (mu ** 2 * dx_phys ** 3)) if noise else 0.0
+        out[n] = (T, ns, eta_eff, inv_a2)
+        a += a * H * (dt / mu)
+    return out, a
+
+
 class Simulation:
     """A real scalar field on a periodic lattice, stepped by graph-captured chunks.
 
     storage: "f64", "f32" (the reference's float32 mode) or "f32c" (compensated).
     table: Table1D / Table2D, or None with vpoly = (c1, c2, c3) for the polynomial
     V'(phi) = c1 phi + c2 phi^2 + c3 phi^3.
+    schedule: (n, 2) rows (T, ns) per step, or (n, 4) rows (T, ns, eta_eff, inv_a2)
+    for an expanding background (``hubble_expansion``); the observables' gradient
+    energy uses the constructor's inv_a2.
     phi0/pi0: initial fields (numpy, FP64); default phi ~ N(0, init_sigma^2), pi = 0.
     """
 
@@ -110,8 +153,11 @@ class Simulation:
         self.thr = obs_threshold
         self.graph_steps = max(2, graph_steps + (graph_steps & 1))  # even: state ends in buffer 0
         self.schedule = np.ascontiguousarray(schedule, np.float64)
-        if self.schedule.ndim != 2 or self.schedule.shape[1] != 2:
-            raise ValueError("schedule must be (n_steps, 2): (T, ns) per step")
+        if self.schedule.ndim != 2 or self.schedule.shape[1] not in (2, 4):
+            raise ValueError("schedule must be (n_steps, 2) (T, ns) or (n_steps, 4) "
+                             "(T, ns, eta_eff, inv_a2) per step")
+        self._sched_fn = ("tipt_rk2_step_table_sched" if self.schedule.shape[1] == 2
+                          else "tipt_rk2_step_table_sched4")
         self._sched = torch.from_numpy(self.schedule).to(self.dev)
         if table is None:
             if vpoly is None:
@@ -200,11 +246,11 @@ class Simulation:
         nx, ny, nz = self.shape
         for q in range(K):
             a, b = q & 1, (q + 1) & 1
-            rc = lib.tipt_rk2_step_table_sched(
+            rc = getattr(lib, self._sched_fn)(
                 self._st(), ptr(self.phi[a]), ptr(self.pi[a]), ptr(self.phi[b]), ptr(self.pi[b]),
                 nx, ny, nz, self._sp, self._vs, ptr(self._sched), self.schedule.shape[0],
                 ptr(self._counter), q, st)
-            L.check(rc, "tipt_rk2_step_table_sched")
+            L.check(rc, self._sched_fn)
             if obs is not None and (not observe_last or q == K - 1):
                 rc = lib.tipt_observables(self._st(), ptr(self.phi[b]), ptr(self.pi[b]), nx, ny,
                                           nz, float(self.dx), float(self.inv_a2), 0.0, 0.0,

@@ -396,6 +396,14 @@ int tipt_thermal_vprime_field(int storage, const void* phi, double T, const tipt
 int tipt_thermal_vprime_table(double phi_lo, double phi_hi, int32_t nphi, const double* Ts,
                               int32_t nT, const tipt_thermal* tp, double* out, void* stream);
 
+/* C:1452-1530 Vprime_field of the complex field: out1, out2 (FP64, N each) =
+ * V'(rho_safe, T) phi_a / rho_safe with rho_safe = max(|phi|, 1e-30), the radial
+ * V' of tipt_thermal_vprime_field, plus the Z_N term of ct (NULL: none). */
+int tipt_thermal_vprime_field_complex(int storage, const void* phi1, const void* phi2, double T,
+                                      const tipt_thermal* tp, const tipt_complex_terms* ct,
+                                      double* out1, double* out2, int64_t nx, int64_t ny,
+                                      int64_t nz, void* stream);
+
 /* R:1364-1385 laplacian_periodic(out, a, dx): the periodic 7-point Laplacian
  * (a[ip] + a[im] + a[jp] + a[jm] + a[kp] + a[km] - 6 a) / dx^2 into out, which
  * has a's storage (F32: float32 neighbour sum, the rest in FP64, as the

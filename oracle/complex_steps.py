@@ -14,14 +14,17 @@ operations:
   pair per site, key (site * 73856093) ^ step in the first half and
   (site * 19349669) ^ step in the second, 0.5 * noise_scale * (r cos, r sin);
 * ``rk2_step_inline`` -- C:3140-: one midpoint step (dt/2 predictor, dt
-  corrector) with the inline thermal V'(rho) and noise arrays.
+  corrector) with the inline thermal V'(rho) and noise arrays;
+* ``field_force`` / ``rk2_step`` / ``rk2_step_fused`` -- C:1452-1737: the
+  un-fused forms with Vprime_field (the radial V' of oracle.thermal.vprime_field at
+  rho_safe, projected, plus the Z_N term).
 """
 from __future__ import annotations
 
 import numpy as np
 
 from . import oracle as O
-from .thermal import vprime_inline
+from .thermal import vprime_field, vprime_inline
 
 
 def _lap(f, inv_dx2):
@@ -121,3 +124,30 @@ def rk2_step_inline(s, dt, dx, eta, T, mu, couplings, noise1, noise2, inv_a2, cb
     """C:3140- on s = [phi1, phi2, pi1, pi2], in place."""
     midpoint(s, 0.5 * dt, dt, dx, eta, mu, inv_a2,
              thermal_force(T, cb, cf, x_min, h_y, couplings, pot_coeffs), noise1, noise2)
+
+
+def field_force(T, cb, cf, x_min, h, couplings, pot_coeffs=(2.0, -1.0), zn=(0.0, 0.0, 0.0)):
+    """C:1452-1530 Vprime_field: V'(rho_safe) phi_a * (1 / rho_safe) (+ Z_N)."""
+    def f(p1, p2):
+        rho = np.sqrt(p1 * p1 + p2 * p2)
+        rho_safe = np.maximum(rho, 1e-30)
+        inv_rho = 1.0 / rho_safe
+        dv = vprime_field(rho_safe, T, cb, cf, x_min, h, pot_coeffs=pot_coeffs, **couplings)
+        return _zn(p1, p2, rho, rho_safe, zn, dv * p1 * inv_rho, dv * p2 * inv_rho)
+    return f
+
+
+def rk2_step(s, dt, dx, eta, T, mu, couplings, noise1, noise2, inv_a2, cb, cf, x_min, h_y,
+             pot_coeffs=(2.0, -1.0), zn=(0.0, 0.0, 0.0)):
+    """C:1533-1607 on s = [phi1, phi2, pi1, pi2], in place."""
+    midpoint(s, 0.5 * dt, dt, dx, eta, mu, inv_a2,
+             field_force(T, cb, cf, x_min, h_y, couplings, pot_coeffs, zn), noise1, noise2)
+
+
+def rk2_step_fused(s, dt, dx, eta, T, T_mid, mu, couplings, noise1, noise2, inv_a2, cb, cf,
+                   x_min, h_y, pot_coeffs=(2.0, -1.0), zn=(0.0, 0.0, 0.0)):
+    """C:1610-1737 on s = [phi1, phi2, pi1, pi2], in place."""
+    for TT in (T, T_mid):
+        midpoint(s, 0.5 * dt, 0.5 * dt, dx, eta, mu, inv_a2,
+                 field_force(TT, cb, cf, x_min, h_y, couplings, pot_coeffs, zn),
+                 0.5 * noise1, 0.5 * noise2)

@@ -105,7 +105,9 @@ def load_complex(zn_params=(0.0, 0.0, 0.0), pot_coeffs=(2.0, -1.0), splines: dic
         COMPLEX_SCRIPT,
         ["_hash_rng_pair", "rk2_step_table", "rk2_fused_table", "compute_winding_number",
          "rk2_fused_single_pass", "_vprime_inline", "_vprime_complex_inline",
-         "baoab_step_table", "overdamped_euler_step_table", "rk2_step_inline"],
+         "baoab_step_table", "overdamped_euler_step_table", "rk2_step_inline",
+         "rk2_step", "rk2_step_fused", "Vprime_field", "laplacian_periodic",
+         "cubic_eval_uniform"],
         ["RK2_INLINE_TILE_J", "RK2_INLINE_TILE_K", "RK2_NF_TILE_J", "RK2_NF_TILE_K",
          "BAOAB_TILE_J", "BAOAB_TILE_K",
          "OVERDAMPED_TILE_J", "OVERDAMPED_TILE_K"],

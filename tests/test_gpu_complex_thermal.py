@@ -170,3 +170,57 @@ def test_complex_thermal_rejects_mismatched_noise(golden):
     with pytest.raises(ValueError):
         CF.rk2_step_inline(*st, 0.05, 1.0, 0.5, 3000.0, 1000.0, 1e-24, 1000.0, 1e6, 1.09, 1.05,
                            1.09, 1.05, n1, None, *tmp, 1.0, splines=_pot(golden("thermal.npz")))
+
+
+# ------------------------------------- complex un-fused stepper (C:1452-1737) ---
+ZN_TAGS = ("u1", "z4")
+
+
+def _zn_of(g, zn_tag):
+    return tuple(g["zn_z4"]) if zn_tag == "z4" else (0.0, 0.0, 0.0)
+
+
+@pytest.mark.parametrize("zn_tag", ZN_TAGS)
+def test_complex_vprime_field_vs_reference(golden, zn_tag):
+    g = golden("complex_unfused.npz")
+    tp = _pot(golden("thermal.npz"))
+    p1 = torch.from_numpy(g[f"vf_{zn_tag}_phi1"]).cuda()
+    p2 = torch.from_numpy(g[f"vf_{zn_tag}_phi2"]).cuda()
+    o1, o2 = torch.empty_like(p1), torch.empty_like(p2)
+    CF.Vprime_field(o1, o2, p1, p2, float(g["T"]), *[float(g[k]) for k in COUPLINGS],
+                    zn=_zn_of(g, zn_tag), splines=tp)
+    for got, k in ((o1, "out1"), (o2, "out2")):
+        ref = g[f"vf_{zn_tag}_{k}"]
+        assert np.abs(got.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", ["rk2_step", "rk2_step_fused"])
+@pytest.mark.parametrize("zn_tag", ZN_TAGS)
+@pytest.mark.parametrize("tag", ["3d", "odd"])
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_complex_unfused_vs_reference(golden, name, zn_tag, tag, storage):
+    """Five steps of the complex script's rk2_step / rk2_step_fused (Vprime_field
+    with the reference's dJ splines, pot_coeffs (2, -1), noise arrays) against the
+    reference kernels; f32c with Z_4 gets the wider bound of the Z_N force."""
+    g = golden("complex_unfused.npz")
+    tp = _pot(golden("thermal.npz"))
+    key = f"{name}_{zn_tag}_{tag}"
+    st = _state(g, key, storage)
+    mid = [torch.empty_like(a) for a in st]
+    p = {k: float(g[k]) for k in ("dt", "dx", "eta", "mu", "inv_a2", "T", "T_mid", "ns")}
+    c = [float(g[k]) for k in COUPLINGS]
+    shape = tuple(g[f"{key}_phi1_0"].shape)
+    ids = [id(a) for a in st]
+    for n in range(5):
+        n1, n2 = _noise(shape, n, p["ns"], 0), _noise(shape, n, p["ns"], 1)
+        if name == "rk2_step":
+            CF.rk2_step(*st, p["dt"], p["dx"], p["eta"], p["T"], p["mu"], *c, n1, n2, None, None,
+                        None, None, *mid, p["inv_a2"], zn=_zn_of(g, zn_tag), splines=tp)
+        else:
+            CF.rk2_step_fused(*st, p["dt"], p["dx"], p["eta"], p["T"], p["T_mid"], p["mu"], *c,
+                              n1, n2, None, None, None, None, *mid, p["inv_a2"],
+                              zn=_zn_of(g, zn_tag), splines=tp)
+    torch.cuda.synchronize()
+    assert [id(a) for a in st] == ids
+    tol = 1e-11 if storage == "f64" else (5e-5 if zn_tag == "z4" else 2e-6)
+    _check(st, g, key, tol)

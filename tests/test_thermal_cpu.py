@@ -144,3 +144,39 @@ def test_unfused_oracle_matches_reference(golden):
             for a, f in ((phi, "phi5"), (pi, "pi5")):
                 ref = g[f"{key}_{f}"]
                 assert np.abs(a - ref).max() <= 1e-12 * np.abs(ref).max(), (key, f)
+
+
+def test_complex_unfused_oracle_matches_reference(golden):
+    """oracle.complex_steps field_force / rk2_step / rk2_step_fused against the
+    complex script's Vprime_field, rk2_step and rk2_step_fused (C:1452-1737),
+    U(1) and Z_4."""
+    from oracle import oracle as O
+    from oracle import complex_steps as CS
+    g = golden("complex_unfused.npz")
+    th = golden("thermal.npz")
+    u, cb, cf = th["u"], th["cb"], th["cf"]
+    x_min, h = float(u[0]), float(u[1] - u[0])
+    c = {k: float(g[k]) for k in _COUPLINGS}
+    dt, dx, eta, mu, inv_a2, T, Tm, ns = (float(g[k]) for k in
+                                          ("dt", "dx", "eta", "mu", "inv_a2", "T", "T_mid", "ns"))
+    for zn_tag, zn in (("u1", (0.0, 0.0, 0.0)), ("z4", tuple(g["zn_z4"]))):
+        d1, d2 = CS.field_force(T, cb, cf, x_min, h, c, zn=zn)(g[f"vf_{zn_tag}_phi1"],
+                                                               g[f"vf_{zn_tag}_phi2"])
+        for got, k in ((d1, "out1"), (d2, "out2")):
+            ref = g[f"vf_{zn_tag}_{k}"]
+            assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max(), (zn_tag, k)
+        for tag in ("3d", "odd"):
+            for name in ("rk2_step", "rk2_step_fused"):
+                key = f"{name}_{zn_tag}_{tag}"
+                s = _state(g, key, 0)
+                shape = s[0].shape
+                for n in range(5):
+                    n1 = O.noise_field(shape, n, O.K_PASS2, 0, ns, 0)
+                    n2 = O.noise_field(shape, n, O.K_PASS2, 0, ns, 1)
+                    if name == "rk2_step":
+                        CS.rk2_step(s, dt, dx, eta, T, mu, c, n1, n2, inv_a2, cb, cf, x_min, h,
+                                    zn=zn)
+                    else:
+                        CS.rk2_step_fused(s, dt, dx, eta, T, Tm, mu, c, n1, n2, inv_a2, cb, cf,
+                                          x_min, h, zn=zn)
+                _close(s, g, key, "_5", 1e-12)

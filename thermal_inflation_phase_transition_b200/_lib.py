@@ -117,6 +117,8 @@ _SIGS = {
     "tipt_thermal_dj": [_i, _p, C.c_int32, _p, _p, _d, _p, _p],
     "tipt_thermal_vprime_field": [_i, _p, _d, C.POINTER(Thermal), _p, _i64, _i64, _i64, _p],
     "tipt_thermal_vprime_table": [_d, _d, C.c_int32, _p, C.c_int32, C.POINTER(Thermal), _p, _p],
+    "tipt_thermal_vprime_field_complex": [_i, _p, _p, _d, C.POINTER(Thermal),
+                                          C.POINTER(ComplexTerms), _p, _p, _i64, _i64, _i64, _p],
     "tipt_laplacian_periodic": [_i, _p, _p, _i64, _i64, _i64, _d, _p],
     "tipt_cubic_eval_uniform": [_p, _i64, _d, _d, C.c_int32, _p, _p, _p, _p, _p, _p],
     "tipt_label_workspace_size": [_i64, _i64, _i64],

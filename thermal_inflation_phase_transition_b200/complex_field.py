@@ -140,6 +140,83 @@ def rk2_step_inline(phi1, phi2, pi1, pi2, dt, dx, eta_eff, T, mu, lam_val, mphi_
         swap_storage(a, b)
 
 
+def _field_sources(phi1, Ts, lam, mphi, bosonMassSquared, bosonCoupling, bosonGaugeCoupling,
+                   fermionCoupling, fermionGaugeCoupling, splines):
+    from .thermal import default_potential
+    tp = splines if splines is not None else default_potential(phi1.device, (2.0, -1.0))
+    kw = _thermal_kw(lam, mphi, bosonMassSquared, bosonCoupling, bosonGaugeCoupling,
+                     fermionCoupling, fermionGaugeCoupling)
+    return [tp.source(T, form="field", **kw) for T in Ts]
+
+
+def Vprime_field(out1, out2, phi1_arr, phi2_arr, T, lam, mphi, bosonMassSquared, bosonCoupling,
+                 bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling, *,
+                 zn=(0.0, 0.0, 0.0), splines=None):
+    """C:1452 Vprime_field of the complex field: (out1, out2) = V'(rho) phi_a / rho
+    (+ the Z_N term of ``zn``), FP64 arithmetic; out float64 (or float32).  The dJ
+    splines default to the complex script's (pot_coeffs (2, -1))."""
+    from .thermal import default_potential
+    need_cuda(out1, out2, phi1_arr, phi2_arr, names=["out1", "out2", "phi1", "phi2"])
+    same_layout(phi1_arr, phi2_arr, names=["phi2"])
+    shape = dims_of(phi1_arr)
+    for o in (out1, out2):
+        if tuple(o.shape) != shape or o.dtype not in (torch.float64, torch.float32):
+            raise ValueError(f"outputs must be float64/float32 with shape {shape}")
+    tp = splines if splines is not None else default_potential(phi1_arr.device, (2.0, -1.0))
+    q = tp.params
+    th = L.Thermal(float(lam), float(mphi), float(bosonMassSquared), float(bosonCoupling),
+                   float(bosonGaugeCoupling), float(fermionCoupling), float(fermionGaugeCoupling),
+                   q.coeff_b, q.coeff_f, q.x_min, q.h, q.nseg, 1, q.spline)
+    ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), 0.0)
+    tmp = [o if o.dtype == torch.float64 and o.is_contiguous() else
+           torch.empty(shape, dtype=torch.float64, device=phi1_arr.device) for o in (out1, out2)]
+    L.call("tipt_thermal_vprime_field_complex", storage_of(phi1_arr), ptr(phi1_arr),
+           ptr(phi2_arr), float(T), th, ct, ptr(tmp[0]), ptr(tmp[1]), *shape, stream_handle())
+    for o, t in zip((out1, out2), tmp):
+        if o is not t:
+            o.copy_(t)
+    return out1, out2
+
+
+def rk2_step(phi1, phi2, pi1, pi2, dt, dx, eta_eff, T, mu, lam, mphi, bosonMassSquared,
+             bosonCoupling, bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling, noise1,
+             noise2, lap1, lap2, Vp1, Vp2, phi1_mid_buf, phi2_mid_buf, pi1_mid_buf, pi2_mid_buf,
+             inv_a2, *, zn=(0.0, 0.0, 0.0), eps4=0.0, splines=None):
+    """C:1533 rk2_step (complex): the un-fused midpoint step with Vprime_field
+    (C:1452) at phi, then at the midpoint, in place, as one fused launch; the
+    scratch arrays lap1 .. Vp2 are accepted and not written; the *_mid_buf tensors
+    exchange storage with phi1 .. pi2."""
+    st = storage_of(phi1)
+    arrs = (phi1, phi2, pi1, pi2, phi1_mid_buf, phi2_mid_buf, pi1_mid_buf, pi2_mid_buf)
+    names = ("phi1", "phi2", "pi1", "pi2", "phi1_mid_buf", "phi2_mid_buf", "pi1_mid_buf",
+             "pi2_mid_buf")
+    need_cuda(*arrs, names=names)
+    same_layout(phi1, *arrs[1:], names=names[1:])
+    _check_noise_pair(noise1, noise2, st, phi1)
+    (vs,) = _field_sources(phi1, [T], lam, mphi, bosonMassSquared, bosonCoupling,
+                           bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling, splines)
+    sp = step_params(dt, dx, eta_eff, mu, inv_a2)
+    ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
+    L.call("tipt_complex_rk2_step_table", st, *[ptr(a) for a in arrs], *dims_of(phi1), sp, vs, ct,
+           ptr(noise1), ptr(noise2), stream_handle())
+    for a, b in zip(arrs[:4], arrs[4:]):
+        swap_storage(a, b)
+
+
+def rk2_step_fused(phi1, phi2, pi1, pi2, dt, dx, eta_eff, T, T_mid, mu, lam, mphi,
+                   bosonMassSquared, bosonCoupling, bosonGaugeCoupling, fermionCoupling,
+                   fermionGaugeCoupling, noise1, noise2, lap1, lap2, Vp1, Vp2, phi1_mid_buf,
+                   phi2_mid_buf, pi1_mid_buf, pi2_mid_buf, inv_a2, *, zn=(0.0, 0.0, 0.0),
+                   eps4=0.0, splines=None):
+    """C:1610 rk2_step_fused (complex): two dt/2 halves with Vprime_field at T, then
+    T_mid, and 0.5 * noise in each, in place (two launches; the state between the
+    halves lives in the *_mid_buf tensors); lap1 .. Vp2 are accepted and not written."""
+    va, vb = _field_sources(phi1, [T, T_mid], lam, mphi, bosonMassSquared, bosonCoupling,
+                            bosonGaugeCoupling, fermionCoupling, fermionGaugeCoupling, splines)
+    _fused((phi1, phi2, pi1, pi2), (phi1_mid_buf, phi2_mid_buf, pi1_mid_buf, pi2_mid_buf), dt, dx,
+           eta_eff, mu, inv_a2, va, vb, zn, eps4, noise1, noise2, 0.0, 0, 0)
+
+
 def rk2_step_table_into(state, out, dt, dx, eta_eff, mu, inv_a2, vsource, *, zn=(0.0, 0.0, 0.0),
                         eps4=0.0, noise_scale=0.0, noise_step=0, seed=0, stream=None):
     """Ping-pong form: state=(phi1, phi2, pi1, pi2) -> out=(phi1', phi2', pi1', pi2')."""
@@ -237,3 +314,8 @@ def compute_winding_number_full(phi1, phi2, *, w_site=True, w3=True, pierced_cap
     L.call("tipt_compute_winding_number", st, ptr(phi1), ptr(phi2), *shape, ptr(ws), ptr(w3t),
            ptr(pl), int(pierced_cap), ptr(counts), stream_handle(stream))
     return WindingResult(ws, w3t, pl, counts)
+
+
+# C:1387 laplacian_periodic and C:1438 cubic_eval_uniform are the real script's
+# kernels (R:1364, R:1415) verbatim.
+from .real_field import cubic_eval_uniform, laplacian_periodic  # noqa: E402,F401

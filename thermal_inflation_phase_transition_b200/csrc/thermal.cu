@@ -187,6 +187,72 @@ extern "C" int tipt_thermal_vprime_field(int storage, const void* phi, double T,
     return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "thermal V' launch");
 }
 
+// C:1452-1530 Vprime_field of the complex field at one site: the radial V' of
+// Vprime_field at rho_safe = max(rho, 1e-30), projected as V' phi_a / rho_safe,
+// plus the Z_N term (C:1519-1527).
+template <int S>
+__global__ void thermal_field_complex_kernel(const void* phi1, const void* phi2, double T,
+                                             tipt_thermal t, tipt_complex_terms ct, double* out1,
+                                             double* out2, int64_t N) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < N;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double p1, p2;
+        if constexpr (S == TIPT_F64) {
+            p1 = static_cast<const double*>(phi1)[s];
+            p2 = static_cast<const double*>(phi2)[s];
+        } else if constexpr (S == TIPT_F32) {
+            p1 = (double)static_cast<const float*>(phi1)[s];
+            p2 = (double)static_cast<const float*>(phi2)[s];
+        } else {
+            const float* a = static_cast<const float*>(phi1);
+            const float* b = static_cast<const float*>(phi2);
+            p1 = (double)a[s] + (double)a[N + s];
+            p2 = (double)b[s] + (double)b[N + s];
+        }
+        const double rho = sqrt(p1 * p1 + p2 * p2);
+        const double rho_safe = rho > 1e-30 ? rho : 1e-30;
+        const double inv_rho = 1.0 / rho_safe;
+        const double dv = thermal_vprime(t, rho_safe, T);
+        double d1 = dv * p1 * inv_rho, d2 = dv * p2 * inv_rho;
+        if (ct.zn_active > 0.5 && ct.zn_n > 0.5 && rho > 1e-20) {
+            const double sn = sin(ct.zn_n * atan2(p2, p1));
+            const double ir2 = inv_rho * inv_rho;
+            d1 += -ct.zn_n * ct.zn_dv * sn * p2 * ir2;
+            d2 += ct.zn_n * ct.zn_dv * sn * p1 * ir2;
+        }
+        out1[s] = d1;
+        out2[s] = d2;
+    }
+}
+
+extern "C" int tipt_thermal_vprime_field_complex(int storage, const void* phi1, const void* phi2,
+                                                 double T, const tipt_thermal* tp,
+                                                 const tipt_complex_terms* ct, double* out1,
+                                                 double* out2, int64_t nx, int64_t ny, int64_t nz,
+                                                 void* stream) {
+    int rc;
+    const int al = elem_align(storage);
+    if ((rc = check_storage(storage)) || (rc = check_dims(nx, ny, nz)) ||
+        (rc = check_ptr(phi1, al, "phi1")) || (rc = check_ptr(phi2, al, "phi2")) ||
+        (rc = check_ptr(out1, 8, "out1")) || (rc = check_ptr(out2, 8, "out2")) ||
+        (rc = check_thermal(tp)))
+        return rc;
+    if (!(T > 0.0)) return fail(TIPT_ERR_ARG, "T must be > 0");
+    tipt_complex_terms terms = {0.0, 0.0, 0.0, 0.0};
+    if (ct) terms = *ct;
+    const int64_t N = nx * ny * nz;
+    int64_t blocks = (N + 255) / 256;
+    if (blocks > (int64_t)num_sms() * 16) blocks = (int64_t)num_sms() * 16;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (storage) {
+        case TIPT_F64: thermal_field_complex_kernel<TIPT_F64><<<(unsigned)blocks, 256, 0, st>>>(phi1, phi2, T, *tp, terms, out1, out2, N); break;
+        case TIPT_F32: thermal_field_complex_kernel<TIPT_F32><<<(unsigned)blocks, 256, 0, st>>>(phi1, phi2, T, *tp, terms, out1, out2, N); break;
+        default: thermal_field_complex_kernel<TIPT_F32C><<<(unsigned)blocks, 256, 0, st>>>(phi1, phi2, T, *tp, terms, out1, out2, N); break;
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "complex thermal V' launch");
+}
+
 extern "C" int tipt_thermal_vprime_table(double phi_lo, double phi_hi, int32_t nphi,
                                          const double* Ts, int32_t nT, const tipt_thermal* tp,
                                          double* out, void* stream) {

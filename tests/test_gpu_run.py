@@ -23,9 +23,10 @@ def _snap(path, step):
 
 @pytest.mark.parametrize("integrator", RUN.INTEGRATORS)
 @pytest.mark.parametrize("hubble", [False, True])
-def test_every_integrator_runs(tmp_path, integrator, hubble):
+@pytest.mark.parametrize("storage", ["f32", "f32c", "f64"])
+def test_every_integrator_runs(tmp_path, integrator, hubble, storage):
     argv = BASE + ["--Nt", "8", "--steps", "4", "--integrator", integrator, "--out",
-                   str(tmp_path), "--storage", "f32c", "--diag_energy"]
+                   str(tmp_path), "--storage", storage, "--diag_energy"]
     if not hubble:
         argv.append("--no_hubble")
     r = RUN.Run(RUN.build_parser().parse_args(argv))

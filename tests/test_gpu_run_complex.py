@@ -19,11 +19,12 @@ def _snap(path, step):
 
 
 @pytest.mark.parametrize("integrator", [None] + RC.INTEGRATORS)
-def test_every_integrator_runs_with_zn_turn_on(tmp_path, integrator):
+@pytest.mark.parametrize("storage", ["f32", "f32c", "f64"])
+def test_every_integrator_runs_with_zn_turn_on(tmp_path, integrator, storage):
     """8 steps with Z_4 switched on below a T that the expanding background crosses
     at the first step (the flag reaches the kernels, unlike the reference's frozen
     global); snapshots carry rho, theta, windings, zn_active and the scale factor."""
-    argv = BASE + ["--Nt", "8", "--steps", "4", "--out", str(tmp_path), "--storage", "f32c",
+    argv = BASE + ["--Nt", "8", "--steps", "4", "--out", str(tmp_path), "--storage", storage,
                    "--zn_order", "4", "--zn_strength", "1e9", "--zn_turn_on_T", "7349.9",
                    "--init_rho", "3000"]
     if integrator:

@@ -153,3 +153,17 @@ def test_step_inline_thermal_vs_reference(golden, tag, storage):
         ref = g[key]
         got = got.cpu().numpy()
         assert np.abs(got - ref).max() <= tol * np.abs(ref).max(), (key, np.abs(got - ref).max())
+
+
+def test_module_level_reference_names(golden):
+    """thermal.Vprime_scalar / build_vprime_table (R:805, R:840) with the reference's
+    splines against the reference's table."""
+    g = golden("thermal.npz")
+    pot = _pot(g, splines=(g["cb"], g["cf"]))
+    tab, tmin, dinv = TH.build_vprime_table(float(g["T"]), -20000.0, 20000.0, 4096, potential=pot)
+    ref = g["table"]
+    np.testing.assert_allclose(tab.cpu().numpy(), ref, rtol=1e-11, atol=1e-11 * np.abs(ref).max())
+    x = np.linspace(-20000.0, 20000.0, 4096)
+    for i in (0, 1000, 2048, 4095):
+        v = TH.Vprime_scalar(x[i], float(g["T"]), potential=pot)
+        assert abs(v - ref[i]) <= 1e-11 * np.abs(ref).max()

@@ -177,3 +177,18 @@ def default_potential(device="cuda", pot_coeffs=(1.0, 1.0)):
     if key not in _DEFAULT:
         _DEFAULT[key] = ThermalPotential(device=dev, pot_coeffs=pot_coeffs)
     return _DEFAULT[key]
+
+
+def Vprime_scalar(phi_val, T_val, *, potential=None):
+    """R:805 Vprime_scalar(phi, T): V'(phi, T) as a Python float, evaluated on the GPU
+    as build_vprime_table evaluates each point; the potential defaults to the
+    reference script's (default_potential)."""
+    tp = potential if potential is not None else default_potential()
+    return float(tp._table(float(phi_val), float(phi_val), 2, [float(T_val)])[0, 0])
+
+
+def build_vprime_table(T_val, phi_min, phi_max, n_table, *, potential=None):
+    """R:840 build_vprime_table(T, phi_min, phi_max, n): (table as a float64 CUDA
+    tensor, phi_min, 1/dphi); the potential defaults to the reference script's."""
+    tp = potential if potential is not None else default_potential()
+    return tp.table(T_val, phi_min, phi_max, n_table)

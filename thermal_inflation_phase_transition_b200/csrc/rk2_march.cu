@@ -166,10 +166,10 @@ __device__ __forceinline__ void ld_pair_g(const E* p, E& a, E& b) {
 template <int S>
 __device__ __forceinline__ void site_update(const RealStageParams& p, const void* s_tab,
                                             float, float, const typename MarchElem<S>::E ph[7],
-                                            const typename MarchElem<S>::E pv[7], uint64_t site,
+                                            const typename MarchElem<S>::E pv[7], double noise,
                                             typename MarchElem<S>::E& a,
                                             typename MarchElem<S>::E& b) {
-    update_f64(p, static_cast<const double*>(s_tab), ph, pv, site_noise<double>(p, site), a, b);
+    update_f64(p, static_cast<const double*>(s_tab), ph, pv, noise, a, b);
 }
 
 // Launch bounds of the two block-size classes: up to 256 consumer threads
@@ -298,12 +298,25 @@ __global__ void __maxnreg__(kMarchRegs)
             return;
         }
         for (int q = 0; q < ni; ++q) {
+            const int i = i0 + q;
+            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2;
+            // the noise reads no tile: drawn before the wait for the next plane
+            double nz[2][2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int col = (h ? half + c : c) + u;
+                    uint64_t site;
+                    if constexpr (WIDE) site = (uint64_t)(rowoff + p.site_offset + col);
+                    else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)col;
+                    nz[h][u] = site_noise<double>(p, site);
+                }
+            }
             if (!mbar_wait(&full[pp.stage], pp.phase)) {
                 if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
                 return;
             }
-            const int i = i0 + q;
-            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {   // pair A (h = 0), pair B (h = 1)
                 const int col = h ? half + c : c;
@@ -333,10 +346,7 @@ __global__ void __maxnreg__(kMarchRegs)
                                      u ? kr[0] : ce[0][1], u ? ce[0][0] : kl[0]};
                     const E pv[7] = {ce[1][u], ip[1][u], im[1][u], jp[1][u], jm[1][u],
                                      u ? kr[1] : ce[1][1], u ? ce[1][0] : kl[1]};
-                    uint64_t site;
-                    if constexpr (WIDE) site = (uint64_t)(rowoff + p.site_offset + col + u);
-                    else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)(col + u);
-                    site_update<S>(p, s_tab, tminf, dinvf, ph, pv, site, op[u], ov[u]);
+                    site_update<S>(p, s_tab, tminf, dinvf, ph, pv, nz[h][u], op[u], ov[u]);
                 }
                 st_pair_g(phi_out + rowoff + col, op[0], op[1]);
                 st_pair_g(pi_out + rowoff + col, ov[0], ov[1]);
@@ -467,12 +477,21 @@ __global__ void __maxnreg__(kMarchRegs)
             return;
         }
         for (int q = 0; q < ni; ++q) {
+            const int i = i0 + q;
+            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2 + k0;
+            // the noise reads no tile: drawn before the wait for the next plane
+            float2 kick[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint64_t site;
+                if constexpr (WIDE) site = (uint64_t)(rowoff + p.site_offset + 2 * h);
+                else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)(2 * h);
+                kick[h] = site_kick_f32c2(p, kc, site);
+            }
             if (!mbar_wait(&full[pp.stage], pp.phase)) {
                 if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
                 return;
             }
-            const int i = i0 + q;
-            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2 + k0;
             F32CIn<float2> in[2];
 #pragma unroll
             for (int f = 0; f < 2; ++f) {
@@ -522,13 +541,9 @@ __global__ void __maxnreg__(kMarchRegs)
             if (lane == 0) mbar_arrive(&empty[pm.stage]);  // plane i-1 is no longer read
             float2 o[2][4];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                uint64_t site;
-                if constexpr (WIDE) site = (uint64_t)(rowoff + p.site_offset + 2 * h);
-                else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)(2 * h);
-                update_f32c<float2, TH>(p, kc, s_tab, in[h], site_kick_f32c2(p, kc, site), o[h][0],
-                                    o[h][1], o[h][2], o[h][3]);
-            }
+            for (int h = 0; h < 2; ++h)
+                update_f32c<float2, TH>(p, kc, s_tab, in[h], kick[h], o[h][0], o[h][1], o[h][2],
+                                        o[h][3]);
             *reinterpret_cast<float4*>(phi_out + rowoff) = make_float4(o[0][0].x, o[0][0].y, o[1][0].x, o[1][0].y);
             *reinterpret_cast<float4*>(phi_out + N + rowoff) = make_float4(o[0][1].x, o[0][1].y, o[1][1].x, o[1][1].y);
             *reinterpret_cast<float4*>(pi_out + rowoff) = make_float4(o[0][2].x, o[0][2].y, o[1][2].x, o[1][2].y);
@@ -656,11 +671,28 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
             return;
         }
         for (int q = 0; q < ni; ++q) {
+            const int64_t rowoff = ((int64_t)(i0 + q) * n1 + jw) * n2 + k0;
+            // the noise reads no tile: drawn before the wait for the next plane
+            float2 zz[2][NF];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint64_t site;
+                if constexpr (WIDE) site = (uint64_t)(rowoff + 2 * h);
+                else site = (uint32_t)rowoff + (uint32_t)(2 * h);
+                const uint64_t ka = noise_key(site, p.step, kPass2Mul, p.seed);
+                const uint64_t kb = noise_key(site + 1, p.step, kPass2Mul, p.seed);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) zz[h][f] = make_float2(0.0f, 0.0f);
+                if constexpr (CPLX) {
+                    if (noisy) gauss_pair_f2(ka, kb, zz[h][0], zz[h][1]);
+                } else {
+                    if (noisy) zz[h][0] = gauss_cos_f2(ka, kb);
+                }
+            }
             if (!mbar_wait(&full[pp.stage], pp.phase)) {
                 if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
                 return;
             }
-            const int64_t rowoff = ((int64_t)(i0 + q) * n1 + jw) * n2 + k0;
             float2 dsum[2][NF][2], cen[2][NF][2];  // [pair][field][hi, lo]
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
@@ -705,20 +737,13 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
             float ah[NF][4], al[NF][4], bh[NF][4], bl[NF][4];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                uint64_t site;
-                if constexpr (WIDE) site = (uint64_t)(rowoff + 2 * h);
-                else site = (uint32_t)rowoff + (uint32_t)(2 * h);
-                const uint64_t ka = noise_key(site, p.step, kPass2Mul, p.seed);
-                const uint64_t kb = noise_key(site + 1, p.step, kPass2Mul, p.seed);
-                float2 z[NF], vp[NF];
+                const float2* z = zz[h];
+                float2 vp[NF];
                 if constexpr (CPLX) {
-                    z[0] = z[1] = make_float2(0.0f, 0.0f);
-                    if (noisy) gauss_pair_f2(ka, kb, z[0], z[1]);
                     complex_force_v<float2>(p.v, s_tab, tminf, dinvf,
                                             v_add(cen[h][0][0], cen[h][0][1]),
                                             v_add(cen[h][1][0], cen[h][1][1]), vp[0], vp[1]);
                 } else {
-                    z[0] = noisy ? gauss_cos_f2(ka, kb) : make_float2(0.0f, 0.0f);
                     const float2 x = v_add(cen[h][0][0], cen[h][0][1]);
                     if (p.v.vkind == TIPT_VP_POLY) {
                         const float2 d = v_fma(v_mul(v_mul(vs<float2>((float)p.v.c3), x), x), x,
@@ -932,13 +957,19 @@ __global__ void __maxnreg__(kMarchRegs)
             return;
         }
         for (int q = 0; q < ni; ++q) {
+            const int i = i0 + q;
+            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2 + k0s + k0;
+            // the noise reads no tile: drawn before the wait for the next plane
+            float2 kick[2];
+            if constexpr (WIDE)
+                complex_kick_f32c2(p, (uint64_t)rowoff, (uint64_t)(rowoff + 1), kick[0], kick[1]);
+            else
+                complex_kick_f32c2(p, (uint32_t)rowoff, (uint32_t)rowoff + 1u, kick[0], kick[1]);
             if (!mbar_wait(&full[pp.stage], pp.phase)) {
                 if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
                 if (edge) asm volatile("cp.async.wait_all;" ::: "memory");
                 return;
             }
-            const int i = i0 + q;
-            const int64_t rowoff = ((int64_t)i * n1 + jw) * n2 + k0s + k0;
             float hv[8];
             if (edge) {
                 asm volatile("cp.async.wait_all;" ::: "memory");
@@ -984,11 +1015,6 @@ __global__ void __maxnreg__(kMarchRegs)
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[pm.stage]);  // plane i-1 is no longer read
-            float2 kick[2];
-            if constexpr (WIDE)
-                complex_kick_f32c2(p, (uint64_t)rowoff, (uint64_t)(rowoff + 1), kick[0], kick[1]);
-            else
-                complex_kick_f32c2(p, (uint32_t)rowoff, (uint32_t)rowoff + 1u, kick[0], kick[1]);
             float2 oh[4], ol[4];
             complex_update_f32c<float2>(p, in, kick, force, oh, ol);
 #pragma unroll

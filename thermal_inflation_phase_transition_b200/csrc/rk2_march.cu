@@ -488,6 +488,25 @@ __global__ void __maxnreg__(kMarchRegs)
                 else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)(2 * h);
                 kick[h] = site_kick_f32c2(p, kc, site);
             }
+            // the centre plane is resident: its values and V' at the centre and
+            // the midpoint are evaluated before the wait as well
+            F32CPre<float2> pre[2];
+            {
+                float4 cen[2][2];  // [field][hi, lo]
+#pragma unroll
+                for (int f = 0; f < 2; ++f)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c)
+                        cen[f][c] = *reinterpret_cast<const float4*>(blk(pc.stage, f, c) + orow + k0);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const auto pick = [h](const float4& v) {
+                        return h ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+                    };
+                    pre[h] = pre_f32c<float2, TH>(p, kc, s_tab, pick(cen[0][0]), pick(cen[0][1]),
+                                                  pick(cen[1][0]), pick(cen[1][1]));
+                }
+            }
             if (!mbar_wait(&full[pp.stage], pp.phase)) {
                 if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
                 return;
@@ -542,8 +561,7 @@ __global__ void __maxnreg__(kMarchRegs)
             float2 o[2][4];
 #pragma unroll
             for (int h = 0; h < 2; ++h)
-                update_f32c<float2, TH>(p, kc, s_tab, in[h], kick[h], o[h][0], o[h][1], o[h][2],
-                                        o[h][3]);
+                post_f32c<float2>(p, in[h], pre[h], kick[h], o[h][0], o[h][1], o[h][2], o[h][3]);
             *reinterpret_cast<float4*>(phi_out + rowoff) = make_float4(o[0][0].x, o[0][0].y, o[1][0].x, o[1][0].y);
             *reinterpret_cast<float4*>(phi_out + N + rowoff) = make_float4(o[0][1].x, o[0][1].y, o[1][1].x, o[1][1].y);
             *reinterpret_cast<float4*>(pi_out + rowoff) = make_float4(o[0][2].x, o[0][2].y, o[1][2].x, o[1][2].y);

@@ -291,10 +291,33 @@ __device__ __forceinline__ V force_v(V inv_a2, V eta, V inv_mu2, V lap, V pv, V 
     return v_sub(v_sub(v_mul(inv_a2, lap), v_mul(eta, pv)), v_mul(dv, inv_mu2));
 }
 
+// The part of the site update that reads only the centre values: the centre
+// and midpoint fields and V' at both (marching kernels evaluate it before the
+// neighbouring plane arrives).
+template <typename V>
+struct F32CPre {
+    V pvc, v1, v2;  // pi (hi + lo), V'(phi), V'(phi + h1 pi)
+};
+
 template <typename V, bool TH = true>
-__device__ __forceinline__ void update_f32c(const RealStageParams& p, const F32CConst& kc,
-                                            const float* s_tab, const F32CIn<V>& x, V kick,
-                                            V& phh, V& phl, V& pih, V& pil) {
+__device__ __forceinline__ F32CPre<V> pre_f32c(const RealStageParams& p, const F32CConst& kc,
+                                               const float* s_tab, V phh, V phl, V pih, V pil) {
+    const V h1 = kvec<V>(p.k2.h1);
+    const V phc = v_add(phh, phl);
+    F32CPre<V> r;
+    r.pvc = v_add(pih, pil);
+    const V pht = v_add(phh, v_fma(h1, r.pvc, phl));
+    r.v1 = vprime_v<V, TH>(p, kc, s_tab, phc);
+    r.v2 = vprime_v<V, TH>(p, kc, s_tab, pht);
+    return r;
+}
+
+// The rest of the site update, from the stencil sums, the centre values and the
+// pre-part.
+template <typename V>
+__device__ __forceinline__ void post_f32c(const RealStageParams& p, const F32CIn<V>& x,
+                                          const F32CPre<V>& pre, V kick, V& phh, V& phl, V& pih,
+                                          V& pil) {
     const V h1 = kvec<V>(p.k2.h1);
     const V h2h = kvec<V>(p.k2.h2h);
     const V h2l = kvec<V>(p.k2.h2l);
@@ -304,21 +327,27 @@ __device__ __forceinline__ void update_f32c(const RealStageParams& p, const F32C
     const V lap = v_mul(v_add(x.dh_phi, x.dl_phi), inv_dx2);
     const V lapv = v_mul(v_add(x.dh_pi, x.dl_pi), inv_dx2);
     const V lap2 = v_fma(h1, lapv, lap);  // Laplacian of phi + h1 pi
-    const V phc = v_add(x.phh, x.phl);
-    const V pvc = v_add(x.pih, x.pil);
-    const V k1 = force_v(inv_a2, eta, inv_mu2, lap, pvc, vprime_v<V, TH>(p, kc, s_tab, phc));
+    const V pvc = pre.pvc;
+    const V k1 = force_v(inv_a2, eta, inv_mu2, lap, pvc, pre.v1);
     // pi~ = pi + h1 k1 as {t_hi, t_lo}
     V t_hi, t_e;
     two_sum(x.pih, v_mul(h1, k1), t_hi, t_e);
     const V t_lo = v_add(x.pil, t_e);
     const V pit = v_add(t_hi, t_lo);
-    const V pht = v_add(x.phh, v_fma(h1, pvc, x.phl));
-    const V k2 = force_v(inv_a2, eta, inv_mu2, lap2, pit, vprime_v<V, TH>(p, kc, s_tab, pht));
+    const V k2 = force_v(inv_a2, eta, inv_mu2, lap2, pit, pre.v2);
     // phi + h2 pi~ with the product's rounding error kept
     const V d_hi = v_mul(h2h, t_hi);
     const V d_lo = v_add(v_fma(h2h, t_hi, v_neg(d_hi)), v_fma(h2h, t_lo, v_mul(h2l, t_hi)));
     ff_add(x.phh, x.phl, d_hi, d_lo, phh, phl);
     ff_add(x.pih, x.pil, v_fma(h2h, k2, kick), vs<V>(0.0f), pih, pil);
+}
+
+template <typename V, bool TH = true>
+__device__ __forceinline__ void update_f32c(const RealStageParams& p, const F32CConst& kc,
+                                            const float* s_tab, const F32CIn<V>& x, V kick,
+                                            V& phh, V& phl, V& pih, V& pil) {
+    const F32CPre<V> pre = pre_f32c<V, TH>(p, kc, s_tab, x.phh, x.phl, x.pih, x.pil);
+    post_f32c<V>(p, x, pre, kick, phh, phl, pih, pil);
 }
 
 // Stencil sums of one planar field for one site from the seven values in

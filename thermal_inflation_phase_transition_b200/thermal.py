@@ -184,7 +184,9 @@ def Vprime_scalar(phi_val, T_val, *, potential=None):
     as build_vprime_table evaluates each point; the potential defaults to the
     reference script's (default_potential)."""
     tp = potential if potential is not None else default_potential()
-    return float(tp._table(float(phi_val), float(phi_val), 2, [float(T_val)])[0, 0])
+    x = float(phi_val)
+    # the first point of a two-point grid is phi itself
+    return float(tp._table(x, x + max(1.0, abs(x)), 2, [float(T_val)])[0, 0])
 
 
 def build_vprime_table(T_val, phi_min, phi_max, n_table, *, potential=None):

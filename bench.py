@@ -240,6 +240,10 @@ def main():
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--storage", choices=["f32c", "f64", "f32"], default="f32c")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-result", choices=["range", "observables"], default="range",
+                    help="per-step result the e2e leg reads back: the new phi's range folded by "
+                         "the step kernel (the reference loop's phi.min()/max()), or the 10 "
+                         "observables of a separate reduction")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["lattice", "complex", "ensemble", "surrogate", "extras"],
                     default="lattice",
@@ -414,8 +418,11 @@ def main():
 
 def run_e2e(args, shape, seed, RF, observables, torch, dev, world):
     """End to end through the public API from pinned HOST buffers: upload the state,
-    K steps of real_field.rk2_step_table (in-place semantics) each followed by the
-    observables reduction and a device->host read of its result, download the state."""
+    K steps of real_field.rk2_step_table (in-place semantics) each followed by a
+    device->host read of the step's result, download the state.  The result is the
+    new phi's range (min, max, non-finite flag) that the step kernel folds as it
+    writes (the reference loop reads phi.min() and phi.max() every step), or with
+    --e2e-result observables the 10 observables of a separate reduction."""
     n = args.size
     N = n ** 3
     rng = np.random.default_rng(99)
@@ -431,7 +438,10 @@ def run_e2e(args, shape, seed, RF, observables, torch, dev, world):
         np.float32 if hdt == torch.float32 else np.float64)))
     if args.storage == "f32c":
         h_phi[1].zero_()
+    use_range = args.e2e_result == "range"
     h_obs = torch.empty((2, 10), dtype=torch.float64).pin_memory()
+    h_rng = torch.empty((2, 4), dtype=torch.int32).pin_memory()
+    prange = RF.PhiRange(dev) if use_range else None
     d_phi = torch.empty(host_shape, dtype=hdt, device=dev)
     d_pi = torch.empty_like(d_phi)
     d_pt, d_vt = torch.empty_like(d_phi), torch.empty_like(d_pi)
@@ -452,16 +462,24 @@ def run_e2e(args, shape, seed, RF, observables, torch, dev, world):
         T = temperature(s)
         RF.rk2_step_table(d_phi, d_pi, DT, DX, ETA, 1.0, None, d_pt, d_vt, 1.0, table, tmin, dinv,
                           NPHI, noise_scale=noise_scale(T), noise_step=s, seed=seed,
-                          vp_T=T, vp_T_min=Tmin, vp_T_dinv=Tdinv)
-        observables(d_phi, d_pi, out=d_obs, workspace=ws)
-        h_obs[s % 2].copy_(d_obs, non_blocking=True)
+                          vp_T=T, vp_T_min=Tmin, vp_T_dinv=Tdinv, phi_range=prange)
+        if use_range:
+            h_rng[s % 2].copy_(prange.last, non_blocking=True)
+        else:
+            observables(d_phi, d_pi, out=d_obs, workspace=ws)
+            h_obs[s % 2].copy_(d_obs, non_blocking=True)
         ready[s % 2].record(stream)
         if s > 0:
             read(s - 1)
 
     def read(s):
         ready[s % 2].synchronize()
-        seen.append(float(h_obs[s % 2, 4]))  # <phi^2> of step s
+        if use_range:
+            lo, hi, bad = RF.PhiRange.decode(h_rng[s % 2].numpy())
+            assert not bad, f"non-finite phi after step {s}"
+            seen.append(hi - lo)  # width of phi's range after step s
+        else:
+            seen.append(float(h_obs[s % 2, 4]))  # <phi^2> of step s
 
     # warm-up (untimed)
     d_phi.copy_(h_phi)
@@ -487,11 +505,14 @@ def run_e2e(args, shape, seed, RF, observables, torch, dev, world):
     wall = time.perf_counter() - t0
     ms = max_over_ranks(ev0.elapsed_time(ev1), world)
     state_bytes = 2 * h_phi.numel() * h_phi.element_size()
+    per_step = 16 if use_range else 80
+    what = ("the new phi's min, max and non-finite flag, folded by the step kernel itself"
+            if use_range else "the 10 observables of a separate reduction")
     return {"value": world * N * K / (ms / 1000.0), "unit": "site-updates/s",
-            "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": state_bytes / K + 80,
-            "wall_s": wall, "steps": K,
+            "h2d_bytes_per_step": state_bytes / K, "d2h_bytes_per_step": state_bytes / K + per_step,
+            "wall_s": wall, "steps": K, "result": args.e2e_result,
             "note": "state uploaded once and downloaded once per run (amortised per step); "
-                    "every step's 10 observables are read back to the host (the host reads "
+                    f"every step's result ({what}) is read back to the host (the host reads "
                     "step s-1's values after enqueuing step s)"}
 
 

@@ -152,6 +152,23 @@ int tipt_rk2_step_table_slab_planes(int storage, const void* phi, const void* pi
                                     int64_t plane_end, const tipt_step_params* sp,
                                     const tipt_vsource* vp, void* stream);
 
+/* tipt_rk2_step_table that also reports the range of the new phi, the
+ * reference loop's per-step phi.min() / phi.max() (R:3655-3660), without a
+ * pass of its own: the launch folds into range[0] the minimum and into
+ * range[1] the maximum of the new phi values (rounded to FP32; compensated
+ * FP32: hi + lo), each as the order-preserving code c(f) = f's bits with the
+ * sign bit set for f >= 0 and all bits inverted for f < 0 (decode: if the top
+ * bit is set clear it, else invert), and sets range[2] = 1 if a value is NaN
+ * or infinite.  The words must hold (0xFFFFFFFF, 0, 0) at the launch: the
+ * launch itself resets range_next (3 words, not overlapping range) to those
+ * values for the following launch, so alternating two buffers needs no
+ * further launches.  No reference counterpart as one call. */
+int tipt_rk2_step_table_range(int storage, const void* phi, const void* pi, void* phi_out,
+                              void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                              const tipt_step_params* sp, const tipt_vsource* vp,
+                              const void* noise, uint32_t* range, uint32_t* range_next,
+                              void* stream);
+
 /* rk2_step_table with the per-step scalars read on the device, for step loops
  * captured once into a CUDA graph and replayed (the reference's host loop
  * R:3619-3768 recomputes them each step on the host).  The step index is

@@ -1,0 +1,111 @@
+"""The step kernel's fused range output (the reference loop's per-step phi.min() /
+phi.max(), R:3655-3660): equal to the range of the field written, bitwise the
+same fields as the plain step, alternating buffers, and the non-finite flag."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+from thermal_inflation_phase_transition_b200 import real_field as RF  # noqa: E402
+from thermal_inflation_phase_transition_b200._common import table_source  # noqa: E402
+
+# (shape, storage): marching kernel (F32C, nz % 4 == 0), generic kernels otherwise
+CASES = [((16, 12, 32), "f32c"), ((9, 7, 5), "f32c"), ((16, 12, 32), "f64"),
+         ((9, 7, 5), "f32"), ((32, 24, 1), "f64")]
+
+
+def _state(shape, storage, seed):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    phi = 0.8 + 0.5 * torch.randn(shape, dtype=torch.float64, device="cuda", generator=g)
+    pi = 0.3 * torch.randn(shape, dtype=torch.float64, device="cuda", generator=g)
+    if storage == "f32c":
+        return RF.to_f32c(phi), RF.to_f32c(pi)
+    if storage == "f32":
+        return phi.float(), pi.float()
+    return phi, pi
+
+
+def _values32(t):
+    if t.dim() == 4:
+        return (t[0] + t[1]).float()          # the FP32 sum the kernel folds
+    return t.float()
+
+
+@pytest.mark.parametrize("shape,storage", CASES)
+def test_range_matches_written_field(shape, storage):
+    x = torch.linspace(-1.0, 4.0, 4096, dtype=torch.float64, device="cuda")
+    vs = table_source(x * x * x - x, -1.0, 4095 / 5.0, 4096)
+    phi, pi = _state(shape, storage, 3)
+    a = [phi.clone(), pi.clone(), torch.empty_like(phi), torch.empty_like(pi)]
+    b = [phi.clone(), pi.clone(), torch.empty_like(phi), torch.empty_like(pi)]
+    rng = RF.PhiRange()
+    for n in range(5):
+        RF.rk2_step_table_into(a[0], a[1], a[2], a[3], 0.05, 1.0, 1.0, 1.0, 1.0, vs,
+                               noise_scale=0.4, noise_step=n, seed=1, phi_range=rng)
+        RF.rk2_step_table_into(b[0], b[1], b[2], b[3], 0.05, 1.0, 1.0, 1.0, 1.0, vs,
+                               noise_scale=0.4, noise_step=n, seed=1)
+        torch.cuda.synchronize()
+        assert torch.equal(a[2], b[2]) and torch.equal(a[3], b[3])
+        lo, hi, bad = RF.PhiRange.decode(rng.last.cpu().numpy())
+        v = _values32(a[2])
+        assert lo == float(v.min()) and hi == float(v.max()) and not bad, n
+        a = [a[2], a[3], a[0], a[1]]
+        b = [b[2], b[3], b[0], b[1]]
+
+
+def test_range_flags_non_finite():
+    vs = table_source(torch.zeros(64, dtype=torch.float64, device="cuda"), 0.0, 1.0, 64)
+    phi, pi = _state((16, 12, 32), "f32c", 5)
+    phi[0, 3, 4, 8] = float("nan")            # planted in the input data
+    rng = RF.PhiRange()
+    po, qo = torch.empty_like(phi), torch.empty_like(pi)
+    RF.rk2_step_table_into(phi, pi, po, qo, 0.05, 1.0, 1.0, 1.0, 1.0, vs, phi_range=rng)
+    torch.cuda.synchronize()
+    assert RF.PhiRange.decode(rng.last.cpu().numpy())[2]
+    # the next launch starts from reset words: a finite state reports no flag
+    phi2, pi2 = _state((16, 12, 32), "f32c", 6)
+    RF.rk2_step_table_into(phi2, pi2, po, qo, 0.05, 1.0, 1.0, 1.0, 1.0, vs, phi_range=rng)
+    RF.rk2_step_table_into(phi2, pi2, po, qo, 0.05, 1.0, 1.0, 1.0, 1.0, vs, phi_range=rng)
+    torch.cuda.synchronize()
+    assert not RF.PhiRange.decode(rng.last.cpu().numpy())[2]
+
+
+def test_reference_signature_with_range():
+    """rk2_step_table (R:1875 signature) with phi_range= keeps its in-place semantics."""
+    shape = (16, 12, 32)
+    x = np.linspace(0.0, 3.0, 512)
+    tab = torch.from_numpy(2 * x - x ** 2).cuda()
+    phi, pi = _state(shape, "f64", 9)
+    rng = RF.PhiRange()
+    RF.rk2_step_table(phi, pi, 0.05, 1.0, 1.0, 1.0, None, torch.empty_like(phi),
+                      torch.empty_like(pi), 1.0, tab, 0.0, 511 / 3.0, 512, noise_scale=0.2,
+                      noise_step=0, phi_range=rng)
+    torch.cuda.synchronize()
+    lo, hi, _ = RF.PhiRange.decode(rng.last.cpu().numpy())
+    assert lo == float(phi.float().min()) and hi == float(phi.float().max())
+
+
+def test_table_source_keeps_its_table_alive():
+    """A V' source built from a temporary table tensor keeps the tensor: later
+    allocations of the same size (filled with NaN) do not reach the table the
+    launches read."""
+    shape = (32, 32, 64)
+    x = torch.linspace(-1.0, 4.0, 4096, dtype=torch.float64, device="cuda")
+    kept = x * x * x - x
+    vs_kept = table_source(kept, -1.0, 4095 / 5.0, 4096)
+    vs_temp = table_source(x * x * x - x, -1.0, 4095 / 5.0, 4096)
+    junk = [torch.full((4096,), float("nan"), dtype=torch.float64, device="cuda")
+            for _ in range(64)]
+    phi, pi = _state(shape, "f32c", 3)
+    outs = []
+    for vs in (vs_kept, vs_temp):
+        po = torch.full_like(phi, 12345.0)
+        qo = torch.full_like(pi, 12345.0)
+        RF.rk2_step_table_into(phi, pi, po, qo, 0.05, 1.0, 1.0, 1.0, 1.0, vs)
+        outs.append((po, qo))
+    torch.cuda.synchronize()
+    assert torch.isfinite(outs[1][0]).all()
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+    del junk

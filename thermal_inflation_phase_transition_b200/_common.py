@@ -65,7 +65,9 @@ def table_source(vp_table, vp_tmin, vp_dinv, vp_npts, T=None, T_min=None, T_dinv
     """V' source from the reference's table arguments (R:1885-1888).
 
     A 1-D float64 CUDA tensor is the reference's table; a 2-D [nT][npts] tensor
-    is the (phi, T) table, blended at T (T_min, T_dinv give its T grid)."""
+    is the (phi, T) table, blended at T (T_min, T_dinv give its T grid).  The
+    source holds a reference to the table tensor, so a source kept for later
+    launches never points at freed memory."""
     need_cuda(vp_table, names=["vp_table"])
     if vp_table.dtype != torch.float64:
         raise TypeError("vp_table must be float64 (the table is built in FP64)")
@@ -73,16 +75,20 @@ def table_source(vp_table, vp_tmin, vp_dinv, vp_npts, T=None, T_min=None, T_dinv
     if vp_table.dim() == 1:
         if vp_table.numel() < npts or npts < 2:
             raise ValueError("vp_npts out of range for vp_table")
-        return L.VSource(L.VP_TABLE, npts, vp_table.data_ptr(), float(vp_tmin), float(vp_dinv),
-                         0, 0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+        vs = L.VSource(L.VP_TABLE, npts, vp_table.data_ptr(), float(vp_tmin), float(vp_dinv),
+                       0, 0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+        vs._keep = vp_table
+        return vs
     if vp_table.dim() == 2:
         if T is None or T_min is None or T_dinv is None:
             raise ValueError("a 2-D table needs T, T_min and T_dinv")
         if vp_table.shape[1] != npts:
             raise ValueError("vp_npts must equal the table's phi extent")
-        return L.VSource(L.VP_TABLE2D, npts, vp_table.data_ptr(), float(vp_tmin), float(vp_dinv),
-                         int(vp_table.shape[0]), 0, float(T_min), float(T_dinv), float(T), 0.0,
-                         0.0, 0.0)
+        vs = L.VSource(L.VP_TABLE2D, npts, vp_table.data_ptr(), float(vp_tmin), float(vp_dinv),
+                       int(vp_table.shape[0]), 0, float(T_min), float(T_dinv), float(T), 0.0,
+                       0.0, 0.0)
+        vs._keep = vp_table
+        return vs
     raise ValueError("vp_table must be 1-D or 2-D")
 
 

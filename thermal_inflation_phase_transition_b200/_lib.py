@@ -73,6 +73,8 @@ _SIGS = {
     "tipt_generate_noise_field": [_i, _p, _i64, _i64, _i64, _d, _u64, _u64, _u64, _i, _p],
     "tipt_rk2_step_table": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
                             C.POINTER(VSource), _p, _p],
+    "tipt_rk2_step_table_range": [_i, _p, _p, _p, _p, _i64, _i64, _i64, C.POINTER(StepParams),
+                                  C.POINTER(VSource), _p, _p, _p, _p],
     "tipt_rk2_fused_table": [_i, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
                              C.POINTER(StepParams), C.POINTER(VSource), C.POINTER(VSource), _p,
                              _p],

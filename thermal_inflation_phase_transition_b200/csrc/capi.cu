@@ -216,6 +216,31 @@ int tipt_rk2_step_table(int storage, const void* phi, const void* pi, void* phi_
     return launch_real_stage(storage, p, (cudaStream_t)stream);
 }
 
+int tipt_rk2_step_table_range(int storage, const void* phi, const void* pi, void* phi_out,
+                              void* pi_out, int64_t nx, int64_t ny, int64_t nz,
+                              const tipt_step_params* sp, const tipt_vsource* vp,
+                              const void* noise, uint32_t* range, uint32_t* range_next,
+                              void* stream) {
+    int rc;
+    if ((rc = check_state(storage, phi, pi, phi_out, pi_out, nx, ny, nz))) return rc;
+    if (!sp) return fail(TIPT_ERR_ARG, "step params are NULL");
+    if ((rc = check_vsource(vp, "vp"))) return rc;
+    if (noise && (rc = check_ptr(noise, storage == TIPT_F32 ? 4 : 8, "noise"))) return rc;
+    if ((rc = check_ptr(range, 4, "range")) || (rc = check_ptr(range_next, 4, "range_next")))
+        return rc;
+    if (overlap(range, range_next, 12)) return fail(TIPT_ERR_ARG, "range and range_next overlap");
+    RealStageParams p = stage_params(phi, pi, phi_out, pi_out, nx, ny, nz, sp, vp);
+    p.h1 = 0.5 * sp->dt;
+    p.h2 = sp->dt;
+    p.noise = noise;
+    p.nfac = 1.0;
+    p.ns_eff = sp->noise_scale;
+    p.mul = kPass2Mul;
+    p.range = reinterpret_cast<unsigned int*>(range);
+    p.range_next = reinterpret_cast<unsigned int*>(range_next);
+    return launch_real_stage(storage, p, (cudaStream_t)stream);
+}
+
 int tipt_rk2_step_table_slab_planes(int storage, const void* phi, const void* pi, void* phi_out,
                                     void* pi_out, int64_t nx_local, int64_t ny, int64_t nz,
                                     int64_t i_lo, int64_t nx_global, int64_t plane_begin,

@@ -372,11 +372,12 @@ __global__ void __maxnreg__(kMarchRegs)
 // 16-byte vector per plane and neighbour) and evaluates them as two site
 // pairs in the lanes of the packed FP32x2 instructions; the stencil sums run
 // in the order of the generic kernel, so results are bitwise identical.
-template <bool WIDE, bool TH>
+template <bool WIDE, bool TH, bool RG>
 __global__ void __maxnreg__(kMarchRegs)
     rk2_stage_march_f32c(RealStageParams p_in, MarchGeom g) {
     RealStageParams p = p_in;
     resolve_schedule(p);
+    if constexpr (RG) reset_next_range(p);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     float* s_tab = reinterpret_cast<float*>(smem);
@@ -462,6 +463,7 @@ __global__ void __maxnreg__(kMarchRegs)
     const int64_t N = (int64_t)n0 * n1 * n2;
     const int orow = r * pitch, urow = (r - 1) * pitch, drow = (r + 1) * pitch;
 
+    RangeAcc racc;
     RingPos pm{0, 0};
     for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
         const int ic = item / g.nJB;
@@ -566,6 +568,14 @@ __global__ void __maxnreg__(kMarchRegs)
             *reinterpret_cast<float4*>(phi_out + N + rowoff) = make_float4(o[0][1].x, o[0][1].y, o[1][1].x, o[1][1].y);
             *reinterpret_cast<float4*>(pi_out + rowoff) = make_float4(o[0][2].x, o[0][2].y, o[1][2].x, o[1][2].y);
             *reinterpret_cast<float4*>(pi_out + N + rowoff) = make_float4(o[0][3].x, o[0][3].y, o[1][3].x, o[1][3].y);
+            if constexpr (RG) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float2 v = v_add(o[h][0], o[h][1]);
+                    racc.fold(v.x);
+                    racc.fold(v.y);
+                }
+            }
             pm = pc;
             pc = pp;
             pp.next(NS);
@@ -577,6 +587,7 @@ __global__ void __maxnreg__(kMarchRegs)
         }
         pm = pp;
     }
+    if constexpr (RG) racc.flush(p.range);
 }
 
 // ------------------------------- alternative integrators, F32C marching ----
@@ -1189,6 +1200,7 @@ static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, 
 
 bool march_supported(int storage, const RealStageParams& p) {
     if (storage != TIPT_F32C && storage != TIPT_F64) return false;
+    if (storage == TIPT_F64 && p.range) return false;  // the generic kernel folds the range
     const uintptr_t a = reinterpret_cast<uintptr_t>(p.phi) | reinterpret_cast<uintptr_t>(p.pi) |
                         reinterpret_cast<uintptr_t>(p.phi_out) |
                         reinterpret_cast<uintptr_t>(p.pi_out);
@@ -1229,12 +1241,22 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
     // 64-bit noise-key sites when an index (array + offset) can exceed 32 bits
     const bool wide = (int64_t)p.n0 * p.n1 * p.n2 + (p.site_offset > 0 ? p.site_offset : 0) >
                       0xFFFFFFFFll;
-    if (storage == TIPT_F32C && p.vkind == TIPT_VP_THERMAL)
-        return wide ? launch_march_k(rk2_stage_march_f32c<true, true>, p, g, smem, st)
-                    : launch_march_k(rk2_stage_march_f32c<false, true>, p, g, smem, st);
-    if (storage == TIPT_F32C)
-        return wide ? launch_march_k(rk2_stage_march_f32c<true, false>, p, g, smem, st)
-                    : launch_march_k(rk2_stage_march_f32c<false, false>, p, g, smem, st);
+    if (storage == TIPT_F32C && p.vkind == TIPT_VP_THERMAL) {
+        if (p.range)
+            return wide ? launch_march_k(rk2_stage_march_f32c<true, true, true>, p, g, smem, st)
+                        : launch_march_k(rk2_stage_march_f32c<false, true, true>, p, g, smem, st);
+        return wide ? launch_march_k(rk2_stage_march_f32c<true, true, false>, p, g, smem, st)
+                    : launch_march_k(rk2_stage_march_f32c<false, true, false>, p, g, smem, st);
+    }
+    if (storage == TIPT_F32C) {
+        if (p.range)
+            return wide ? launch_march_k(rk2_stage_march_f32c<true, false, true>, p, g, smem, st)
+                        : launch_march_k(rk2_stage_march_f32c<false, false, true>, p, g, smem, st);
+        return wide ? launch_march_k(rk2_stage_march_f32c<true, false, false>, p, g, smem, st)
+                    : launch_march_k(rk2_stage_march_f32c<false, false, false>, p, g, smem, st);
+    }
+    if (storage == TIPT_F64 && p.range)
+        return fail(TIPT_ERR_UNSUPPORTED, "FP64 marching stage takes no range output");
     if (storage == TIPT_F64)
         return wide ? launch_march_k(rk2_stage_march<TIPT_F64, true>, p, g, smem, st)
                     : launch_march_k(rk2_stage_march<TIPT_F64, false>, p, g, smem, st);

@@ -10,10 +10,12 @@
 
 namespace tipt {
 
-template <int S, bool TH>
+template <int S, bool TH, bool RG>
 __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
     RealStageParams p = p_in;
     resolve_schedule(p);
+    if constexpr (RG) reset_next_range(p);
+    RangeAcc racc;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using TT = typename std::conditional<S == TIPT_F32C, float, double>::type;
     TT* s_tab = reinterpret_cast<TT*>(smem_raw);
@@ -50,6 +52,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
                        site_noise<double>(p, (uint64_t)(s + p.site_offset)), a, b);
             static_cast<double*>(p.phi_out)[s] = a;
             static_cast<double*>(p.pi_out)[s] = b;
+            if constexpr (RG) racc.fold((float)a);
         } else if constexpr (S == TIPT_F32) {
             const float* phi = static_cast<const float*>(p.phi);
             const float* pi = static_cast<const float*>(p.pi);
@@ -64,6 +67,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
                        site_noise<float>(p, (uint64_t)(s + p.site_offset)), a, b);
             static_cast<float*>(p.phi_out)[s] = a;
             static_cast<float*>(p.pi_out)[s] = b;
+            if constexpr (RG) racc.fold(a);
         } else {
             // planar {hi, lo}: hi plane at [0, N), lo plane at [N, 2N)
             const float* phi = static_cast<const float*>(p.phi);
@@ -92,8 +96,10 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
             po[N + s] = b;
             vo[s] = c;
             vo[N + s] = d;
+            if constexpr (RG) racc.fold(__fadd_rn(a, b));
         }
     }
+    if constexpr (RG) racc.flush(p.range);
 }
 
 // Bytes of shared memory the V' row needs for storage S (0 if polynomial).
@@ -115,7 +121,9 @@ int num_sms() {
 
 template <int S>
 static int launch_generic(RealStageParams p, int64_t smem, cudaStream_t st) {
-    auto kern = p.vkind == TIPT_VP_THERMAL ? rk2_stage_generic<S, true> : rk2_stage_generic<S, false>;
+    auto kern = p.vkind == TIPT_VP_THERMAL
+                    ? (p.range ? rk2_stage_generic<S, true, true> : rk2_stage_generic<S, true, false>)
+                    : (p.range ? rk2_stage_generic<S, false, true> : rk2_stage_generic<S, false, false>);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);

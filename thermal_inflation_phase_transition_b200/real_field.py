@@ -63,13 +63,15 @@ def generate_noise_field(noise, scale, seed, *, mul=K_PASS2, hash_seed=0, compon
 
 def rk2_step_table(phi, pi, dt, dx, eta_eff, mu, noise, phi_tmp, pi_tmp, inv_a2, vp_table,
                    vp_tmin, vp_dinv, vp_npts, *, noise_scale=0.0, noise_step=0, seed=0,
-                   vp_T=None, vp_T_min=None, vp_T_dinv=None):
+                   vp_T=None, vp_T_min=None, vp_T_dinv=None, phi_range=None):
     """R:1875 rk2_step_table: one midpoint RK2 step, updating phi and pi in place.
 
     The fused kernel writes the new state into phi_tmp / pi_tmp and the tensors
     then exchange storages, so on return phi, pi hold the new state (the
     reference's in-place result) and phi_tmp, pi_tmp hold the old one (the
-    reference leaves the midpoint state there; both are scratch)."""
+    reference leaves the midpoint state there; both are scratch).  ``phi_range``
+    (a PhiRange) receives the new phi's minimum and maximum from the same launch
+    (the reference's per-step phi.min() / phi.max())."""
     st = storage_of(phi)
     need_cuda(phi, pi, phi_tmp, pi_tmp, names=["phi", "pi", "phi_tmp", "pi_tmp"])
     same_layout(phi, pi, phi_tmp, pi_tmp, names=["pi", "phi_tmp", "pi_tmp"])
@@ -77,8 +79,13 @@ def rk2_step_table(phi, pi, dt, dx, eta_eff, mu, noise, phi_tmp, pi_tmp, inv_a2,
     nx, ny, nz = dims_of(phi)
     vs = table_source(vp_table, vp_tmin, vp_dinv, vp_npts, vp_T, vp_T_min, vp_T_dinv)
     sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
-    L.call("tipt_rk2_step_table", st, ptr(phi), ptr(pi), ptr(phi_tmp), ptr(pi_tmp), nx, ny, nz,
-           sp, vs, ptr(noise), stream_handle())
+    if phi_range is None:
+        L.call("tipt_rk2_step_table", st, ptr(phi), ptr(pi), ptr(phi_tmp), ptr(pi_tmp), nx, ny,
+               nz, sp, vs, ptr(noise), stream_handle())
+    else:
+        cur, nxt = phi_range.next_pair()
+        L.call("tipt_rk2_step_table_range", st, ptr(phi), ptr(pi), ptr(phi_tmp), ptr(pi_tmp), nx,
+               ny, nz, sp, vs, ptr(noise), ptr(cur), ptr(nxt), stream_handle())
     swap_storage(phi, phi_tmp)
     swap_storage(pi, pi_tmp)
 
@@ -110,15 +117,60 @@ def rk2_step_inline(phi, pi, dt, dx, eta_eff, T, mu, lam_val, mphi_val, bosonMas
 
 
 def rk2_step_table_into(phi, pi, phi_out, pi_out, dt, dx, eta_eff, mu, inv_a2, vsource, *,
-                        noise=None, noise_scale=0.0, noise_step=0, seed=0, stream=None):
+                        noise=None, noise_scale=0.0, noise_step=0, seed=0, stream=None,
+                        phi_range=None):
     """Ping-pong form of rk2_step_table: (phi, pi) -> (phi_out, pi_out), no swap.
 
-    ``vsource`` is a prepared V' source (``table_source`` / ``poly_source``)."""
+    ``vsource`` is a prepared V' source (``table_source`` / ``poly_source``);
+    ``phi_range`` (a PhiRange) receives the range of phi_out from the same launch."""
     st = storage_of(phi)
     nx, ny, nz = dims_of(phi)
     sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
-    L.call("tipt_rk2_step_table", st, ptr(phi), ptr(pi), ptr(phi_out), ptr(pi_out), nx, ny, nz,
-           sp, vsource, ptr(noise), stream_handle(stream))
+    if phi_range is None:
+        L.call("tipt_rk2_step_table", st, ptr(phi), ptr(pi), ptr(phi_out), ptr(pi_out), nx, ny,
+               nz, sp, vsource, ptr(noise), stream_handle(stream))
+        return
+    cur, nxt = phi_range.next_pair()
+    L.call("tipt_rk2_step_table_range", st, ptr(phi), ptr(pi), ptr(phi_out), ptr(pi_out), nx, ny,
+           nz, sp, vsource, ptr(noise), ptr(cur), ptr(nxt), stream_handle(stream))
+
+
+class PhiRange:
+    """Range of phi after each step, folded by the step kernel itself (the reference
+    loop reads phi.min() and phi.max() every step, R:3655-3660, for its V' table
+    check).  Two 3-word device buffers alternate: a step writes one and resets the
+    other for the next step, so reading a step's range needs no extra launch.
+
+        rng = PhiRange(device)
+        rk2_step_table_into(phi, pi, po, qo, ..., vs, phi_range=rng)
+        lo, hi, nonfinite = rng.decode(rng.last.cpu())     # or copy rng.last to a host buffer
+    """
+
+    def __init__(self, device="cuda"):
+        self.buf = torch.empty((2, 4), dtype=torch.int32, device=device)
+        self.buf[:, 0] = -1          # 0xFFFFFFFF: minimum code not yet seen
+        self.buf[:, 1:] = 0
+        self.k = 0
+        self.last = self.buf[1]
+
+    def next_pair(self):
+        """(this step's words, the next step's words) and advance."""
+        cur, nxt = self.buf[self.k], self.buf[self.k ^ 1]
+        self.k ^= 1
+        self.last = cur
+        return cur, nxt
+
+    @staticmethod
+    def decode(words):
+        """(min, max, nonfinite) from a step's 3 (or 4) int32 words on the host."""
+        import numpy as np
+        w = np.asarray(words, dtype=np.int64).astype(np.uint32)
+
+        def f(c):
+            c = int(c)
+            u = c & 0x7FFFFFFF if c & 0x80000000 else (~c) & 0xFFFFFFFF
+            return float(np.array([u], np.uint32).view(np.float32)[0])
+        return f(w[0]), f(w[1]), bool(w[2])
 
 
 def rk2_fused_table(phi, pi, dt, dx, eta_eff, mu, noise, phi_tmp, pi_tmp, inv_a2, vp_table_T,

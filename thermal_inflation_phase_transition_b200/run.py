@@ -253,6 +253,15 @@ class Run:
         self.tab_mid = self.tp.table(T_mid, lo, hi, TABLE_SIZE)
         self.t_lo, self.t_hi, self.T_last = lo, hi, T
 
+    def _phi_range(self):
+        """(min, max) of phi: from the previous step's fused range when it has one
+        (rk2_nonfused), else two reductions."""
+        if self.prange is not None and self._range_valid:
+            lo, hi, _ = RF.PhiRange.decode(self.prange.last.cpu().numpy())
+            return lo, hi
+        v = self._values(self.phi)
+        return float(v.min()), float(v.max())
+
     def _need_rebuild(self, n, T):
         if self.tab is None:
             return True
@@ -260,8 +269,8 @@ class Run:
             return True
         if (n - self.n_start) % self.args.range_check_every:
             return False
-        v = self._values(self.phi)
-        return float(v.min()) < self.t_lo or float(v.max()) > self.t_hi
+        lo, hi = self._phi_range()
+        return lo < self.t_lo or hi > self.t_hi
 
     # ------------------------------------------------------------- loop ---
     def scalars(self, n):
@@ -300,7 +309,8 @@ class Run:
         RF.generate_noise_field(self.noise, ns, n)                            # R:3752-3757
         if self.integrator == "rk2_nonfused":
             RF.rk2_step_table(self.phi, self.pi, dt, dx, eta_eff, mu, self.noise, self.mid[0],
-                              self.mid[1], inv_a2, *tab)
+                              self.mid[1], inv_a2, *tab, phi_range=self.prange)
+            self._range_valid = True
         elif self.integrator == "rk2_nonfused_inline":
             RF.rk2_step_inline(self.phi, self.pi, dt, dx, eta_eff, T, mu, *c, self.noise,
                                self.mid[0], self.mid[1], inv_a2, splines=self.tp)
@@ -324,6 +334,10 @@ class Run:
         ndt = torch.float32 if a.storage == "f32" else torch.float64
         self.noise = torch.empty(self.shape, dtype=ndt, device=self.dev)
         self.tab = None
+        # the default integrator's step folds phi's range as it writes (the
+        # per-step phi.min() / phi.max() of the table check, R:3655-3660)
+        self.prange = RF.PhiRange(self.dev) if self.integrator == "rk2_nonfused" else None
+        self._range_valid = False
         writer = SnapshotWriter(self.state_path, checkpoint_every=CHECKPOINT_EVERY)
         dense_on = a.phi_threshold is not None and a.steps_dense is not None
         dense_active = False

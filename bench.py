@@ -155,7 +155,7 @@ def barrier(world):
 
 
 # -------------------------------------------------------------- CPU arms ---
-def cpu_oracle_rate(n_side, budget_s=12.0, max_steps=20, shape=None):
+def cpu_oracle_rate(n_side, budget_s=12.0, max_steps=20, shape=None, warmup=1):
     """Site-updates/s of the CPU restatement (oracle/, OpenMP, all host threads) on
     the same step: FP64 midpoint RK2, blended 2-D table row, inline hash noise."""
     from oracle import oracle as O
@@ -173,11 +173,13 @@ def cpu_oracle_rate(n_side, budget_s=12.0, max_steps=20, shape=None):
         O.rk2_step_table(phi, pi, DT, DX, ETA, 1.0, None, *tmp, 1.0, row, tmin, dinv, NPHI,
                          noise_scale=noise_scale(T), noise_step=n, noise_seed=1)
 
-    one(0)
+    for w in range(max(1, warmup)):
+        one(w)
+    w0 = max(1, warmup)
     t0 = time.perf_counter()
     n = 0
     while n < max_steps and (time.perf_counter() - t0) < budget_s:
-        one(n + 1)
+        one(w0 + n)
         n += 1
     el = time.perf_counter() - t0
     return n * phi.size / el, n, O.num_threads(), shape
@@ -191,17 +193,18 @@ def run_reference(args, world, rank):
         return
     n = args.size
     shape = (n, n, n)
+    warm = max(3, args.warmup)
     rate, steps, threads, shp = cpu_oracle_rate(n, budget_s=max(30.0, 1.0), max_steps=max(
-        args.steps, 1), shape=shape)
+        args.steps, 1), shape=shape, warmup=warm)
     line = {
         "metric": METRIC, "value": rate, "unit": "site-updates/s", "impl": "reference",
-        "n_gpus": args.gpus, "steps": steps, "warmup": 1,
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm,
         "ms_per_step": 1000.0 * n ** 3 / rate, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload_name(n, "f64"), "lattice": [n, n, n]},
         "cpu_baseline": {"value": rate, "unit": "site-updates/s", "cores": threads,
                          "kind": "port",
-                         "sample": f"{steps} full {n}^3 FP64 steps (after 1 warm-up step) of "
+                         "sample": f"{steps} full {n}^3 FP64 steps (after {warm} warm-up steps) of "
                                    "the CPU restatement, OpenMP over all host threads"},
         "e2e": {"value": rate, "unit": "site-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},

@@ -32,6 +32,8 @@ def _state(shape, storage, seed):
     pi = 0.4 * torch.randn(shape, dtype=torch.float64, device=DEV, generator=g)
     if storage == "f32c":
         return RF.to_f32c(phi), RF.to_f32c(pi)
+    if storage == "f32":
+        return phi.float(), pi.float()
     return phi, pi
 
 
@@ -66,7 +68,7 @@ SHAPES = [(16, 8, 64), (7, 8, 48), (70, 8, 16), (32, 32, 32), (9, 4, 512), (24, 
 
 
 @pytest.mark.parametrize("shape", SHAPES)
-@pytest.mark.parametrize("storage", ["f32c", "f64"])
+@pytest.mark.parametrize("storage", ["f32c", "f64", "f32"])
 def test_march_equals_generic(shape, storage):
     ref = _run(1, shape, storage)
     got = _run(2, shape, storage)

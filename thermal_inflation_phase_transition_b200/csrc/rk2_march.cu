@@ -141,26 +141,49 @@ struct MarchElem<TIPT_F64> {
     using E = double;
     using TT = double;
 };
+// The reference's float32 mode: float32 planes, the FP64 V' table (R:1914-1933).
+template <>
+struct MarchElem<TIPT_F32> {
+    using E = float;
+    using TT = double;
+};
 
-// 16-byte pair loads/stores of two consecutive 8-byte elements.
+// Pair loads/stores of two consecutive elements (16 bytes for 8-byte elements,
+// 8 bytes for 4-byte ones).
 template <typename E>
 __device__ __forceinline__ void ld_pair_s(const E* p, E& a, E& b) {
-    const float4 v = *reinterpret_cast<const float4*>(p);
-    a = *reinterpret_cast<const E*>(&v.x);
-    b = *reinterpret_cast<const E*>(&v.z);
+    if constexpr (sizeof(E) == 8) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        a = *reinterpret_cast<const E*>(&v.x);
+        b = *reinterpret_cast<const E*>(&v.z);
+    } else {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        a = v.x;
+        b = v.y;
+    }
 }
 template <typename E>
 __device__ __forceinline__ void st_pair_g(E* p, const E& a, const E& b) {
-    float4 v;
-    *reinterpret_cast<E*>(&v.x) = a;
-    *reinterpret_cast<E*>(&v.z) = b;
-    *reinterpret_cast<float4*>(p) = v;
+    if constexpr (sizeof(E) == 8) {
+        float4 v;
+        *reinterpret_cast<E*>(&v.x) = a;
+        *reinterpret_cast<E*>(&v.z) = b;
+        *reinterpret_cast<float4*>(p) = v;
+    } else {
+        *reinterpret_cast<float2*>(p) = make_float2(a, b);
+    }
 }
 template <typename E>
 __device__ __forceinline__ void ld_pair_g(const E* p, E& a, E& b) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-    a = *reinterpret_cast<const E*>(&v.x);
-    b = *reinterpret_cast<const E*>(&v.z);
+    if constexpr (sizeof(E) == 8) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+        a = *reinterpret_cast<const E*>(&v.x);
+        b = *reinterpret_cast<const E*>(&v.z);
+    } else {
+        const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+        a = v.x;
+        b = v.y;
+    }
 }
 
 template <int S>
@@ -169,7 +192,8 @@ __device__ __forceinline__ void site_update(const RealStageParams& p, const void
                                             const typename MarchElem<S>::E pv[7], double noise,
                                             typename MarchElem<S>::E& a,
                                             typename MarchElem<S>::E& b) {
-    update_f64(p, static_cast<const double*>(s_tab), ph, pv, noise, a, b);
+    if constexpr (S == TIPT_F64) update_f64(p, static_cast<const double*>(s_tab), ph, pv, noise, a, b);
+    else update_f32(p, static_cast<const double*>(s_tab), ph, pv, noise, a, b);
 }
 
 // Launch bounds of the two block-size classes: up to 256 consumer threads
@@ -310,7 +334,7 @@ __global__ void __maxnreg__(kMarchRegs)
                     uint64_t site;
                     if constexpr (WIDE) site = (uint64_t)(rowoff + p.site_offset + col);
                     else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)col;
-                    nz[h][u] = site_noise<double>(p, site);
+                    nz[h][u] = site_noise<E>(p, site);
                 }
             }
             if (!mbar_wait(&full[pp.stage], pp.phase)) {
@@ -1140,7 +1164,7 @@ static int ctas_per_sm(const MarchGeom& g, int tpr) {
 // Shared-memory ring layout of a storage: FP64 -> one 8-byte plane per field;
 // F32C -> two 4-byte planes (hi, lo) per field.
 static int layout_es(int storage) { return storage == TIPT_F64 ? 8 : 4; }
-static int layout_planes(int storage) { return storage == TIPT_F64 ? 1 : 2; }
+static int layout_planes(int storage) { return storage == TIPT_F32C ? 2 : 1; }
 
 // Tile geometry of the real-field marching kernels: n1 x n2 rows, nplanes
 // planes to compute, `comps` component planes of `es`-byte elements per ring
@@ -1199,8 +1223,8 @@ static bool geometry(int storage, const RealStageParams& p, int64_t smem_table, 
 }
 
 bool march_supported(int storage, const RealStageParams& p) {
-    if (storage != TIPT_F32C && storage != TIPT_F64) return false;
-    if (storage == TIPT_F64 && p.range) return false;  // the generic kernel folds the range
+    if (storage != TIPT_F32C && storage != TIPT_F64 && storage != TIPT_F32) return false;
+    if (storage != TIPT_F32C && p.range) return false;  // the generic kernel folds the range
     const uintptr_t a = reinterpret_cast<uintptr_t>(p.phi) | reinterpret_cast<uintptr_t>(p.pi) |
                         reinterpret_cast<uintptr_t>(p.phi_out) |
                         reinterpret_cast<uintptr_t>(p.pi_out);
@@ -1255,12 +1279,15 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
         return wide ? launch_march_k(rk2_stage_march_f32c<true, false, false>, p, g, smem, st)
                     : launch_march_k(rk2_stage_march_f32c<false, false, false>, p, g, smem, st);
     }
-    if (storage == TIPT_F64 && p.range)
-        return fail(TIPT_ERR_UNSUPPORTED, "FP64 marching stage takes no range output");
+    if (storage != TIPT_F32C && p.range)
+        return fail(TIPT_ERR_UNSUPPORTED, "the FP64 / float32 marching stage takes no range output");
     if (storage == TIPT_F64)
         return wide ? launch_march_k(rk2_stage_march<TIPT_F64, true>, p, g, smem, st)
                     : launch_march_k(rk2_stage_march<TIPT_F64, false>, p, g, smem, st);
-    return fail(TIPT_ERR_STORAGE, "marching kernel takes F32C or F64");
+    if (storage == TIPT_F32)
+        return wide ? launch_march_k(rk2_stage_march<TIPT_F32, true>, p, g, smem, st)
+                    : launch_march_k(rk2_stage_march<TIPT_F32, false>, p, g, smem, st);
+    return fail(TIPT_ERR_STORAGE, "marching kernel takes F32C, F64 or F32");
 }
 
 // The alternative integrators on the marching ring: compensated FP32,

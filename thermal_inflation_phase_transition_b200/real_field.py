@@ -144,7 +144,10 @@ class PhiRange:
         rng = PhiRange(device)
         rk2_step_table_into(phi, pi, po, qo, ..., vs, phi_range=rng)
         lo, hi, nonfinite = rng.decode(rng.last.cpu())     # or copy rng.last to a host buffer
-    """
+
+    A CUDA graph bakes the two buffers into its launches: capture an even number of
+    steps per graph, so that each buffer is written by one step and reset by the
+    other on every replay."""
 
     def __init__(self, device="cuda"):
         self.buf = torch.empty((2, 4), dtype=torch.int32, device=device)

@@ -133,15 +133,18 @@ def test_rk2_step_table_f32c_vs_fp64(golden, tag):
     assert np.abs(pi - ref_pi).max() <= 2e-6 * np.abs(ref_pi).max()
 
 
-@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 3, 1), (5, 1, 7), (1, 1, 9), (40, 36, 34)])
-@pytest.mark.parametrize("storage", ["f64", "f32c"])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 3, 1), (5, 1, 7), (1, 1, 9), (40, 36, 34),
+                                   (3, 8, 32)])
+@pytest.mark.parametrize("storage", ["f64", "f32c", "f32"])
 def test_rk2_edge_shapes_vs_oracle(shape, storage):
     rng = np.random.default_rng(7)
     phi0 = rng.normal(0.5, 0.6, shape)
     pi0 = rng.normal(0.0, 0.3, shape)
     tab, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.01), 0.0, 3.0, 1024)
+    if storage == "f32":  # the oracle's float32 mode runs on float32 arrays
+        phi0, pi0 = phi0.astype(np.float32), pi0.astype(np.float32)
     a, b = phi0.copy(), pi0.copy()
-    tmp = [np.empty(shape), np.empty(shape)]
+    tmp = [np.empty(shape, a.dtype), np.empty(shape, a.dtype)]
     phi, pi = as_state(phi0, storage), as_state(pi0, storage)
     pt, vt = torch.empty_like(phi), torch.empty_like(pi)
     for n in range(3):
@@ -150,7 +153,7 @@ def test_rk2_edge_shapes_vs_oracle(shape, storage):
         RF.rk2_step_table(phi, pi, 0.05, 1.0, 0.9, 1.0, None, pt, vt, 1.0, cu(tab), tmin, dinv,
                           1024, noise_scale=0.3, noise_step=n, seed=3)
     torch.cuda.synchronize()
-    tol = 1e-13 if storage == "f64" else 2e-6
+    tol = {"f64": 1e-13, "f32c": 2e-6, "f32": 1e-6}[storage]
     np.testing.assert_allclose(to_np(phi), a, rtol=0, atol=tol * max(1.0, np.abs(a).max()))
     np.testing.assert_allclose(to_np(pi), b, rtol=0, atol=tol * max(1.0, np.abs(b).max()))
 

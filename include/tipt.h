@@ -236,6 +236,19 @@ int tipt_complex_rk2_step_table(int storage, const void* phi1, const void* phi2,
                                 const tipt_vsource* vp, const tipt_complex_terms* ct,
                                 const void* noise1, const void* noise2, void* stream);
 
+/* tipt_complex_rk2_step_table that also reports the range of the new |Phi|
+ * (the complex loop's per-step rho check, C:4263-4288) without a pass of its
+ * own: range / range_next as in tipt_rk2_step_table_range, folded from
+ * rho = sqrt(phi1^2 + phi2^2) of the values written (FP32; compensated FP32:
+ * hi + lo; FP64: computed in FP64, rounded to FP32). */
+int tipt_complex_rk2_step_table_range(int storage, const void* phi1, const void* phi2,
+                                      const void* pi1, const void* pi2, void* phi1_out,
+                                      void* phi2_out, void* pi1_out, void* pi2_out, int64_t nx,
+                                      int64_t ny, int64_t nz, const tipt_step_params* sp,
+                                      const tipt_vsource* vp, const tipt_complex_terms* ct,
+                                      const void* noise1, const void* noise2, uint32_t* range,
+                                      uint32_t* range_next, void* stream);
+
 /* Complex rk2_fused_table (C:1789-2064): two dt/2 midpoint halves, the first
  * with vp_T, the second with vp_Tm; array noise adds 0.5*noise_a in each half.
  * With noise1 == noise2 == NULL the halves use the inline hash pairs of the

@@ -109,3 +109,51 @@ def test_table_source_keeps_its_table_alive():
     assert torch.isfinite(outs[1][0]).all()
     assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
     del junk
+
+
+# complex field: the range of |Phi| (C:4263-4288)
+CPLX_CASES = [((8, 8, 256), "f32c"), ((9, 7, 5), "f32c"), ((9, 7, 5), "f64"), ((9, 7, 5), "f32")]
+
+
+def _cstate(shape, storage, seed):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    st = [0.6 * torch.randn(shape, dtype=torch.float64, device="cuda", generator=g)
+          for _ in range(4)]
+    if storage == "f32c":
+        return [RF.to_f32c(a) for a in st]
+    if storage == "f32":
+        return [a.float() for a in st]
+    return st
+
+
+def _rho32(a, b):
+    if a.dim() == 4:
+        a, b = (a[0] + a[1]).float(), (b[0] + b[1]).float()
+        return torch.sqrt(a * a + b * b)
+    if a.dtype == torch.float32:
+        return torch.sqrt(a * a + b * b)
+    return torch.sqrt(a * a + b * b).float()
+
+
+@pytest.mark.parametrize("shape,storage", CPLX_CASES)
+def test_complex_rho_range(shape, storage):
+    from thermal_inflation_phase_transition_b200 import complex_field as CF
+    x = torch.linspace(0.0, 4.0, 4096, dtype=torch.float64, device="cuda")
+    vs = table_source(x * x * x - x, 0.0, 4095 / 4.0, 4096)
+    a = _cstate(shape, storage, 2)
+    b = [t.clone() for t in a]
+    oa = [torch.empty_like(t) for t in a]
+    ob = [torch.empty_like(t) for t in a]
+    rng = RF.PhiRange()
+    for n in range(3):
+        CF.rk2_step_table_into(a, oa, 0.05, 1.0, 1.0, 1.0, 1.0, vs, noise_scale=0.3,
+                               noise_step=n, seed=2, rho_range=rng)
+        CF.rk2_step_table_into(b, ob, 0.05, 1.0, 1.0, 1.0, 1.0, vs, noise_scale=0.3,
+                               noise_step=n, seed=2)
+        torch.cuda.synchronize()
+        assert all(torch.equal(u, v) for u, v in zip(oa, ob))
+        lo, hi, bad = RF.PhiRange.decode(rng.last.cpu().numpy())
+        r = _rho32(oa[0], oa[1])
+        assert lo == float(r.min()) and hi == float(r.max()) and not bad, n
+        a, oa = oa, a
+        b, ob = ob, b

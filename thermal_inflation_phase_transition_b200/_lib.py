@@ -97,6 +97,9 @@ _SIGS = {
     "tipt_complex_rk2_step_table": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
                                     C.POINTER(StepParams), C.POINTER(VSource),
                                     C.POINTER(ComplexTerms), _p, _p, _p],
+    "tipt_complex_rk2_step_table_range": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _i64, _i64,
+                                    C.POINTER(StepParams), C.POINTER(VSource),
+                                    C.POINTER(ComplexTerms), _p, _p, _p, _p, _p],
     "tipt_complex_rk2_fused_table": [_i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64,
                                      _i64, _i64, C.POINTER(StepParams), C.POINTER(VSource),
                                      C.POINTER(VSource), C.POINTER(ComplexTerms), _p, _p, _p],

@@ -20,9 +20,12 @@ from ._common import (dims_of, need_cuda, poly_source, ptr, same_layout, step_pa
 
 def rk2_step_table(phi1, phi2, pi1, pi2, dt, dx, eta_eff, mu, noise1, noise2, phi1_tmp,
                    phi2_tmp, pi1_tmp, pi2_tmp, inv_a2, vp_table, vp_tmin, vp_dinv, vp_npts, *,
-                   zn=(0.0, 0.0, 0.0), eps4=0.0, noise_scale=0.0, noise_step=0, seed=0):
+                   zn=(0.0, 0.0, 0.0), eps4=0.0, noise_scale=0.0, noise_step=0, seed=0,
+                   rho_range=None):
     """C:2067 rk2_step_table (complex): one midpoint step, in place (storage exchange
-    with the *_tmp tensors, as real_field.rk2_step_table)."""
+    with the *_tmp tensors, as real_field.rk2_step_table).  ``rho_range`` (a
+    real_field.PhiRange) receives the new |Phi|'s minimum and maximum from the same
+    launch (the complex loop's per-step rho check, C:4263-4288)."""
     st = storage_of(phi1)
     arrs = (phi1, phi2, pi1, pi2, phi1_tmp, phi2_tmp, pi1_tmp, pi2_tmp)
     names = ("phi1", "phi2", "pi1", "pi2", "phi1_tmp", "phi2_tmp", "pi1_tmp", "pi2_tmp")
@@ -40,9 +43,13 @@ def rk2_step_table(phi1, phi2, pi1, pi2, dt, dx, eta_eff, mu, noise1, noise2, ph
     vs = table_source(vp_table, vp_tmin, vp_dinv, vp_npts)
     sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
     ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
-    L.call("tipt_complex_rk2_step_table", st, ptr(phi1), ptr(phi2), ptr(pi1), ptr(pi2),
-           ptr(phi1_tmp), ptr(phi2_tmp), ptr(pi1_tmp), ptr(pi2_tmp), nx, ny, nz, sp, vs, ct,
-           ptr(noise1), ptr(noise2), stream_handle())
+    args = (st, ptr(phi1), ptr(phi2), ptr(pi1), ptr(pi2), ptr(phi1_tmp), ptr(phi2_tmp),
+            ptr(pi1_tmp), ptr(pi2_tmp), nx, ny, nz, sp, vs, ct, ptr(noise1), ptr(noise2))
+    if rho_range is None:
+        L.call("tipt_complex_rk2_step_table", *args, stream_handle())
+    else:
+        cur, nxt = rho_range.next_pair()
+        L.call("tipt_complex_rk2_step_table_range", *args, ptr(cur), ptr(nxt), stream_handle())
     for a, b in ((phi1, phi1_tmp), (phi2, phi2_tmp), (pi1, pi1_tmp), (pi2, pi2_tmp)):
         swap_storage(a, b)
 
@@ -218,14 +225,22 @@ def rk2_step_fused(phi1, phi2, pi1, pi2, dt, dx, eta_eff, T, T_mid, mu, lam, mph
 
 
 def rk2_step_table_into(state, out, dt, dx, eta_eff, mu, inv_a2, vsource, *, zn=(0.0, 0.0, 0.0),
-                        eps4=0.0, noise_scale=0.0, noise_step=0, seed=0, stream=None):
-    """Ping-pong form: state=(phi1, phi2, pi1, pi2) -> out=(phi1', phi2', pi1', pi2')."""
+                        eps4=0.0, noise_scale=0.0, noise_step=0, seed=0, stream=None,
+                        rho_range=None):
+    """Ping-pong form: state=(phi1, phi2, pi1, pi2) -> out=(phi1', phi2', pi1', pi2');
+    ``rho_range`` (a real_field.PhiRange) receives the range of the new |Phi|."""
     st = storage_of(state[0])
     nx, ny, nz = dims_of(state[0])
     sp = step_params(dt, dx, eta_eff, mu, inv_a2, noise_scale, noise_step, seed)
     ct = L.ComplexTerms(float(zn[0]), float(zn[1]), float(zn[2]), float(eps4))
-    L.call("tipt_complex_rk2_step_table", st, *[ptr(a) for a in state], *[ptr(a) for a in out],
-           nx, ny, nz, sp, vsource, ct, None, None, stream_handle(stream))
+    args = (st, *[ptr(a) for a in state], *[ptr(a) for a in out], nx, ny, nz, sp, vsource, ct,
+            None, None)
+    if rho_range is None:
+        L.call("tipt_complex_rk2_step_table", *args, stream_handle(stream))
+    else:
+        cur, nxt = rho_range.next_pair()
+        L.call("tipt_complex_rk2_step_table_range", *args, ptr(cur), ptr(nxt),
+               stream_handle(stream))
 
 
 def _vsource_1d(vp_table, vp_tmin, vp_dinv, vp_npts, vpoly):

@@ -26,8 +26,10 @@ __device__ __forceinline__ void complex_noise(const ComplexStageParams& p, uint6
     }
 }
 
-template <int S, bool TH>
+template <int S, bool TH, bool RG>
 __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams p) {
+    if constexpr (RG) reset_range_words(p.range_next);
+    RangeAcc racc;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using TT = typename std::conditional<S == TIPT_F32C, float, double>::type;
     TT* s_tab = reinterpret_cast<TT*>(smem_raw);
@@ -76,10 +78,12 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
             double k2a = p.inv_a2 * lapt[0] - p.eta * pta - d1 * p.inv_mu2;
             double k2b = p.inv_a2 * lapt[1] - p.eta * ptb - d2 * p.inv_mu2;
             complex_noise<double>(p, (uint64_t)s, n1, n2);
-            static_cast<double*>(p.o[0])[s] = a[0][0] + p.h2 * pta;
-            static_cast<double*>(p.o[1])[s] = a[1][0] + p.h2 * ptb;
+            const double o0 = a[0][0] + p.h2 * pta, o1 = a[1][0] + p.h2 * ptb;
+            static_cast<double*>(p.o[0])[s] = o0;
+            static_cast<double*>(p.o[1])[s] = o1;
             static_cast<double*>(p.o[2])[s] = a[2][0] + (p.h2 * k2a + n1);
             static_cast<double*>(p.o[3])[s] = a[3][0] + (p.h2 * k2b + n2);
+            if constexpr (RG) racc.fold(rho_f64(o0, o1));
         } else if constexpr (S == TIPT_F32) {
             double n1, n2;
             // float32 storage, FP64 arithmetic after the float32 neighbour sums,
@@ -111,8 +115,11 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
             double k2a = p.inv_a2 * lapt[0] - p.eta * (double)pta - d1 * p.inv_mu2;
             double k2b = p.inv_a2 * lapt[1] - p.eta * (double)ptb - d2 * p.inv_mu2;
             complex_noise<float>(p, (uint64_t)s, n1, n2);
-            static_cast<float*>(p.o[0])[s] = __double2float_rn((double)a[0][0] + p.h2 * (double)pta);
-            static_cast<float*>(p.o[1])[s] = __double2float_rn((double)a[1][0] + p.h2 * (double)ptb);
+            const float o0 = __double2float_rn((double)a[0][0] + p.h2 * (double)pta);
+            const float o1 = __double2float_rn((double)a[1][0] + p.h2 * (double)ptb);
+            static_cast<float*>(p.o[0])[s] = o0;
+            static_cast<float*>(p.o[1])[s] = o1;
+            if constexpr (RG) racc.fold(rho_f32(o0, o1));
             static_cast<float*>(p.o[2])[s] = __double2float_rn((double)a[2][0] + (p.h2 * k2a + n1));
             static_cast<float*>(p.o[3])[s] = __double2float_rn((double)a[3][0] + (p.h2 * k2b + n2));
         } else {
@@ -172,16 +179,20 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
                 po[s] = oh[f];
                 po[N + s] = ol[f];
             }
+            if constexpr (RG)
+                racc.fold(rho_f32(__fadd_rn(oh[0], ol[0]), __fadd_rn(oh[1], ol[1])));
         }
     }
+    if constexpr (RG) racc.flush(p.range);
 }
 
 constexpr int64_t kMaxTableSmemC = 96 * 1024;
 
 template <int S>
 static int launch_complex_generic(ComplexStageParams p, int64_t smem, cudaStream_t st) {
-    auto kern = p.vkind == TIPT_VP_THERMAL ? complex_stage_generic<S, true>
-                                           : complex_stage_generic<S, false>;
+    auto kern = p.vkind == TIPT_VP_THERMAL
+                    ? (p.range ? complex_stage_generic<S, true, true> : complex_stage_generic<S, true, false>)
+                    : (p.range ? complex_stage_generic<S, false, true> : complex_stage_generic<S, false, false>);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -308,6 +319,27 @@ extern "C" int tipt_complex_rk2_step_table(int storage, const void* phi1, const 
     int rc = complex_stage_call(storage, phi1, phi2, pi1, pi2, phi1_out, phi2_out, pi1_out,
                                 pi2_out, nx, ny, nz, sp, vp, ct, noise1, noise2, p);
     if (rc) return rc;
+    return launch_complex_stage(storage, p, (cudaStream_t)stream);
+}
+
+extern "C" int tipt_complex_rk2_step_table_range(int storage, const void* phi1, const void* phi2,
+                                                 const void* pi1, const void* pi2, void* phi1_out,
+                                                 void* phi2_out, void* pi1_out, void* pi2_out,
+                                                 int64_t nx, int64_t ny, int64_t nz,
+                                                 const tipt_step_params* sp,
+                                                 const tipt_vsource* vp,
+                                                 const tipt_complex_terms* ct, const void* noise1,
+                                                 const void* noise2, uint32_t* range,
+                                                 uint32_t* range_next, void* stream) {
+    ComplexStageParams p;
+    int rc = complex_stage_call(storage, phi1, phi2, pi1, pi2, phi1_out, phi2_out, pi1_out,
+                                pi2_out, nx, ny, nz, sp, vp, ct, noise1, noise2, p);
+    if (rc) return rc;
+    if ((rc = check_ptr(range, 4, "range")) || (rc = check_ptr(range_next, 4, "range_next")))
+        return rc;
+    if (overlap(range, range_next, 12)) return fail(TIPT_ERR_ARG, "range and range_next overlap");
+    p.range = reinterpret_cast<unsigned int*>(range);
+    p.range_next = reinterpret_cast<unsigned int*>(range_next);
     return launch_complex_stage(storage, p, (cudaStream_t)stream);
 }
 

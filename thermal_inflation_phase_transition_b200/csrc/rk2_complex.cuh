@@ -25,7 +25,21 @@ struct ComplexStageParams {
     double c1, c2, c3;
     int table_in_smem;
     ThermalSite th;  // TIPT_VP_THERMAL: the inline thermal V'(rho) at T
+    // Range of the new |Phi| (optional, the complex loop's per-step rho check,
+    // C:4263-4288): as RealStageParams::range, folded from rho = sqrt(phi1^2 +
+    // phi2^2) of the values written (FP32 for the compensated and float32
+    // storages, FP64 rounded to FP32 for FP64).
+    unsigned int* range;
+    unsigned int* range_next;
 };
+
+// rho of the values written, as the range folds it.
+__device__ __forceinline__ float rho_f32(float a, float b) {
+    return __fsqrt_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)));
+}
+__device__ __forceinline__ float rho_f64(double a, double b) {
+    return (float)__dsqrt_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+}
 
 // C:2137-2158 projection + Z_N (reference form), then eps*Re(Phi^4) whose
 // gradient is 4 eps (p1^3 - 3 p1 p2^2, 3 p1^2 p2 - p2^3).  FP64 (and the

@@ -858,13 +858,14 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
 // per plane and neighbour) and evaluates them in the two lanes of the packed
 // FP32x2 instructions with the arithmetic of the generic kernel
 // (complex_update_f32c), so the results are bitwise identical.
-template <bool WIDE>
+template <bool WIDE, bool RG>
 __global__ void __maxnreg__(kMarchRegs)
     complex_stage_march_f32c(const __grid_constant__ CUtensorMap tm0,
                              const __grid_constant__ CUtensorMap tm1,
                              const __grid_constant__ CUtensorMap tm2,
                              const __grid_constant__ CUtensorMap tm3, ComplexStageParams p,
                              MarchGeom g) {
+    if constexpr (RG) reset_range_words(p.range_next);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     float* s_tab = reinterpret_cast<float*>(smem);
@@ -989,6 +990,7 @@ __global__ void __maxnreg__(kMarchRegs)
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
 
+    RangeAcc racc;
     RingPos pm{0, 0};
     for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
         const int ic = item / nJK;
@@ -1076,6 +1078,11 @@ __global__ void __maxnreg__(kMarchRegs)
                 *reinterpret_cast<float2*>(po + rowoff) = oh[f];
                 *reinterpret_cast<float2*>(po + N + rowoff) = ol[f];
             }
+            if constexpr (RG) {
+                const float2 v1 = v_add(oh[0], ol[0]), v2 = v_add(oh[1], ol[1]);
+                racc.fold(rho_f32(v1.x, v2.x));
+                racc.fold(rho_f32(v1.y, v2.y));
+            }
             pm = pc;
             pc = pp;
             pp.next(NS);
@@ -1087,6 +1094,7 @@ __global__ void __maxnreg__(kMarchRegs)
         }
         pm = pp;
     }
+    if constexpr (RG) racc.flush(p.range);
 }
 
 // ------------------------------------------------------------------ host ---
@@ -1442,7 +1450,8 @@ int launch_complex_march(const ComplexStageParams& p, cudaStream_t st) {
     for (int f = 0; f < 4; ++f)
         if (!make_map(&tm[f], p.f[f], 2 * p.n0, p.n1, p.n2, 4, g.BK))
             return fail(TIPT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    auto kern = wide ? complex_stage_march_f32c<true> : complex_stage_march_f32c<false>;
+    auto kern = p.range ? (wide ? complex_stage_march_f32c<true, true> : complex_stage_march_f32c<false, true>)
+                        : (wide ? complex_stage_march_f32c<true, false> : complex_stage_march_f32c<false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess)

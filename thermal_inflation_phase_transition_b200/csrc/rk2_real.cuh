@@ -68,44 +68,9 @@ struct RealStageParams {
     unsigned int* range_next;
 };
 
-// Order-preserving integer code of a float (unsigned comparison = float order).
-__device__ __forceinline__ unsigned int ord_code(float f) {
-    const unsigned int u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-
-// Per-thread running range of the values a launch writes.
-struct RangeAcc {
-    float lo, hi;
-    unsigned int bad;
-    __device__ __forceinline__ RangeAcc() : lo(INFINITY), hi(-INFINITY), bad(0u) {}
-    __device__ __forceinline__ void fold(float v) {
-        lo = fminf(lo, v);
-        hi = fmaxf(hi, v);
-        bad |= !(fabsf(v) <= 3.402823466e38f);   // NaN or infinite
-    }
-    // Reduction over the warp's active lanes (lanes that left early are not
-    // waited for); the lowest active lane folds it into range[0..2].
-    __device__ __forceinline__ void flush(unsigned int* range) {
-        const unsigned int m = __activemask();
-        const unsigned int l = __reduce_min_sync(m, ord_code(lo));
-        const unsigned int h = __reduce_max_sync(m, ord_code(hi));
-        const unsigned int b = __reduce_or_sync(m, bad);
-        if ((int)(threadIdx.x & 31) == __ffs(m) - 1) {
-            atomicMin(&range[0], l);
-            atomicMax(&range[1], h);
-            if (b) atomicOr(&range[2], 1u);
-        }
-    }
-};
-
 // Block 0, thread 0 resets the range words of the following launch.
 __device__ __forceinline__ void reset_next_range(const RealStageParams& p) {
-    if (p.range_next && blockIdx.x == 0 && threadIdx.x == 0) {
-        p.range_next[0] = 0xFFFFFFFFu;
-        p.range_next[1] = 0u;
-        p.range_next[2] = 0u;
-    }
+    reset_range_words(p.range_next);
 }
 
 // Resolve the per-step scalars of a scheduled launch (no-op otherwise).

@@ -5,6 +5,7 @@
 //                      C = simulation/latticeSimComplex_numba.py.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -16,6 +17,46 @@ constexpr uint64_t kPass2Mul = 73856093ull;   // R:2518 (pass 2 / midpoint)
 constexpr uint64_t kPass4Mul = 19349669ull;   // R:2643 (pass 4)
 constexpr uint64_t kSeedStride = 0x9E3779B97F4A7C15ull;
 constexpr double kTwoPiLit = 6.283185307179586;  // literal of R:2520
+
+// Order-preserving integer code of a float (unsigned comparison = float order).
+__device__ __forceinline__ unsigned int ord_code(float f) {
+    const unsigned int u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// Per-thread running range of the values a launch writes.
+struct RangeAcc {
+    float lo, hi;
+    unsigned int bad;
+    __device__ __forceinline__ RangeAcc() : lo(INFINITY), hi(-INFINITY), bad(0u) {}
+    __device__ __forceinline__ void fold(float v) {
+        lo = fminf(lo, v);
+        hi = fmaxf(hi, v);
+        bad |= !(fabsf(v) <= 3.402823466e38f);   // NaN or infinite
+    }
+    // Reduction over the warp's active lanes (lanes that left early are not
+    // waited for); the lowest active lane folds it into range[0..2].
+    __device__ __forceinline__ void flush(unsigned int* range) {
+        const unsigned int m = __activemask();
+        const unsigned int l = __reduce_min_sync(m, ord_code(lo));
+        const unsigned int h = __reduce_max_sync(m, ord_code(hi));
+        const unsigned int b = __reduce_or_sync(m, bad);
+        if ((int)(threadIdx.x & 31) == __ffs(m) - 1) {
+            atomicMin(&range[0], l);
+            atomicMax(&range[1], h);
+            if (b) atomicOr(&range[2], 1u);
+        }
+    }
+};
+
+// Block 0, thread 0 resets three range words for the following launch.
+__device__ __forceinline__ void reset_range_words(unsigned int* next) {
+    if (next && blockIdx.x == 0 && threadIdx.x == 0) {
+        next[0] = 0xFFFFFFFFu;
+        next[1] = 0u;
+        next[2] = 0u;
+    }
+}
 
 // ---------------------------------------------------------------- noise ----
 // R:2322-2336 _hash_rng_pair: splitmix-style mix -> two 53-bit uniforms.  The

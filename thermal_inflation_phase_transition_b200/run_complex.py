@@ -176,6 +176,10 @@ class ComplexRun:
         return (RF.from_f32c(t) if t.dim() == 4 else t).double()
 
     def _rho_max(self):
+        """max |Phi|: from the previous step's fused range when it has one
+        (rk2_nonfused), else a reduction."""
+        if getattr(self, "rrange", None) is not None and self._range_valid:
+            return RF.PhiRange.decode(self.rrange.last.cpu().numpy())[1]
         p1, p2 = self._v(self.st[0]), self._v(self.st[1])
         return float(torch.sqrt(p1 * p1 + p2 * p2).max())
 
@@ -269,7 +273,9 @@ class ComplexRun:
         RF.generate_noise_field(n1, ns, n, component=0)
         RF.generate_noise_field(n2, ns, n, component=1)
         if self.integrator == "rk2_nonfused":
-            CF.rk2_step_table(*st, dt, dx, eta_eff, mu, n1, n2, *self.mid, inv_a2, *tab, zn=zn)
+            CF.rk2_step_table(*st, dt, dx, eta_eff, mu, n1, n2, *self.mid, inv_a2, *tab, zn=zn,
+                              rho_range=self.rrange)
+            self._range_valid = True
         elif self.integrator == "rk2_nonfused_inline":
             CF.rk2_step_inline(*st, dt, dx, eta_eff, T, mu, *c, n1, n2, *self.mid, inv_a2, zn=zn,
                                splines=self.tp)
@@ -298,6 +304,9 @@ class ComplexRun:
         ndt = torch.float32 if a.storage == "f32" else torch.float64
         self.noise = [torch.empty(self.shape, dtype=ndt, device=self.dev) for _ in range(2)]
         self.tab = None
+        # the default RK2 step folds |Phi|'s range as it writes (the table check)
+        self.rrange = RF.PhiRange(self.dev) if self.integrator == "rk2_nonfused" else None
+        self._range_valid = False
         writer = SnapshotWriter(self.state_path, checkpoint_every=CHECKPOINT_EVERY)
         dense_on = a.phi_threshold is not None and a.steps_dense is not None
         dense_active = False

@@ -11,9 +11,13 @@ Synthetic inputs (the reference has no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tipt|reference]
 
-N > 1 (torchrun, one rank per GPU): each rank steps its own independent
-512^3 replica (seed 1 + rank) -- replicas, weak scaling, no collective on the
-data path; the elapsed time is the max over ranks.
+N > 1 (torchrun, one rank per GPU): by default one (N*512) x 512 x 512 lattice
+split into x-slabs of 512 planes per rank (weak scaling), with the ghost planes
+of phi and pi exchanged point to point over NCCL every step, overlapped with
+the interior planes (slab.Slab); the W ranks reproduce the single-lattice step
+bit for bit.  `--decomp replicas` runs independent 512^3 replicas instead (seed
+1 + rank, no collective on the data path).  The elapsed time is the max over
+ranks.
 """
 from __future__ import annotations
 
@@ -130,6 +134,9 @@ def dist_setup(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
+        # NCCL's communicator set-up log (ranks, devices, transports) on stderr
+        os.environ.setdefault("NCCL_DEBUG", "INFO")
+        os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
@@ -155,17 +162,20 @@ def barrier(world):
 
 
 # -------------------------------------------------------------- CPU arms ---
-def cpu_oracle_rate(n_side, budget_s=12.0, max_steps=20, shape=None, warmup=1):
+def cpu_oracle_rate(n_side, budget_s=12.0, max_steps=20, shape=None, warmup=1,
+                    dtype=np.float64):
     """Site-updates/s of the CPU restatement (oracle/, OpenMP, all host threads) on
-    the same step: FP64 midpoint RK2, blended 2-D table row, inline hash noise."""
+    the same step: midpoint RK2, blended 2-D table row, inline hash noise.  float64
+    arrays: the FP64 step; float32 arrays: the reference's float32 mode (its default,
+    USE_FLOAT32 = True, R:348: float32 state and neighbour sums, FP64 arithmetic)."""
     from oracle import oracle as O
     O.build()
     shape = shape or (n_side, n_side, n_side)
     t2, tmin, dinv, Tmin, Tdinv = build_table_2d()
     rng = np.random.default_rng(1)
-    phi = rng.normal(0.0, 0.01, shape)
-    pi = np.zeros(shape)
-    tmp = [np.empty(shape), np.empty(shape)]
+    phi = rng.normal(0.0, 0.01, shape).astype(dtype)
+    pi = np.zeros(shape, dtype)
+    tmp = [np.empty(shape, dtype), np.empty(shape, dtype)]
 
     def one(n):
         T = temperature(n)
@@ -187,25 +197,33 @@ def cpu_oracle_rate(n_side, budget_s=12.0, max_steps=20, shape=None, warmup=1):
 
 def run_reference(args, world, rank):
     """--impl reference: the reference's CPU algorithm for this path (the oracle
-    port, since the reference is numba/Python and cannot travel), all host
-    threads, on this arm's workload; each step is one full-lattice step."""
+    port: the reference is numba/Python inside scripts that cannot be imported and
+    cannot travel), all host threads, on this arm's workload; each step is one
+    full-lattice step.  The value is the reference's default precision, float32
+    arrays (USE_FLOAT32 = True, R:348; the oracle's float32 mode is pinned to the
+    reference kernel on float32 arrays); the FP64 mode is timed beside it."""
     if rank != 0:
         return
     n = args.size
     shape = (n, n, n)
     warm = max(3, args.warmup)
-    rate, steps, threads, shp = cpu_oracle_rate(n, budget_s=max(30.0, 1.0), max_steps=max(
-        args.steps, 1), shape=shape, warmup=warm)
+    rate, steps, threads, shp = cpu_oracle_rate(n, budget_s=30.0, max_steps=max(args.steps, 1),
+                                                shape=shape, warmup=warm, dtype=np.float32)
+    rate64, steps64, _, _ = cpu_oracle_rate(n, budget_s=30.0, max_steps=max(args.steps, 1),
+                                            shape=shape, warmup=1)
     line = {
         "metric": METRIC, "value": rate, "unit": "site-updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": steps, "warmup": warm,
         "ms_per_step": 1000.0 * n ** 3 / rate, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(n, "f64"), "lattice": [n, n, n]},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(n, "f32"), "lattice": [n, n, n],
+                   "reference_mode": "float32 arrays (the reference's default, R:348)"},
         "cpu_baseline": {"value": rate, "unit": "site-updates/s", "cores": threads,
                          "kind": "port",
-                         "sample": f"{steps} full {n}^3 FP64 steps (after {warm} warm-up steps) of "
-                                   "the CPU restatement, OpenMP over all host threads"},
+                         "sample": f"{steps} full {n}^3 steps on float32 arrays (after {warm} "
+                                   "warm-up steps) of the CPU restatement of the reference's "
+                                   "float32 mode, OpenMP over all host threads",
+                         "fp64_value": rate64, "fp64_steps": steps64},
         "e2e": {"value": rate, "unit": "site-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -248,19 +266,25 @@ def main():
                          "the step kernel (the reference loop's phi.min()/max()), or the 10 "
                          "observables of a separate reduction")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["lattice", "complex", "ensemble", "surrogate", "extras"],
+    ap.add_argument("--workload", choices=["lattice", "complex", "ensemble", "surrogate", "extras",
+                                           "precision"],
                     default="lattice",
                     help="lattice: the 512^3 site-update headline; ensemble: Gamma estimates "
                          "per GPU-hour of the batched replica engine vs one-at-a-time launches")
-    ap.add_argument("--decomp", choices=["replicas", "slab"], default="replicas",
-                    help="N > 1: independent n^3 replicas per rank (default), or one "
-                         "(N n) x n x n lattice in x-slabs of n planes per rank with a halo "
-                         "exchange of the ghost planes every step (slab.Slab)")
+    ap.add_argument("--decomp", choices=["replicas", "slab"], default=None,
+                    help="N > 1: one (N n) x n x n lattice in x-slabs of n planes per rank "
+                         "with a halo exchange of the ghost planes every step (slab.Slab; "
+                         "the default), or independent n^3 replicas per rank; N = 1: the "
+                         "single-lattice step (default) or one slab with local ghost copies")
+    ap.add_argument("--prec-steps", type=int, default=10000,
+                    help="steps of the precision workload (FP32C beside FP64)")
     ap.add_argument("--ens-steps", type=int, default=2000)
     ap.add_argument("--ens-plain", type=int, default=6,
                     help="replicas per size class timed one at a time")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.decomp is None:
+        args.decomp = "slab" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else "replicas"
     if args.workload == "ensemble" and args.impl == "tipt":
         run_ensemble_bench(args)
         return
@@ -272,6 +296,9 @@ def main():
         return
     if args.workload == "extras" and args.impl == "tipt":
         run_extras_bench(args)
+        return
+    if args.workload == "precision" and args.impl == "tipt":
+        run_precision_bench(args)
         return
 
     if args.impl == "reference":
@@ -583,6 +610,80 @@ def run_ensemble_bench(args):
     }
     print(json.dumps(line, default=lambda o: o.item() if hasattr(o, "item") else str(o)),
           flush=True)
+
+
+def run_precision_bench(args):
+    """The cooling run in compensated FP32 beside FP64: n^3 (--size; 256 for the
+    two-storage comparison the workload names, 512 for the headline lattice), T
+    cooling linearly 1.05 -> 0.98 over 10^4 steps (temperature(t), R:2828-2829),
+    2-D V'(phi, T) table 4096 x 256 (bilinear), hash noise seed 1, the same initial
+    field.  Both runs go through the graph-captured driver with the 10 observables
+    reduced (FP64, fixed order) after every step.  Reports the error of every
+    observable against the FP64 run (max over the 10^4 steps), the converted-fraction
+    curve of both runs and their largest difference, and each storage's step
+    throughput (site-updates/s, algorithmic HBM GB/s) timed without the
+    observables."""
+    import torch
+    from thermal_inflation_phase_transition_b200 import driver as D
+    from thermal_inflation_phase_transition_b200.observables import OBS_NAMES, OBS_INDEX
+
+    torch.cuda.set_device(0)
+    n = args.size
+    shape = (n, n, n)
+    steps = args.prec_steps
+    tab = D.Table2D.build(D.toy_vprime, 0.0, 3.0, 4096, 0.97, 1.06, 256)
+    sched = D.linear_cooling(T_START, T_END, N_COOL, steps, dt=DT)
+    kw = dict(table=tab, schedule=sched, seed=1, init_seed=7, graph_steps=100)
+    res, rate = {}, {}
+    for storage in ("f64", "f32c"):
+        sim = D.Simulation(shape, storage=storage, **kw)
+        t0 = time.perf_counter()
+        res[storage] = sim.run(steps)
+        wall = time.perf_counter() - t0
+        # step throughput without the observables (fresh instance, same workload)
+        s2 = D.Simulation(shape, storage=storage, **kw)
+        s2.run(100, observe=False)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s2.run(200, observe=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 200
+        rate[storage] = {"ms_per_step": ms, "site_updates_per_s": n ** 3 / (ms / 1e3),
+                         "hbm_gbs_algorithmic": BYTES_PER_SITE[storage] * n ** 3 / (ms / 1e3) / 1e9,
+                         "run_wall_s_with_observables": wall}
+        del sim, s2
+        torch.cuda.empty_cache()
+    a, b = res["f64"], res["f32c"]
+    errs = {}
+    for q, name in enumerate(OBS_NAMES):
+        if name == "n_nonfinite":
+            continue
+        d = np.abs(b[:, q] - a[:, q])
+        scale = np.maximum(np.abs(a[:, q]), 1e-300)
+        errs[name] = {"max_abs": float(d.max()), "max_rel": float((d / scale).max()),
+                      "final_rel": float(d[-1] / scale[-1])}
+    kf = OBS_INDEX["frac_above"]
+    every = max(1, steps // 40)
+    idx = np.arange(every - 1, steps, every)
+    line = {
+        "metric": "compensated-FP32 error against FP64 (max over the run)", "unit": "relative",
+        "value": errs["phi2_mean"]["max_rel"], "higher_is_better": False,
+        "workload": "precision", "steps": steps, "n_gpus": 1, "data": "synthetic",
+        "config": {"workload": f"real scalar field {n}^3 periodic, T cooling 1.05->0.98 over "
+                               f"1e4 steps, 2-D V' table 4096x256, hash noise seed 1, "
+                               "f32c and f64 from the same initial field",
+                   "lattice": [n, n, n], "dt": DT},
+        "phi2_mean_max_rel_err": errs["phi2_mean"]["max_rel"],
+        "phi2_mean_target": 1e-6,
+        "observable_errors_vs_f64": errs,
+        "frac_above_1": {"steps": idx.tolist(), "f64": a[idx, kf].tolist(),
+                         "f32c": b[idx, kf].tolist(),
+                         "max_abs_diff_all_steps": float(np.abs(b[:, kf] - a[:, kf]).max())},
+        "throughput": rate,
+    }
+    print(json.dumps(line), flush=True)
 
 
 def run_complex_bench(args):

@@ -536,6 +536,14 @@ int tipt_set_march_kseg(int kseg);
  * (R:3882-3944): failures are reported, never trapped. */
 int tipt_device_status(int* status, int clear);
 
+/* Test of the bounded device waits (no reference counterpart; the reference's
+ * only failure handling is the host NaN guard, R:3882-3944): arms the next
+ * compensated-FP32 marching stage launch to withhold ring position `position`
+ * in its block 0, so that block's consumers wait for a plane that never
+ * arrives, give up after the bounded wait (2 s), set TIPT_ERR_TIMEOUT and
+ * return; nothing is left in flight.  One launch only; position < 0 disarms. */
+int tipt_test_withhold_plane(int position);
+
 #ifdef __cplusplus
 }
 #endif

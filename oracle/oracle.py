@@ -60,6 +60,7 @@ def _declare(L):
     L.orc_rk2_fused_table_f64.argtypes = base + [_p, _d, _d, _i64, _p, _d, _d, _i64, _p, _d, _u64, _u64]
     L.orc_rk2_fused_table_f32.argtypes = base + [_p, _d, _d, _i64, _p, _d, _d, _i64, _p, _d, _u64, _u64]
     L.orc_rk2_fused_poly_f64.argtypes = base + [_d, _d, _d, _u64, _u64]
+    L.orc_rk2_step_poly_f64.argtypes = base + [_d, _d, _d, _d, _u64, _u64]
     L.orc_rk2_step_table_complex_f64.argtypes = (
         [_p] * 8 + [_i64, _i64, _i64, _d, _d, _d, _d, _d, _p, _d, _d, _i64, _d, _d, _d, _d,
                     _p, _p, _d, _u64, _u64])
@@ -167,6 +168,19 @@ def rk2_fused_table(phi, pi, dt, dx, eta_eff, mu, noise, phi_tmp, pi_tmp, inv_a2
       _ptr(_c(vp_table_T, np.float64)), vp_tmin_T, vp_dinv_T, vp_npts_T,
       _ptr(_c(vp_table_Tm, np.float64)), vp_tmin_Tm, vp_dinv_Tm, vp_npts_Tm, _ptr(noise),
       noise_scale, noise_step, noise_seed)
+
+
+def rk2_step_poly(phi, pi, dt, dx, eta_eff, mu, inv_a2, c1, c2, c3, *, noise_scale=0.0,
+                  noise_step=0, noise_seed=0):
+    """R:1875 rk2_step_table with V'(x) = c1 x + c2 x^2 + c3 x^3 instead of the table (the
+    batched replicas' toy potential), FP64, in place, inline hash noise."""
+    nx, ny, nz = phi.shape
+    for a in (phi, pi):
+        _c(a, np.float64)
+    tmp = [np.empty_like(phi), np.empty_like(pi)]
+    lib().orc_rk2_step_poly_f64(_ptr(phi), _ptr(pi), _ptr(tmp[0]), _ptr(tmp[1]), nx, ny, nz, dt,
+                                dx, eta_eff, mu, inv_a2, c1, c2, c3, noise_scale, noise_step,
+                                noise_seed)
 
 
 def rk2_fused_single_pass_poly(phi, pi, dt, dx, eta_eff, mu, lam, mphi, noise_scale, noise_step,

@@ -315,6 +315,20 @@ void orc_rk2_fused_poly_f64(double *phi, double *pi, double *phi_tmp, double *pi
                  K_PASS4, 0.5);
 }
 
+/* rk2_step_table (R:1875-1966) with the polynomial V'(x) = c1 x + c2 x^2 +
+ * c3 x^3 in place of the table (the toy potential family of the batched
+ * replicas: c1 = 2D(T^2-T0^2), c2 = -3ET, c3 = lam), FP64, inline hash noise
+ * ns*z(site, step, K_PASS2, seed). */
+void orc_rk2_step_poly_f64(double *phi, double *pi, double *phi_tmp, double *pi_tmp,
+                           int64_t nx, int64_t ny, int64_t nz, double dt, double dx,
+                           double eta_eff, double mu, double inv_a2, double c1, double c2,
+                           double c3, double ns, uint64_t step, uint64_t seed) {
+    noise_src n = {NULL, ns, step, seed};
+    vsrc_t v = {NULL, 0, 0, 0, c3, -c1, c2};
+    midpoint_f64(phi, pi, phi_tmp, pi_tmp, nx, ny, nz, 0.5 * dt, dt, dx, eta_eff, mu, inv_a2,
+                 &v, &n, K_PASS2, 1.0);
+}
+
 void orc_rk2_fused_table_f32(float *phi, float *pi, float *phi_tmp, float *pi_tmp, int64_t nx,
                              int64_t ny, int64_t nz, double dt, double dx, double eta_eff,
                              double mu, double inv_a2, const double *tab_a, double tmin_a,

@@ -2,7 +2,7 @@
 numba kernels (AST-extracted by ref_extract.py from the reference checkout).
 
 Run in a container that has the reference checkout and numba:
-    python tests/golden/make_golden.py
+    TIPT_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py
 The fixtures are small .npz files; the GPU box never needs the reference.
 
 Every fixture stores its inputs, the reference's outputs and the parameters,

@@ -1,7 +1,7 @@
 """Golden fixture of the complex-field fused and inline steppers
 (tests/golden/complex_thermal.npz), generated with the REFERENCE's own kernels:
 
-    python tests/golden/make_golden_complex_thermal.py
+    TIPT_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden_complex_thermal.py
 
 AST-extracted complex-field kernels (ref_extract.load_complex), run unmodified:
 * five steps of ``rk2_fused_table`` (C:1789-2064) with V'(rho) tables at T and

@@ -1,7 +1,7 @@
 """Golden fixture of the complex script's un-fused stepper
 (tests/golden/complex_unfused.npz), generated with the REFERENCE's own kernels:
 
-    python tests/golden/make_golden_complex_unfused.py
+    TIPT_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden_complex_unfused.py
 
 AST-extracted complex-field kernels (ref_extract.load_complex) with the dJ
 splines of tests/golden/thermal.npz and the script's _POT_COEFFS = (2, -1), run

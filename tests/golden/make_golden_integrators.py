@@ -2,7 +2,7 @@
 overdamped Euler-Maruyama, R:1973-2193, C:2222-2528), generated by running the
 REFERENCE's own numba kernels (AST-extracted by ref_extract.py):
 
-    python tests/golden/make_golden_integrators.py
+    TIPT_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden_integrators.py
 
 The reference kernels update the field in place inside a parallel loop, so a
 site can see neighbours already advanced in the same sweep, and they draw their

@@ -1,7 +1,7 @@
 """Golden fixtures of the thermal V' path (tests/golden/thermal.npz), generated
 from the REFERENCE's own code:
 
-    python tests/golden/make_golden_thermal.py
+    TIPT_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden_thermal.py
 
 * dJ_B(u), dJ_F(u) on the reference's grid (u = m/T in [0, 100], 256 points):
   the quadratures ``FlatonPotential._dJb_exact`` / ``_dJf_exact`` of

@@ -1,7 +1,7 @@
 """Golden fixture of rk2_fused_single_pass with the thermal inline V'
 (tests/golden/thermal_inline.npz), generated with the REFERENCE's own kernels:
 
-    python tests/golden/make_golden_thermal_inline.py
+    TIPT_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden_thermal_inline.py
 
 The spline coefficients are those of tests/golden/thermal.npz (the reference's
 dJ_B / dJ_F quadratures on its 256-point grid, not-a-knot splines; see

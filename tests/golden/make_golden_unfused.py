@@ -1,7 +1,7 @@
 """Golden fixture of the reference's un-fused stepper and its array helpers
 (tests/golden/unfused.npz), generated with the REFERENCE's own kernels:
 
-    python tests/golden/make_golden_unfused.py
+    TIPT_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden_unfused.py
 
 AST-extracted real-field kernels (ref_extract.load_real) with the dJ splines of
 tests/golden/thermal.npz as module globals, run unmodified:

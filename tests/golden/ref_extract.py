@@ -22,7 +22,12 @@ import os
 import numba as nb
 import numpy as np
 
-REF_ROOT = os.environ.get("TIPT_REFERENCE_ROOT", "/root/reference")
+# The reference checkout's root directory: set TIPT_REFERENCE_ROOT before running
+# a fixture generator (there is no default location).
+REF_ROOT = os.environ.get("TIPT_REFERENCE_ROOT", "")
+if not REF_ROOT or not os.path.isdir(os.path.join(REF_ROOT, "simulation")):
+    raise RuntimeError("set TIPT_REFERENCE_ROOT to the reference checkout (the directory that "
+                       "holds simulation/latticeSimeRescale_numba.py)")
 REAL_SCRIPT = os.path.join(REF_ROOT, "simulation", "latticeSimeRescale_numba.py")
 COMPLEX_SCRIPT = os.path.join(REF_ROOT, "simulation", "latticeSimComplex_numba.py")
 

@@ -54,3 +54,63 @@ def test_ensemble_mixed_lattice_shapes_step():
         phi, pi = ens.replica_state(r)
         assert torch.isfinite(phi).all() and torch.isfinite(pi).all()
         assert float(pi.abs().max()) > 0
+
+
+# ---------------------------------------------------------------- vs the oracle
+# The batched replicas (and the single lattice with the same polynomial V') against
+# the CPU oracle's midpoint step with V'(x) = c1 x + c2 x^2 + c3 x^3 (R:1875-1966
+# with the polynomial source), replica by replica: own extents, seed, T and E.
+from oracle import oracle as O  # noqa: E402
+
+# one replica of each size class of the 1792-replica mix, scaled down
+# (128^2 -> 32^2 2-D, 64^3 -> 16^3, 96^3 -> 24^3), plus an odd extent
+MIX = [EN.ReplicaSpec((32, 32, 1), 0.985, 0.052, 31), EN.ReplicaSpec((16, 16, 16), 1.004, 0.041, 32),
+       EN.ReplicaSpec((24, 24, 24), 0.992, 0.058, 33), EN.ReplicaSpec((32, 32, 1), 1.009, 0.047, 34),
+       EN.ReplicaSpec((10, 6, 14), 0.981, 0.06, 35)]
+TOL = {"f64": 1e-12, "f32c": 2e-6}
+
+
+def _oracle_replica(sp, phi0, nsteps, dt=0.05):
+    c1, c2, c3 = EN.toy_coefficients(sp.T, sp.E, sp.D, sp.lam, sp.T0)
+    ns = (2.0 * 1.0 * sp.T * dt / 1.0) ** 0.5
+    phi = phi0.reshape(sp.shape).copy()
+    pi = np.zeros_like(phi)
+    for n in range(nsteps):
+        O.rk2_step_poly(phi, pi, dt, 1.0, 1.0, 1.0, 1.0, c1, c2, c3, noise_scale=ns,
+                        noise_step=n, noise_seed=sp.seed)
+    return phi, pi
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_ensemble_vs_oracle(storage):
+    K = 8
+    ens = EN.Ensemble(MIX, storage=storage, stop_frac=2.0, check_every=K, init_seed=3)
+    phi0 = [EN.replica_initial_phi(int(np.prod(sp.shape)), sp.seed, 3, 0.01, "cuda")
+            .cpu().numpy() for sp in MIX]
+    ens.run(K)
+    for r, sp in enumerate(MIX):
+        ref_phi, ref_pi = _oracle_replica(sp, phi0[r], K)
+        a, b = ens.replica_state(r)
+        shape = EN._canonical(sp.shape)
+        a = a.cpu().numpy().reshape(sp.shape)
+        b = b.cpu().numpy().reshape(sp.shape)
+        scale = max(np.abs(ref_phi).max(), np.abs(ref_pi).max())
+        err = max(np.abs(a - ref_phi).max(), np.abs(b - ref_pi).max()) / scale
+        assert err < TOL[storage], (r, shape, err)
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32c"])
+def test_single_lattice_poly_vs_oracle(storage):
+    """Simulation(vpoly=...) -- the per-replica plain path -- against the oracle."""
+    sp = EN.ReplicaSpec((16, 12, 8), 0.99, 0.05, 41)
+    rng = np.random.default_rng(2)
+    phi0 = rng.normal(0.6, 0.5, sp.shape)
+    sim = Simulation(sp.shape, storage=storage, table=None,
+                     vpoly=EN.toy_coefficients(sp.T, sp.E), schedule=constant_temperature(sp.T, 1, dt=0.05),
+                     seed=sp.seed, phi0=phi0, graph_steps=6)
+    sim.run(6, observe=False)
+    a, b = (t.cpu().numpy() for t in sim.fields())
+    ref_phi, ref_pi = _oracle_replica(sp, phi0, 6)
+    scale = max(np.abs(ref_phi).max(), np.abs(ref_pi).max())
+    err = max(np.abs(a - ref_phi).max(), np.abs(b - ref_pi).max()) / scale
+    assert err < TOL[storage], err

@@ -225,3 +225,28 @@ def test_complex_march_row_segments_equal_generic(shape, kseg, tiles):
     b = _crun(2, shape, tiles=tiles, kseg=kseg)
     for x, y in zip(a, b):
         assert torch.equal(x, y)
+
+
+def test_bounded_wait_expires_and_reports():
+    """A plane that never arrives: block 0's producer withholds ring position 5 (no
+    copy is issued for it or after it, so none is left in flight).  Its consumers'
+    bounded waits run out, the launch returns, the device status reads
+    TIPT_ERR_TIMEOUT (6), and the context stays usable: the next steps on it equal
+    the generic kernel's bit for bit and leave the status clear."""
+    assert L.device_status(clear=True) == 0
+    shape = (32, 32, 64)
+    L.set_kernel_policy(2)
+    phi, pi = _state(shape, "f32c", 11)
+    t1, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.01), 0.0, 3.0, 4096)
+    vs = table_source(torch.from_numpy(t1).to(DEV), tmin, dinv, 4096)
+    po, qo = torch.empty_like(phi), torch.empty_like(pi)
+    L.test_withhold_plane(5)
+    RF.rk2_step_table_into(phi, pi, po, qo, 0.05, 1.0, 0.9, 1.0, 1.0, vs, noise_scale=0.3,
+                           noise_step=0, seed=7)
+    torch.cuda.synchronize()
+    assert L.device_status(clear=True) == 6  # TIPT_ERR_TIMEOUT
+    # armed for one launch only: the next launches run normally
+    ref = _run(1, shape, "f32c")
+    got = _run(2, shape, "f32c")
+    assert torch.equal(ref[0], got[0]) and torch.equal(ref[1], got[1])
+    assert L.device_status() == 0

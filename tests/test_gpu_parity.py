@@ -355,6 +355,31 @@ def test_winding_vs_reference(golden, tag):
     assert np.array_equal(lst, want)
 
 
+@pytest.mark.parametrize("tag", ["a", "b"])
+@pytest.mark.parametrize("cast", ["f32", "f64"])
+def test_winding_evolved_strings_vs_reference(golden, tag, cast):
+    """String networks evolved by the reference's complex kernels (48^3 after a
+    quench; 40x32x24, hotter and noisier), ~10^4 pierced plaquettes per
+    orientation and hundreds of links with phase differences near +-pi, where
+    the atan2 rounding decides the integer: per-site windings, per-orientation
+    windings, the string count (C:4661) and the pierced-plaquette counts are
+    bit-exact against the reference's compute_winding_number (C:2683-2744) on the
+    FP64 casts of its float32 fields (C:4627-4629) and its tools/winding.py."""
+    g = golden("strings.npz")
+    p1, p2 = cu(g[f"{tag}_phi1"]), cu(g[f"{tag}_phi2"])
+    if cast == "f64":
+        p1, p2 = p1.double(), p2.double()
+    w = torch.empty(p1.shape, dtype=torch.float32, device=DEV)
+    CF.compute_winding_number(p1, p2, w)
+    res = CF.compute_winding_number_full(p1, p2, pierced_cap=3 * p1.numel())
+    torch.cuda.synchronize()
+    assert np.array_equal(w.cpu().numpy(), g[f"{tag}_w"].astype(np.float32))
+    assert np.array_equal(res.w3.cpu().numpy(), g[f"{tag}_w3"])
+    c = res.host_counts()
+    assert c["n_strings"] == int(g[f"{tag}_n_strings"])
+    assert [c["pierced_xy"], c["pierced_xz"], c["pierced_yz"]] == g[f"{tag}_n_pierced"].tolist()
+
+
 def test_winding_list_capacity_clamps():
     g = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden",
                                             "winding.npz"))

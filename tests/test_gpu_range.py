@@ -1,6 +1,8 @@
 """The step kernel's fused range output (the reference loop's per-step phi.min() /
-phi.max(), R:3655-3660): equal to the range of the field written, bitwise the
-same fields as the plain step, alternating buffers, and the non-finite flag."""
+phi.max(), R:3655-3660): the range of the field written, rounded outward to FP32
+(so a value one FP64 ulp outside a table bound is never folded back inside it),
+bitwise the same fields as the plain step, alternating buffers, and the
+non-finite flag."""
 import numpy as np
 import pytest
 
@@ -27,10 +29,23 @@ def _state(shape, storage, seed):
     return phi, pi
 
 
-def _values32(t):
+def _exact(t):
+    """The values written in FP64: hi + lo of a compensated field (exact here)."""
     if t.dim() == 4:
-        return (t[0] + t[1]).float()          # the FP32 sum the kernel folds
-    return t.float()
+        return t[0].double() + t[1].double()
+    return t.double()
+
+
+def rd32(x):
+    """Largest FP32 value <= x (x a float64 scalar)."""
+    f = np.float32(x)
+    return float(np.nextafter(f, np.float32(-np.inf))) if float(f) > x else float(f)
+
+
+def ru32(x):
+    """Smallest FP32 value >= x."""
+    f = np.float32(x)
+    return float(np.nextafter(f, np.float32(np.inf))) if float(f) < x else float(f)
 
 
 @pytest.mark.parametrize("shape,storage", CASES)
@@ -49,8 +64,8 @@ def test_range_matches_written_field(shape, storage):
         torch.cuda.synchronize()
         assert torch.equal(a[2], b[2]) and torch.equal(a[3], b[3])
         lo, hi, bad = RF.PhiRange.decode(rng.last.cpu().numpy())
-        v = _values32(a[2])
-        assert lo == float(v.min()) and hi == float(v.max()) and not bad, n
+        v = _exact(a[2])
+        assert lo == rd32(float(v.min())) and hi == ru32(float(v.max())) and not bad, n
         a = [a[2], a[3], a[0], a[1]]
         b = [b[2], b[3], b[0], b[1]]
 
@@ -84,7 +99,40 @@ def test_reference_signature_with_range():
                       noise_step=0, phi_range=rng)
     torch.cuda.synchronize()
     lo, hi, _ = RF.PhiRange.decode(rng.last.cpu().numpy())
-    assert lo == float(phi.float().min()) and hi == float(phi.float().max())
+    assert lo == rd32(float(phi.min())) and hi == ru32(float(phi.max()))
+
+
+def test_range_rounds_outward_at_a_table_bound():
+    """A phi one FP64 ulp above the table's upper bound t_hi (an FP32 value) reads
+    as above it, and one ulp below the lower bound as below it: the rebuild test
+    of the run loop (lo < t_lo or hi > t_hi) sees both, as the reference's
+    full-precision phi.min()/phi.max() would (nearest rounding to FP32 would map
+    both back onto the bound)."""
+    shape = (16, 12, 32)
+    t_lo, t_hi = 0.25, 3.0
+    vs = table_source(torch.zeros(64, dtype=torch.float64, device="cuda"), 0.0, 1.0, 64)
+    phi = torch.full(shape, 1.0, dtype=torch.float64, device="cuda")
+    phi[1, 2, 3] = np.nextafter(t_hi, np.inf)
+    phi[4, 5, 6] = np.nextafter(t_lo, -np.inf)
+    pi = torch.zeros_like(phi)
+    rng = RF.PhiRange()
+    po, qo = torch.empty_like(phi), torch.empty_like(pi)
+    # dt = 0 and no noise: the step writes phi unchanged
+    RF.rk2_step_table_into(phi, pi, po, qo, 0.0, 1.0, 1.0, 1.0, 1.0, vs, phi_range=rng)
+    torch.cuda.synchronize()
+    assert torch.equal(po, phi)
+    lo, hi, bad = RF.PhiRange.decode(rng.last.cpu().numpy())
+    assert hi > t_hi and lo < t_lo and not bad
+    assert hi == ru32(float(phi.max())) and lo == rd32(float(phi.min()))
+    # compensated storage: hi + lo just outside the bounds
+    pc = RF.to_f32c(phi)
+    assert float((pc[0].double() + pc[1].double()).max()) > t_hi
+    qc = torch.zeros_like(pc)
+    RF.rk2_step_table_into(pc, qc, torch.empty_like(pc), torch.empty_like(qc), 0.0, 1.0, 1.0,
+                           1.0, 1.0, vs, phi_range=rng)
+    torch.cuda.synchronize()
+    lo, hi, bad = RF.PhiRange.decode(rng.last.cpu().numpy())
+    assert hi > t_hi and lo < t_lo and not bad
 
 
 def test_table_source_keeps_its_table_alive():
@@ -126,13 +174,21 @@ def _cstate(shape, storage, seed):
     return st
 
 
-def _rho32(a, b):
+def _rho_check(a, b, lo, hi):
+    """float32 storage: the FP32 |Phi| of the reference's float32 arrays, exactly.
+    FP64: the FP64 |Phi| rounded outward.  Compensated: FP32 bounds that enclose
+    the exact |Phi| and lie within 4 FP32 ulp of it."""
     if a.dim() == 4:
-        a, b = (a[0] + a[1]).float(), (b[0] + b[1]).float()
-        return torch.sqrt(a * a + b * b)
+        ae, be = a[0].double() + a[1].double(), b[0].double() + b[1].double()
+        r = torch.sqrt(ae * ae + be * be)
+        rmin, rmax = float(r.min()), float(r.max())
+        return lo <= rmin and hi >= rmax and rmin - lo <= 4 * 2.0 ** -24 * rmin \
+            and hi - rmax <= 4 * 2.0 ** -24 * rmax
     if a.dtype == torch.float32:
-        return torch.sqrt(a * a + b * b)
-    return torch.sqrt(a * a + b * b).float()
+        r = torch.sqrt(a * a + b * b)
+        return lo == float(r.min()) and hi == float(r.max())
+    r = torch.sqrt(a * a + b * b)
+    return lo == rd32(float(r.min())) and hi == ru32(float(r.max()))
 
 
 @pytest.mark.parametrize("shape,storage", CPLX_CASES)
@@ -153,7 +209,6 @@ def test_complex_rho_range(shape, storage):
         torch.cuda.synchronize()
         assert all(torch.equal(u, v) for u, v in zip(oa, ob))
         lo, hi, bad = RF.PhiRange.decode(rng.last.cpu().numpy())
-        r = _rho32(oa[0], oa[1])
-        assert lo == float(r.min()) and hi == float(r.max()) and not bad, n
+        assert _rho_check(oa[0], oa[1], lo, hi) and not bad, n
         a, oa = oa, a
         b, ob = ob, b

@@ -144,6 +144,18 @@ def test_winding_matches_reference(golden, tag):
     assert cnt[0] + cnt[1] + cnt[2] > 0
 
 
+@pytest.mark.parametrize("tag", ("a", "b"))
+def test_winding_evolved_strings_match_reference(golden, tag):
+    """String networks evolved by the reference's complex kernels (strings.npz):
+    integer windings, per-orientation windings and counts are exact."""
+    g = golden("strings.npz")
+    w, w3, cnt = O.winding(g[f"{tag}_phi1"], g[f"{tag}_phi2"])
+    assert np.array_equal(np.round(w), g[f"{tag}_w"].astype(np.float32))
+    assert np.array_equal(w3, g[f"{tag}_w3"])
+    assert cnt[3] == int(g[f"{tag}_n_strings"])
+    assert list(cnt[:3]) == g[f"{tag}_n_pierced"].tolist()
+
+
 @pytest.mark.parametrize("tag", CASES)
 def test_energies(golden, tag):
     g = golden("energies.npz")

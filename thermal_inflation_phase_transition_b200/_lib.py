@@ -140,6 +140,7 @@ _SIGS = {
     "tipt_set_march_tiles": [_i, _i, _i],
     "tipt_set_march_kseg": [_i],
     "tipt_device_status": [C.POINTER(C.c_int), _i],
+    "tipt_test_withhold_plane": [_i],
 }
 _RESTYPE = {"tipt_version": C.c_char_p, "tipt_status_string": C.c_char_p,
             "tipt_last_error": C.c_char_p, "tipt_observables_workspace_size": C.c_int64,
@@ -195,6 +196,12 @@ def set_march_tiles(rows: int = 0, planes: int = 0, stages: int = 0) -> None:
 def set_march_kseg(kseg: int) -> None:
     """Row segment of the complex marching kernel (0 = automatic; tests/tuning)."""
     call("tipt_set_march_kseg", int(kseg))
+
+
+def test_withhold_plane(position: int) -> None:
+    """Test of the bounded device waits: the next compensated-FP32 marching stage
+    launch withholds ring position `position` in its block 0 (< 0 disarms)."""
+    call("tipt_test_withhold_plane", int(position))
 
 
 def device_status(clear: bool = False) -> int:

@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
             static_cast<double*>(p.o[1])[s] = o1;
             static_cast<double*>(p.o[2])[s] = a[2][0] + (p.h2 * k2a + n1);
             static_cast<double*>(p.o[3])[s] = a[3][0] + (p.h2 * k2b + n2);
-            if constexpr (RG) racc.fold(rho_f64(o0, o1));
+            if constexpr (RG) fold_rho_f64(racc, o0, o1);
         } else if constexpr (S == TIPT_F32) {
             double n1, n2;
             // float32 storage, FP64 arithmetic after the float32 neighbour sums,
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
                 po[N + s] = ol[f];
             }
             if constexpr (RG)
-                racc.fold(rho_f32(__fadd_rn(oh[0], ol[0]), __fadd_rn(oh[1], ol[1])));
+                fold_rho_ff(racc, oh[0], ol[0], oh[1], ol[1]);
         }
     }
     if constexpr (RG) racc.flush(p.range);

@@ -33,12 +33,23 @@ struct ComplexStageParams {
     unsigned int* range_next;
 };
 
-// rho of the values written, as the range folds it.
+// rho of the values written, as the range folds it.  float32 storage: the
+// FP32 value the reference's float32 arrays give.  FP64: the FP64 value,
+// rounded outward to FP32.  Compensated FP32 (a = ah + al, b = bh + bl): FP32
+// bounds from directed roundings, |ah| - |al| <= |a| <= |ah| + |al|, so the
+// folded range encloses the exact |Phi| of every site written.
 __device__ __forceinline__ float rho_f32(float a, float b) {
     return __fsqrt_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)));
 }
-__device__ __forceinline__ float rho_f64(double a, double b) {
-    return (float)__dsqrt_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+__device__ __forceinline__ void fold_rho_f64(RangeAcc& r, double a, double b) {
+    r.fold_d(__dsqrt_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b))));
+}
+__device__ __forceinline__ void fold_rho_ff(RangeAcc& r, float ah, float al, float bh, float bl) {
+    const float au = __fadd_ru(fabsf(ah), fabsf(al)), bu = __fadd_ru(fabsf(bh), fabsf(bl));
+    const float ad = fmaxf(__fsub_rd(fabsf(ah), fabsf(al)), 0.0f);
+    const float bd = fmaxf(__fsub_rd(fabsf(bh), fabsf(bl)), 0.0f);
+    r.fold(__fsqrt_rd(__fadd_rd(__fmul_rd(ad, ad), __fmul_rd(bd, bd))),
+           __fsqrt_ru(__fadd_ru(__fmul_ru(au, au), __fmul_ru(bu, bu))));
 }
 
 // C:2137-2158 projection + Z_N (reference form), then eps*Re(Phi^4) whose

@@ -441,6 +441,9 @@ __global__ void __maxnreg__(kMarchRegs)
         const uint32_t plane_tx = (uint32_t)(4 * rows * n2 * 4);
         const float* const src_phi = static_cast<const float*>(p.phi);
         const float* const src_pi = static_cast<const float*>(p.pi);
+        // test of the bounded waits: block 0 stops issuing at this ring position
+        const uint32_t stop_at = (p.test_withhold > 0 && blockIdx.x == 0)
+                                     ? (uint32_t)(p.test_withhold - 1) : 0xFFFFFFFFu;
         RingPos w{0, 0};
         uint32_t issued = 0;
         bool ok = true;
@@ -449,6 +452,10 @@ __global__ void __maxnreg__(kMarchRegs)
             const int j0 = (item - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
             const int npl = min(g.CI, p.i_end - i0) + 2;
             for (int q = 0; q < npl; ++q) {
+                if (issued == stop_at) {  // nothing is issued from here on
+                    ok = false;
+                    break;
+                }
                 if (issued >= NS && !mbar_wait(&empty[w.stage], w.phase ^ 1u)) {
                     ok = false;
                     break;
@@ -465,7 +472,7 @@ __global__ void __maxnreg__(kMarchRegs)
                 w.next(NS);
             }
         }
-        if (!ok) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
+        if (!ok && issued != stop_at) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
         RingPos d = w;
         for (uint32_t k = 0; k < NS && k < issued; ++k) {
             d.stage = d.stage == 0 ? NS - 1 : d.stage - 1;
@@ -595,9 +602,8 @@ __global__ void __maxnreg__(kMarchRegs)
             if constexpr (RG) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const float2 v = v_add(o[h][0], o[h][1]);
-                    racc.fold(v.x);
-                    racc.fold(v.y);
+                    racc.fold_ff(o[h][0].x, o[h][1].x);
+                    racc.fold_ff(o[h][0].y, o[h][1].y);
                 }
             }
             pm = pc;
@@ -1079,9 +1085,8 @@ __global__ void __maxnreg__(kMarchRegs)
                 *reinterpret_cast<float2*>(po + N + rowoff) = ol[f];
             }
             if constexpr (RG) {
-                const float2 v1 = v_add(oh[0], ol[0]), v2 = v_add(oh[1], ol[1]);
-                racc.fold(rho_f32(v1.x, v2.x));
-                racc.fold(rho_f32(v1.y, v2.y));
+                fold_rho_ff(racc, oh[0].x, ol[0].x, oh[1].x, ol[1].x);
+                fold_rho_ff(racc, oh[0].y, ol[0].y, oh[1].y, ol[1].y);
             }
             pm = pc;
             pc = pp;
@@ -1136,6 +1141,10 @@ static bool make_map(CUtensorMap* tm, const void* base, int planes, int n1, int 
 
 // Tile shape; 0 = choose automatically.  Set by tipt_set_march_tiles().
 static int g_force_tj = 0, g_force_ci = 0, g_force_stages = 0;
+
+// One-shot test of the bounded waits (tipt_test_withhold_plane): the next
+// compensated-FP32 marching stage launch withholds a ring position in block 0.
+static int g_test_withhold = 0;
 
 // TMA box width (elements of `es` bytes).  A tensor copy's shared-memory
 // destination must be 128-byte aligned: rows sit at multiples of the
@@ -1281,11 +1290,14 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
                     : launch_march_k(rk2_stage_march_f32c<false, true, false>, p, g, smem, st);
     }
     if (storage == TIPT_F32C) {
-        if (p.range)
-            return wide ? launch_march_k(rk2_stage_march_f32c<true, false, true>, p, g, smem, st)
-                        : launch_march_k(rk2_stage_march_f32c<false, false, true>, p, g, smem, st);
-        return wide ? launch_march_k(rk2_stage_march_f32c<true, false, false>, p, g, smem, st)
-                    : launch_march_k(rk2_stage_march_f32c<false, false, false>, p, g, smem, st);
+        RealStageParams q = p;
+        q.test_withhold = g_test_withhold;
+        g_test_withhold = 0;
+        if (q.range)
+            return wide ? launch_march_k(rk2_stage_march_f32c<true, false, true>, q, g, smem, st)
+                        : launch_march_k(rk2_stage_march_f32c<false, false, true>, q, g, smem, st);
+        return wide ? launch_march_k(rk2_stage_march_f32c<true, false, false>, q, g, smem, st)
+                    : launch_march_k(rk2_stage_march_f32c<false, false, false>, q, g, smem, st);
     }
     if (storage != TIPT_F32C && p.range)
         return fail(TIPT_ERR_UNSUPPORTED, "the FP64 / float32 marching stage takes no range output");
@@ -1490,6 +1502,16 @@ extern "C" int tipt_set_march_tiles(int rows, int planes, int stages) {
     g_force_tj = rows;
     g_force_ci = planes;
     g_force_stages = stages;
+    return TIPT_OK;
+}
+
+// Test of the bounded device waits: the next compensated-FP32 marching stage
+// launch (polynomial or table V') withholds ring position `position` (>= 0) in
+// its block 0 -- no copy is issued for it or after it, so nothing is left in
+// flight -- and the consumers of that block give up waiting after the bounded
+// wait (2 s), record TIPT_ERR_TIMEOUT and return.  position < 0 disarms.
+extern "C" int tipt_test_withhold_plane(int position) {
+    g_test_withhold = position >= 0 ? position + 1 : 0;
     return TIPT_OK;
 }
 

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
                        site_noise<double>(p, (uint64_t)(s + p.site_offset)), a, b);
             static_cast<double*>(p.phi_out)[s] = a;
             static_cast<double*>(p.pi_out)[s] = b;
-            if constexpr (RG) racc.fold((float)a);
+            if constexpr (RG) racc.fold_d(a);
         } else if constexpr (S == TIPT_F32) {
             const float* phi = static_cast<const float*>(p.phi);
             const float* pi = static_cast<const float*>(p.pi);
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
             po[N + s] = b;
             vo[s] = c;
             vo[N + s] = d;
-            if constexpr (RG) racc.fold(__fadd_rn(a, b));
+            if constexpr (RG) racc.fold_ff(a, b);
         }
     }
     if constexpr (RG) racc.flush(p.range);

@@ -61,11 +61,16 @@ struct RealStageParams {
     ThermalSite th;  // TIPT_VP_THERMAL: the inline thermal V' at T
     // Range of the new phi (optional, the reference loop's per-step phi.min() /
     // phi.max(), R:3655-3660): the launch folds the minimum and maximum of the
-    // values written (rounded to FP32, order-preserving integer codes) and a
-    // non-finite flag into range[0..2]; block 0 first resets range_next[0..2]
-    // for the following launch.
+    // values written (rounded outward to FP32, as order-preserving integer codes)
+    // and a non-finite flag into range[0..2]; block 0 first resets
+    // range_next[0..2] for the following launch.
     unsigned int* range;
     unsigned int* range_next;
+    // Test of the bounded device waits (0 = off): with k > 0 the producer of
+    // block 0 of the compensated-FP32 marching stage issues no copy from ring
+    // position k - 1 on, so its consumers' waits for that plane expire and
+    // report TIPT_ERR_TIMEOUT (tipt_test_withhold_plane arms one launch).
+    int test_withhold;
 };
 
 // Block 0, thread 0 resets the range words of the following launch.

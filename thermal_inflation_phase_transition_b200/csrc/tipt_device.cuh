@@ -24,15 +24,30 @@ __device__ __forceinline__ unsigned int ord_code(float f) {
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-// Per-thread running range of the values a launch writes.
+// Per-thread running range of the values a launch writes.  A value that FP32
+// cannot hold exactly is folded as the pair (rounded down, rounded up), so the
+// range always encloses the values written: a host test `lo < t_lo` or
+// `hi > t_hi` against a wider-precision bound then never misses a value just
+// outside it.  Values beyond the FP32 range count as non-finite.
 struct RangeAcc {
     float lo, hi;
     unsigned int bad;
     __device__ __forceinline__ RangeAcc() : lo(INFINITY), hi(-INFINITY), bad(0u) {}
-    __device__ __forceinline__ void fold(float v) {
-        lo = fminf(lo, v);
-        hi = fmaxf(hi, v);
-        bad |= !(fabsf(v) <= 3.402823466e38f);   // NaN or infinite
+    __device__ __forceinline__ void fold(float v) { fold(v, v); }
+    // vd <= exact value <= vu
+    __device__ __forceinline__ void fold(float vd, float vu) {
+        lo = fminf(lo, vd);
+        hi = fmaxf(hi, vu);
+        bad |= !(vd >= -3.402823466e38f && vu <= 3.402823466e38f);   // NaN or infinite
+    }
+    // an FP64 value
+    __device__ __forceinline__ void fold_d(double v) {
+        fold(__double2float_rd(v), __double2float_ru(v));
+    }
+    // a compensated value hi + lo: the directed FP32 sums round the exact sum
+    // down and up
+    __device__ __forceinline__ void fold_ff(float h, float l) {
+        fold(__fadd_rd(h, l), __fadd_ru(h, l));
     }
     // Reduction over the warp's active lanes (lanes that left early are not
     // waited for); the lowest active lane folds it into range[0..2].

@@ -9,7 +9,11 @@ Real field (nucleation): 64 replicas of a 32^3 periodic lattice, toy potential
 V = D(T^2-T0^2)phi^2 - E T phi^3 + lam/4 phi^4 (D = 0.1, E = 0.05, lam = 0.1,
 T0 = 1) at T = 1.07 (above T0: the symmetric phase is metastable and the
 first passage is spread over thousands of steps), V' tabulated on 4096 points
-of [0, 3], dt = 0.05, dx = 1, gamma = 1, phi ~ N(0, 0.01^2), pi = 0.  Each
+of [-3, 4] -- the range the noisy field explores, phi < 0 included, so the
+table represents the same potential as the polynomial V' of the batched
+engine the test compares with (a table starting at 0 would extrapolate
+linearly below it, a different potential for phi < 0) -- dt = 0.05, dx = 1,
+gamma = 1, phi ~ N(0, 0.01^2), pi = 0.  Each
 replica is stepped by the reference's ``rk2_step_table`` (R:1875-1966) on
 float32 arrays (its default precision, USE_FLOAT32, R:348) until the converted
 fraction mean(phi > 1) exceeds 1/2 at a check every 10 steps (at most 10^4
@@ -79,8 +83,8 @@ def toy(x, T):
 def real_runs(R, fill):
     c = REAL
     shape, T = c["shape"], c["T"]
-    x = np.linspace(0.0, 3.0, 4096)
-    tab, tmin, dinv, npts = toy(x, T).astype(np.float64), 0.0, 4095 / 3.0, 4096
+    x = np.linspace(-3.0, 4.0, 4096)
+    tab, tmin, dinv, npts = toy(x, T).astype(np.float64), -3.0, 4095 / 7.0, 4096
     ns = math.sqrt(2.0 * T * DT)
     f32 = np.float32
     n1, n2 = np.empty(shape), np.empty(shape)

@@ -50,8 +50,11 @@ struct RealStageParams {
     // FP32 constants of the compensated storage as lane pairs (x = y), rounded
     // from the FP64 parameters on the host (set_f32c_pairs): the packed FP32x2
     // instructions then read them from the parameter bank.
+    // lap_scale = inv_a2 inv_dx2, neg_eta = -eta, neg_imu2 = -inv_mu2 (the forces as
+    // two fused multiply-adds); tmd = -tmin dinv (the table index as one).
     struct {
         float2 h1, h2h, h2l, inv_dx2, inv_a2, eta, inv_mu2, c1, c2, c3, tmin, dinv;
+        float2 lap_scale, neg_eta, neg_imu2, tmd;
     } k2;
     // Planes computed: [i_begin, i_end) of the n0 planes (all planes, periodic
     // in i, when i_end = 0); the noise key's site is the array index plus
@@ -91,6 +94,9 @@ __device__ __forceinline__ void resolve_schedule(RealStageParams& p) {
         p.inv_a2 = row[3];
         p.k2.eta = make_float2((float)p.eta, (float)p.eta);
         p.k2.inv_a2 = make_float2((float)p.inv_a2, (float)p.inv_a2);
+        const float ls = (float)(p.inv_a2 * p.inv_dx2), ne = (float)(-p.eta);
+        p.k2.lap_scale = make_float2(ls, ls);
+        p.k2.neg_eta = make_float2(ne, ne);
     }
     p.step += s;
 }
@@ -170,6 +176,10 @@ __host__ __device__ inline void set_f32c_pairs(RealStageParams& p) {
     p.k2.c3 = pr((float)p.c3);
     p.k2.tmin = pr((float)p.tmin);
     p.k2.dinv = pr((float)p.dinv);
+    p.k2.lap_scale = pr((float)(p.inv_a2 * p.inv_dx2));
+    p.k2.neg_eta = pr((float)(-p.eta));
+    p.k2.neg_imu2 = pr((float)(-p.inv_mu2));
+    p.k2.tmd = pr((float)(-p.tmin * p.dinv));
 }
 
 // A lane-pair constant as a lane vector.
@@ -222,8 +232,8 @@ __device__ __forceinline__ V vprime_v(const RealStageParams& p, const F32CConst&
                                                  (double)vlane(x, l)));
         return r;
     }
-    return lerp_table_f32<V>(s_tab, v_mul(v_sub(x, kvec<V>(p.k2.tmin)), kvec<V>(p.k2.dinv)),
-                             kc.last);
+    // fractional index x dinv - tmin dinv (one rounding; the compensated-FP32 rule)
+    return lerp_table_f32<V>(s_tab, v_fma(x, kvec<V>(p.k2.dinv), kvec<V>(p.k2.tmd)), kc.last);
 }
 
 // Noise increment for one site (FP64): array value * nfac, or ns_eff * z.
@@ -308,6 +318,12 @@ __device__ __forceinline__ V force_v(V inv_a2, V eta, V inv_mu2, V lap, V pv, V 
     return v_sub(v_sub(v_mul(inv_a2, lap), v_mul(eta, pv)), v_mul(dv, inv_mu2));
 }
 
+// The same from lapA = inv_a2 lap as two fused multiply-adds (the real field).
+template <typename V>
+__device__ __forceinline__ V force_fma(V neg_eta, V neg_imu2, V lapA, V pv, V dv) {
+    return v_fma(neg_imu2, dv, v_fma(neg_eta, pv, lapA));
+}
+
 // The part of the site update that reads only the centre values: the centre
 // and midpoint fields and V' at both (marching kernels evaluate it before the
 // neighbouring plane arrives).
@@ -338,25 +354,25 @@ __device__ __forceinline__ void post_f32c(const RealStageParams& p, const F32CIn
     const V h1 = kvec<V>(p.k2.h1);
     const V h2h = kvec<V>(p.k2.h2h);
     const V h2l = kvec<V>(p.k2.h2l);
-    const V inv_dx2 = kvec<V>(p.k2.inv_dx2);
-    const V inv_a2 = kvec<V>(p.k2.inv_a2), eta = kvec<V>(p.k2.eta),
-            inv_mu2 = kvec<V>(p.k2.inv_mu2);
-    const V lap = v_mul(v_add(x.dh_phi, x.dl_phi), inv_dx2);
-    const V lapv = v_mul(v_add(x.dh_pi, x.dl_pi), inv_dx2);
-    const V lap2 = v_fma(h1, lapv, lap);  // Laplacian of phi + h1 pi
+    const V lsc = kvec<V>(p.k2.lap_scale);
+    const V neg_eta = kvec<V>(p.k2.neg_eta), neg_imu2 = kvec<V>(p.k2.neg_imu2);
+    // Laplacians times inv_a2 (inv_a2 inv_dx2 applied once)
+    const V lap = v_mul(v_add(x.dh_phi, x.dl_phi), lsc);
+    const V lapv = v_mul(v_add(x.dh_pi, x.dl_pi), lsc);
+    const V lap2 = v_fma(h1, lapv, lap);  // of phi + h1 pi
     const V pvc = pre.pvc;
-    const V k1 = force_v(inv_a2, eta, inv_mu2, lap, pvc, pre.v1);
+    const V k1 = force_fma(neg_eta, neg_imu2, lap, pvc, pre.v1);
     // pi~ = pi + h1 k1 as {t_hi, t_lo}
     V t_hi, t_e;
     two_sum(x.pih, v_mul(h1, k1), t_hi, t_e);
     const V t_lo = v_add(x.pil, t_e);
     const V pit = v_add(t_hi, t_lo);
-    const V k2 = force_v(inv_a2, eta, inv_mu2, lap2, pit, pre.v2);
+    const V k2 = force_fma(neg_eta, neg_imu2, lap2, pit, pre.v2);
     // phi + h2 pi~ with the product's rounding error kept
     const V d_hi = v_mul(h2h, t_hi);
     const V d_lo = v_add(v_fma(h2h, t_hi, v_neg(d_hi)), v_fma(h2h, t_lo, v_mul(h2l, t_hi)));
     ff_add(x.phh, x.phl, d_hi, d_lo, phh, phl);
-    ff_add(x.pih, x.pil, v_fma(h2h, k2, kick), vs<V>(0.0f), pih, pil);
+    ff_add1(x.pih, x.pil, v_fma(h2h, k2, kick), pih, pil);
 }
 
 template <typename V, bool TH = true>

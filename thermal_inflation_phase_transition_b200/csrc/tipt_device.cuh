@@ -144,19 +144,24 @@ __device__ __forceinline__ float2 v_neg(float2 a) { return make_float2(-a.x, -a.
 
 // FP32 Box-Muller for the compensated-FP32 storage.  The hash is the same
 // integer computation; only the Gaussian transform runs in FP32, from the
-// 53-bit integers m1, m2 (u = m * 2^-53) held as 32-bit halves (hi < 2^21):
-//  * log(u1): the atanh series of log(1 + g), g = u1 - 1 formed exactly from
-//    the halves, for u1 >= 1/2; the hardware base-2 logarithm for u1 < 1/2
-//    (log_u1 below).  The reference's clamp u1 >= 1e-12 is m1 <= 9007.
-//  * cos/sin(2 pi u2) (complex field): 2 u2 = m2 * 2^-52; the nearest quarter
-//    turn q is read from the high half (exact), the remainder x lies in
-//    [-pi/4, pi/4] and the Taylor series of sin (to x^9) and cos (to x^10) are
-//    truncated below 3e-9.  cos alone (real field): the nearest half turn, x in
-//    [-pi/2, pi/2] and the cos series to x^12 (truncated below 7e-9).
+// 53-bit integers m1, m2 (u = m * 2^-53):
+//  * log(u1), from the halves h1 = m1 >> 32 (< 2^21) and l1 = m1 mod 2^32: the
+//    atanh series of log(1 + g), g = u1 - 1 formed exactly from the halves,
+//    for u1 >= 1/2; the hardware base-2 logarithm for u1 < 1/2 (log_u1 below).
+//    The reference's clamp u1 >= 1e-12 is applied to the FP32 value of u1.
+//  * the angle 2 pi u2, from the top 31 bits t2 of m2 (u2 = t2 2^-31 to within
+//    2^-31, an angle error below 3e-9): cos alone (real field) by the nearest
+//    half turn, x in [-pi/2, pi/2] and the Taylor series of cos to x^12
+//    (truncated below 7e-9); cos and sin (complex field) by the nearest quarter
+//    turn, x in [-pi/4, pi/4] and the series of sin (to x^9) and cos (to x^10),
+//    truncated below 3e-9.
 //  * sqrt via rsqrt and one Newton step.
 // The absolute error of z against the FP64 reference value is a few 1e-7.
-__device__ __forceinline__ void hash_words(uint64_t x, uint32_t& h1, uint32_t& l1, uint32_t& h2,
-                                           uint32_t& l2) {
+//
+// hash_words: the three words of the hash the FP32 transform reads.  t2 = bits
+// 33..63 of the last product, which the final x ^= x >> 31 of R:2334 leaves
+// unchanged (it alters bits 0..32 only), so that step is skipped for m2.
+__device__ __forceinline__ void hash_words(uint64_t x, uint32_t& h1, uint32_t& l1, uint32_t& t2) {
     x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
     x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
     x = x ^ (x >> 31);
@@ -165,26 +170,21 @@ __device__ __forceinline__ void hash_words(uint64_t x, uint32_t& h1, uint32_t& l
     constexpr uint64_t kC = 0x9E3779B97F4A7C15ull, kCs = kC ^ (kC >> 30);
     x = x * 0x2545F4914F6CDD1Dull;
     x = (x ^ (x >> 30) ^ kCs) * 0xBF58476D1CE4E5B9ull;
-    x = x ^ (x >> 31);
-    const uint64_t m2 = x >> 11;
     h1 = (uint32_t)(m1 >> 32);
     l1 = (uint32_t)m1;
-    h2 = (uint32_t)(m2 >> 32);
-    l2 = (uint32_t)m2;
+    t2 = (uint32_t)(x >> 33);
 }
 
 
 // log(u1) for one lane from the halves h, l of m1 (u1 = m1 2^-53):
 //  * u1 >= 1/2: g = u1 - 1 = (h - 2^21) 2^-21 + l 2^-53 (exact to 2^-45), and
 //    log(1 + g) = 2 atanh(s), s = g / (2 + g) in [-1/3, 0], summed as
-//    2 s (1 + s^2/3 + ... + s^14/15) (the atanh series, truncated below 2e-8);
+//    2 s (1 + s^2/3 + ... + s^12/13) (the atanh series, truncated below 1e-8);
 //  * u1 < 1/2: log2(u1) ln 2 with the hardware base-2 logarithm (lg2.approx;
 //    |log2 u1| >= 1 there, so its absolute error of about 2^-22 is a relative
-//    error below 2e-7).
+//    error below 2e-7), u1 first clamped to 1e-12 (R:2336).
 // Both are formed and one is selected, so the lanes of a warp do not diverge.
-// The reference's clamp u1 >= 1e-12 is m1 <= 9007.
 constexpr float kLn2 = 0.693147182464599609375f;     // ln 2 rounded to FP32
-constexpr float kLog1em12 = -27.631021115928547f;    // log(1e-12)
 
 __device__ __forceinline__ float lg2_approx(float x) {
     float y;
@@ -209,8 +209,7 @@ __device__ __forceinline__ V log_u1_v(V hf, V lo) {
     else r = make_float2(rcp_approx(d.x), rcp_approx(d.y));
     const V s = v_mul(g, r);
     const V w = v_mul(s, s);
-    V poly = v_fma(w, vs<V>(1.0f / 15.0f), vs<V>(1.0f / 13.0f));
-    poly = v_fma(w, poly, vs<V>(1.0f / 11.0f));
+    V poly = v_fma(w, vs<V>(1.0f / 13.0f), vs<V>(1.0f / 11.0f));
     poly = v_fma(w, poly, vs<V>(1.0f / 9.0f));
     poly = v_fma(w, poly, vs<V>(1.0f / 7.0f));
     poly = v_fma(w, poly, vs<V>(1.0f / 5.0f));
@@ -220,13 +219,17 @@ __device__ __forceinline__ V log_u1_v(V hf, V lo) {
     return v_fma(two_s, poly, two_s);  // log(1 + g): the u1 >= 1/2 branch
 }
 
+// log(u1) of the u1 < 1/2 branch for one lane from u1 in FP32
+__device__ __forceinline__ float log_far(float u) {
+    return __fmul_rn(lg2_approx(fmaxf(u, 1e-12f)), kLn2);
+}
+
 __device__ __forceinline__ float log_u1(uint32_t h, uint32_t l) {
     const float lo = __fmul_rn((float)l, 0x1p-53f);
     const float hf = (float)h;  // exact: h < 2^21
     const float near = log_u1_v<float>(hf, lo);
-    const float far = __fmul_rn(lg2_approx(__fmaf_rn(hf, 0x1p-21f, lo)), kLn2);
-    const float lg = h >= (1u << 20) ? near : far;
-    return (h == 0u && l <= 9007u) ? kLog1em12 : lg;
+    const float far = log_far(__fmaf_rn(hf, 0x1p-21f, lo));
+    return h >= (1u << 20) ? near : far;
 }
 
 // log_u1 for two keys in the lanes of a float2.
@@ -235,19 +238,16 @@ __device__ __forceinline__ float2 log_u1_2(uint32_t ha, uint32_t la, uint32_t hb
     const float2 hf = make_float2((float)ha, (float)hb);
     const float2 near = log_u1_v<float2>(hf, lo);
     const float2 u = v_fma(hf, vs<float2>(0x1p-21f), lo);
-    const float2 far = v_mul(make_float2(lg2_approx(u.x), lg2_approx(u.y)), vs<float2>(kLn2));
-    float2 lg = make_float2(ha >= (1u << 20) ? near.x : far.x, hb >= (1u << 20) ? near.y : far.y);
-    lg.x = (ha == 0u && la <= 9007u) ? kLog1em12 : lg.x;
-    lg.y = (hb == 0u && lb <= 9007u) ? kLog1em12 : lg.y;
-    return lg;
+    return make_float2(ha >= (1u << 20) ? near.x : log_far(u.x),
+                       hb >= (1u << 20) ? near.y : log_far(u.y));
 }
 
-// Integer half of the angle reduction: quarter turns q and the remainder x.
-__device__ __forceinline__ void angle_reduce(uint32_t h, uint32_t l, uint32_t& q, float& x) {
-    q = (h + (1u << 18)) >> 19;                        // nearest multiple of 2^51 in m2
-    const int rh = (int)h - (int)(q << 19);            // |rh| <= 2^18, exact in FP32
-    // x = pi * 2^-52 * (rh 2^32 + l)
-    x = __fmaf_rn((float)rh, 2.99605662e-6f /* pi 2^-20 */, __fmul_rn((float)l, 6.97573699e-16f));
+// Quarter-turn reduction of 2 pi u2 (u2 = t 2^-31): q = round(4 u2) and the
+// remainder x = 2 pi u2 - q pi/2 in [-pi/4, pi/4].
+__device__ __forceinline__ void angle_reduce(uint32_t t, uint32_t& q, float& x) {
+    q = (t + (1u << 28)) >> 29;                        // nearest multiple of 2^29
+    const int rh = (int)t - (int)(q << 29);            // |rh| <= 2^28
+    x = __fmul_rn((float)rh, 0x1.921fb6p-29f /* (pi/2) 2^-29, rounded to FP32 */);
 }
 
 __device__ __forceinline__ void sincos_series1(float x, float& sn, float& cs) {
@@ -293,16 +293,12 @@ __device__ __forceinline__ V radius_from_log(V lg) {
 }
 
 // cos(2 pi u2) alone (the real field draws only the cos branch): half-turn
-// reduction 2 u2 = q + x/pi with q = round(m2 2^-52) in {0, 1, 2} and
-// x in [-pi/2, pi/2], cos = (-1)^q cos x; the Taylor series of cos x to x^12
-// is truncated below 7e-9 on that interval.  Returns the sign bit (q odd) with
-// the cos x value.
-__device__ __forceinline__ void half_turn_reduce(uint32_t h, uint32_t l, uint32_t& sign,
-                                                 float& x) {
-    const uint32_t q = (h + (1u << 19)) >> 20;        // nearest multiple of 2^52 in m2
-    const int rh = (int)h - (int)(q << 20);            // |rh| <= 2^19, exact in FP32
-    // x = pi * 2^-52 * (rh 2^32 + l)
-    x = __fmaf_rn((float)rh, 2.99605662e-6f /* pi 2^-20 */, __fmul_rn((float)l, 6.97573699e-16f));
+// reduction 2 u2 = q + x/pi with q = round(2 u2) in {0, 1, 2} and
+// x in [-pi/2, pi/2], cos = (-1)^q cos x.  Returns the sign bit (q odd) with x.
+__device__ __forceinline__ void half_turn_reduce(uint32_t t, uint32_t& sign, float& x) {
+    const uint32_t q = (t + (1u << 29)) >> 30;         // nearest multiple of 2^30
+    const int rh = (int)t - (int)(q << 30);            // |rh| <= 2^29
+    x = __fmul_rn((float)rh, 0x1.921fb6p-29f /* pi 2^-30, rounded to FP32 */);
     sign = q << 31;                                    // q = 2 shifts out: even
 }
 
@@ -323,24 +319,24 @@ __device__ __forceinline__ float flip_sign(float v, uint32_t sign) {
 
 // z (cos branch) for one key, FP32.
 __device__ __forceinline__ float gauss_cos_f(uint64_t key) {
-    uint32_t h1, l1, h2, l2, sg;
-    hash_words(key, h1, l1, h2, l2);
+    uint32_t h1, l1, t2, sg;
+    hash_words(key, h1, l1, t2);
     float x;
     const float lg = log_u1(h1, l1);
-    half_turn_reduce(h2, l2, sg, x);
+    half_turn_reduce(t2, sg, x);
     return __fmul_rn(radius_from_log<float>(lg), flip_sign(cos_series<float>(x), sg));
 }
 
 // z for two keys in the two lanes of a float2 (bitwise the same as two calls
 // of gauss_cos_f).
 __device__ __forceinline__ float2 gauss_cos_f2(uint64_t key0, uint64_t key1) {
-    uint32_t h1a, l1a, h2a, l2a, h1b, l1b, h2b, l2b, sa, sb;
-    hash_words(key0, h1a, l1a, h2a, l2a);
-    hash_words(key1, h1b, l1b, h2b, l2b);
+    uint32_t h1a, l1a, t2a, h1b, l1b, t2b, sa, sb;
+    hash_words(key0, h1a, l1a, t2a);
+    hash_words(key1, h1b, l1b, t2b);
     float xa, xb;
     const float2 lg = log_u1_2(h1a, l1a, h1b, l1b);
-    half_turn_reduce(h2a, l2a, sa, xa);
-    half_turn_reduce(h2b, l2b, sb, xb);
+    half_turn_reduce(t2a, sa, xa);
+    half_turn_reduce(t2b, sb, xb);
     const float2 cx = cos_series<float2>(make_float2(xa, xb));
     const float2 c = make_float2(flip_sign(cx.x, sa), flip_sign(cx.y, sb));
     return v_mul(radius_from_log<float2>(lg), c);
@@ -348,11 +344,11 @@ __device__ __forceinline__ float2 gauss_cos_f2(uint64_t key0, uint64_t key1) {
 
 // (z1, z2) = r (cos, sin) for one key (complex field, one pair per site).
 __device__ __forceinline__ void gauss_pair_f(uint64_t key, float& z1, float& z2) {
-    uint32_t h1, l1, h2, l2, q;
-    hash_words(key, h1, l1, h2, l2);
+    uint32_t h1, l1, t2, q;
+    hash_words(key, h1, l1, t2);
     float x, sn, cs, c, s;
     const float lg = log_u1(h1, l1);
-    angle_reduce(h2, l2, q, x);
+    angle_reduce(t2, q, x);
     sincos_series<float>(x, sn, cs);
     quarter_turn(q, sn, cs, c, s);
     const float r = radius_from_log<float>(lg);
@@ -364,13 +360,13 @@ __device__ __forceinline__ void gauss_pair_f(uint64_t key, float& z1, float& z2)
 // calls of gauss_pair_f).
 __device__ __forceinline__ void gauss_pair_f2(uint64_t key0, uint64_t key1, float2& z1,
                                               float2& z2) {
-    uint32_t h1a, l1a, h2a, l2a, h1b, l1b, h2b, l2b, qa, qb;
-    hash_words(key0, h1a, l1a, h2a, l2a);
-    hash_words(key1, h1b, l1b, h2b, l2b);
+    uint32_t h1a, l1a, t2a, h1b, l1b, t2b, qa, qb;
+    hash_words(key0, h1a, l1a, t2a);
+    hash_words(key1, h1b, l1b, t2b);
     float xa, xb;
     const float2 lg = log_u1_2(h1a, l1a, h1b, l1b);
-    angle_reduce(h2a, l2a, qa, xa);
-    angle_reduce(h2b, l2b, qb, xb);
+    angle_reduce(t2a, qa, xa);
+    angle_reduce(t2b, qb, xb);
     float2 sn, cs;
     sincos_series<float2>(make_float2(xa, xb), sn, cs);
     float2 c, s;
@@ -398,6 +394,16 @@ __device__ __forceinline__ void ff_add(V ahi, V alo, V dhi, V dlo, V& hi, V& lo)
     V s, e;
     two_sum(ahi, dhi, s, e);
     const V t = v_add(v_add(alo, dlo), e);
+    hi = v_add(s, t);
+    lo = v_sub(t, v_sub(hi, s));
+}
+
+// (hi, lo) + d for a single FP32 increment d, renormalised.
+template <typename V>
+__device__ __forceinline__ void ff_add1(V ahi, V alo, V d, V& hi, V& lo) {
+    V s, e;
+    two_sum(ahi, d, s, e);
+    const V t = v_add(alo, e);
     hi = v_add(s, t);
     lo = v_sub(t, v_sub(hi, s));
 }
@@ -436,20 +442,26 @@ __device__ __forceinline__ void vset(float2& v, int l, float x) {
     else v.x = x;
 }
 
+__device__ __forceinline__ float v_add_rz(float a, float b) { return __fadd_rz(a, b); }
+__device__ __forceinline__ float2 v_add_rz(float2 a, float2 b) { return __fadd2_rz(a, b); }
+
 template <typename V>
 __device__ __forceinline__ V lerp_table_f32(const float* s_tab, V fidx, float last) {
     constexpr int NL = sizeof(V) / sizeof(float);
-    V fi, a, b;
+    V c;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) vset(c, l, fminf(fmaxf(vlane(fidx, l), 0.0f), last));
+    // c in [0, last]: c + 2^23 rounded toward zero is trunc(c) + 2^23 exactly, so
+    // its low mantissa bits are the index and subtracting 2^23 gives trunc(c)
+    const V t = v_add_rz(c, vs<V>(0x1p23f));
+    V a, b;
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-        float c = vlane(fidx, l);
-        c = c > 0.0f ? c : 0.0f;
-        c = c < last ? c : last;
-        const int idx = (int)c;
-        vset(fi, l, (float)idx);
+        const int idx = (int)(__float_as_uint(vlane(t, l)) - 0x4B000000u);
         vset(a, l, s_tab[idx]);
         vset(b, l, s_tab[idx + 1]);
     }
+    const V fi = v_sub(t, vs<V>(0x1p23f));
     return v_fma(v_sub(fidx, fi), v_sub(b, a), a);
 }
 

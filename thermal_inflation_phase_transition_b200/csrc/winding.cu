@@ -17,11 +17,6 @@ constexpr double kPiD = 3.141592653589793;  // the double nearest pi (numpy's np
 
 __device__ __forceinline__ int wrap_count(double d) { return d > kPiD ? 1 : (d < -kPiD ? -1 : 0); }
 
-// Winding of the loop a -> b -> c -> e -> a.
-__device__ __forceinline__ int plaquette(double a, double b, double c, double e) {
-    return -(wrap_count(b - a) + wrap_count(c - b) + wrap_count(e - c) + wrap_count(a - e));
-}
-
 // Site value in FP64; F32C is planar (hi plane, then lo plane N sites later).
 template <int S>
 __device__ __forceinline__ double load_field(const void* p, int64_t s, int64_t N) {
@@ -44,61 +39,110 @@ struct WindParams {
     unsigned long long* counts;  // [5]
 };
 
-template <int S>
-__global__ void __launch_bounds__(256) winding_kernel(WindParams p) {
+// Tiled kernel.  A block takes a tile of TI x TJ x TK sites (k contiguous) and
+// its forward halo (one more plane, row and column, periodic): the phase of
+// every halo-region site is computed once (FP64 atan2 of the FP64 field
+// values, as the reference computes it on FP64 casts, C:4627-4629) into shared
+// memory, then the wrap count of each forward edge,
+//   e_i(s) = wrap(theta(s + i) - theta(s)),  e_j, e_k alike,
+// and every plaquette is a signed sum of four edge counts: the reference's
+// atan2(sin d, cos d) over an edge traversed backwards is the wrap of -d, and
+// IEEE subtraction gives (a - b) = -(b - a) exactly, so wrap(-d) = -wrap(d):
+//   XY(s) = -(e_i(s) + e_j(s + i) - e_i(s + j) - e_j(s)),  XZ, YZ alike.
+// One atan2 per region site instead of seven per site, and 3 FP64
+// differences per site instead of 12; the decisions are those of the
+// reference's per-plaquette differences bit for bit.
+template <int TK>
+struct WindTile {
+    static constexpr int TJ = TK == 32 ? 8 : (TK == 8 ? 16 : 64);
+    static constexpr int TI = TK == 32 ? 8 : (TK == 8 ? 16 : 32);
+    static constexpr int RI = TI + 1, RJ = TJ + 1, RK = TK + 1;
+    static constexpr int REGION = RI * RJ * RK;
+    static constexpr int INTERIOR = TI * TJ * TK;
+};
+
+template <int S, int TK>
+__global__ void __launch_bounds__(256) winding_tiled_kernel(WindParams p) {
+    using W = WindTile<TK>;
+    __shared__ double s_th[W::REGION];
+    __shared__ int8_t s_e[3][W::REGION];
     const int64_t n12 = (int64_t)p.n1 * p.n2;
     const int64_t N = (int64_t)p.n0 * n12;
+    const int nti = (p.n0 + W::TI - 1) / W::TI, ntj = (p.n1 + W::TJ - 1) / W::TJ,
+              ntk = (p.n2 + TK - 1) / TK;
+    const int64_t tiles = (int64_t)nti * ntj * ntk;
     const unsigned lane = threadIdx.x & 31;
-    // grid-stride loop with a warp-uniform trip count (ballots need full warps)
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const int64_t start = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
     unsigned long long c_xy = 0, c_xz = 0, c_yz = 0, c_str = 0;
-    for (int64_t base = start; base < N; base += stride) {
-        const int64_t s = base + lane;
-        const bool live = s < N;
-        int wxy = 0, wxz = 0, wyz = 0;
-        if (live) {
-            const int k = (int)(s % p.n2);
-            const int64_t r = s / p.n2;
-            const int j = (int)(r % p.n1);
-            const int i = (int)(r / p.n1);
-            const int64_t oi = (i + 1 < p.n0) ? n12 : -(int64_t)(p.n0 - 1) * n12;
-            const int64_t oj = (j + 1 < p.n1) ? (int64_t)p.n2 : -(int64_t)(p.n1 - 1) * p.n2;
-            const int64_t ok = (k + 1 < p.n2) ? 1 : -(int64_t)(p.n2 - 1);
-            auto th = [&](int64_t q) { return atan2(load_field<S>(p.phi2, q, N), load_field<S>(p.phi1, q, N)); };
-            const double t00 = th(s), t10 = th(s + oi), t11 = th(s + oi + oj), t01 = th(s + oj);
-            const double t1k = th(s + oi + ok), t0k = th(s + ok), tj1k = th(s + oj + ok);
-            wxy = plaquette(t00, t10, t11, t01);   // (i,j)->(i+1,j)->(i+1,j+1)->(i,j+1)
-            wxz = plaquette(t00, t10, t1k, t0k);   // (i,k)->(i+1,k)->(i+1,k+1)->(i,k+1)
-            wyz = plaquette(t00, t01, tj1k, t0k);  // (j,k)->(j+1,k)->(j+1,k+1)->(j,k+1)
-            const int w = wxy + wxz + wyz;
-            if (p.w_site) p.w_site[s] = (float)w;
-            if (p.w3) {
-                p.w3[s] = (int8_t)wxy;
-                p.w3[N + s] = (int8_t)wxz;
-                p.w3[2 * N + s] = (int8_t)wyz;
-            }
-            c_xy += wxy != 0;
-            c_xz += wxz != 0;
-            c_yz += wyz != 0;
-            c_str += (w > 0 ? w : -w) > 0;  // |w| > 0.5 for integer w
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int tk = (int)(tile % ntk);
+        const int64_t tr = tile / ntk;
+        const int tj = (int)(tr % ntj), ti = (int)(tr / ntj);
+        const int i0 = ti * W::TI, j0 = tj * W::TJ, k0 = tk * TK;
+        // phases of the region (coordinates taken modulo the lattice)
+        for (int q = threadIdx.x; q < W::REGION; q += blockDim.x) {
+            const int c = q % W::RK, rr = q / W::RK;
+            const int b = rr % W::RJ, a = rr / W::RJ;
+            const int i = (i0 + a) % p.n0, j = (j0 + b) % p.n1, k = (k0 + c) % p.n2;
+            const int64_t sq = (int64_t)i * n12 + (int64_t)j * p.n2 + k;
+            s_th[q] = atan2(load_field<S>(p.phi2, sq, N), load_field<S>(p.phi1, sq, N));
         }
-        if (p.pierced) {
-            // warp-ballot compaction: one atomic per warp and orientation
-            const int wo[3] = {wxy, wxz, wyz};
+        __syncthreads();
+        // forward-edge wrap counts (the far faces are never read)
+        for (int q = threadIdx.x; q < W::REGION; q += blockDim.x) {
+            const int c = q % W::RK, rr = q / W::RK;
+            const int b = rr % W::RJ, a = rr / W::RJ;
+            const double t = s_th[q];
+            s_e[0][q] = (int8_t)(a < W::TI ? wrap_count(s_th[q + W::RJ * W::RK] - t) : 0);
+            s_e[1][q] = (int8_t)(b < W::TJ ? wrap_count(s_th[q + W::RK] - t) : 0);
+            s_e[2][q] = (int8_t)(c < TK ? wrap_count(s_th[q + 1] - t) : 0);
+        }
+        __syncthreads();
+        // plaquettes: warp-uniform trip count (the ballots need full warps)
+        for (int q0 = threadIdx.x & ~31; q0 < W::INTERIOR; q0 += blockDim.x) {
+            const int q = q0 + (int)lane;
+            const int c = q % TK, rr = q / TK;
+            const int b = rr % W::TJ, a = rr / W::TJ;
+            const int i = i0 + a, j = j0 + b, k = k0 + c;
+            const bool live = i < p.n0 && j < p.n1 && k < p.n2;
+            int wxy = 0, wxz = 0, wyz = 0;
+            int64_t s = 0;
+            if (live) {
+                const int r0 = (a * W::RJ + b) * W::RK + c;
+                const int ri = r0 + W::RJ * W::RK, rj = r0 + W::RK, rk = r0 + 1;
+                wxy = -(s_e[0][r0] + s_e[1][ri] - s_e[0][rj] - s_e[1][r0]);
+                wxz = -(s_e[0][r0] + s_e[2][ri] - s_e[0][rk] - s_e[2][r0]);
+                wyz = -(s_e[1][r0] + s_e[2][rj] - s_e[1][rk] - s_e[2][r0]);
+                s = (int64_t)i * n12 + (int64_t)j * p.n2 + k;
+                const int w = wxy + wxz + wyz;
+                if (p.w_site) p.w_site[s] = (float)w;
+                if (p.w3) {
+                    p.w3[s] = (int8_t)wxy;
+                    p.w3[N + s] = (int8_t)wxz;
+                    p.w3[2 * N + s] = (int8_t)wyz;
+                }
+                c_xy += wxy != 0;
+                c_xz += wxz != 0;
+                c_yz += wyz != 0;
+                c_str += w != 0;  // |w| > 0.5 for integer w
+            }
+            if (p.pierced) {
+                // warp-ballot compaction: one atomic per warp and orientation
+                const int wo[3] = {wxy, wxz, wyz};
 #pragma unroll
-            for (int o = 0; o < 3; ++o) {
-                const unsigned m = __ballot_sync(0xffffffffu, live && wo[o] != 0);
-                if (m == 0) continue;
-                unsigned long long b0 = 0;
-                if (lane == 0) b0 = atomicAdd(&p.counts[4], (unsigned long long)__popc(m));
-                b0 = __shfl_sync(0xffffffffu, b0, 0);
-                if (live && wo[o] != 0) {
-                    const unsigned long long slot = b0 + __popc(m & ((1u << lane) - 1u));
-                    if ((int64_t)slot < p.cap) p.pierced[slot] = (uint32_t)(s * 3 + o);
+                for (int o = 0; o < 3; ++o) {
+                    const unsigned m = __ballot_sync(0xffffffffu, live && wo[o] != 0);
+                    if (m == 0) continue;
+                    unsigned long long b0 = 0;
+                    if (lane == 0) b0 = atomicAdd(&p.counts[4], (unsigned long long)__popc(m));
+                    b0 = __shfl_sync(0xffffffffu, b0, 0);
+                    if (live && wo[o] != 0) {
+                        const unsigned long long slot = b0 + __popc(m & ((1u << lane) - 1u));
+                        if ((int64_t)slot < p.cap) p.pierced[slot] = (uint32_t)(s * 3 + o);
+                    }
                 }
             }
         }
+        __syncthreads();  // the region buffers are refilled by the next tile
     }
     // warp totals -> one atomic per warp and counter
 #pragma unroll
@@ -153,14 +197,28 @@ extern "C" int tipt_compute_winding_number(int storage, const void* phi1, const 
     p.pierced = pierced;
     p.cap = pierced ? pierced_cap : 0;
     p.counts = reinterpret_cast<unsigned long long*>(counts);
-    const int64_t N = nx * ny * nz;
-    int64_t blocks = (N + 255) / 256;
-    const int64_t capb = (int64_t)num_sms() * 8;
-    if (blocks > capb) blocks = capb;
-    switch (storage) {
-        case TIPT_F64: winding_kernel<TIPT_F64><<<(unsigned)blocks, 256, 0, st>>>(p); break;
-        case TIPT_F32: winding_kernel<TIPT_F32><<<(unsigned)blocks, 256, 0, st>>>(p); break;
-        default: winding_kernel<TIPT_F32C><<<(unsigned)blocks, 256, 0, st>>>(p); break;
+    // tile shape by the contiguous extent: 8 x 8 x 32, 16 x 16 x 8 or 32 x 64 x 1
+    const int tk = nz >= 24 ? 32 : (nz >= 6 ? 8 : 1);
+    const int64_t cap_blocks = (int64_t)num_sms() * 8;
+    auto grid = [&](int ti, int tj, int tkk) {
+        const int64_t nb = ((nx + ti - 1) / ti) * ((ny + tj - 1) / tj) * ((nz + tkk - 1) / tkk);
+        return (unsigned)(nb < cap_blocks ? nb : cap_blocks);
+    };
+    if (tk == 32) {
+        const unsigned nb = grid(WindTile<32>::TI, WindTile<32>::TJ, 32);
+        if (storage == TIPT_F64) winding_tiled_kernel<TIPT_F64, 32><<<nb, 256, 0, st>>>(p);
+        else if (storage == TIPT_F32) winding_tiled_kernel<TIPT_F32, 32><<<nb, 256, 0, st>>>(p);
+        else winding_tiled_kernel<TIPT_F32C, 32><<<nb, 256, 0, st>>>(p);
+    } else if (tk == 8) {
+        const unsigned nb = grid(WindTile<8>::TI, WindTile<8>::TJ, 8);
+        if (storage == TIPT_F64) winding_tiled_kernel<TIPT_F64, 8><<<nb, 256, 0, st>>>(p);
+        else if (storage == TIPT_F32) winding_tiled_kernel<TIPT_F32, 8><<<nb, 256, 0, st>>>(p);
+        else winding_tiled_kernel<TIPT_F32C, 8><<<nb, 256, 0, st>>>(p);
+    } else {
+        const unsigned nb = grid(WindTile<1>::TI, WindTile<1>::TJ, 1);
+        if (storage == TIPT_F64) winding_tiled_kernel<TIPT_F64, 1><<<nb, 256, 0, st>>>(p);
+        else if (storage == TIPT_F32) winding_tiled_kernel<TIPT_F32, 1><<<nb, 256, 0, st>>>(p);
+        else winding_tiled_kernel<TIPT_F32C, 1><<<nb, 256, 0, st>>>(p);
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "winding launch");

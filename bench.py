@@ -279,6 +279,8 @@ def main():
     ap.add_argument("--prec-steps", type=int, default=10000,
                     help="steps of the precision workload (FP32C beside FP64)")
     ap.add_argument("--ens-steps", type=int, default=2000)
+    ap.add_argument("--ens-scale", type=int, default=1,
+                    help="divide the replica counts of the ensemble workload (profiling runs)")
     ap.add_argument("--ens-plain", type=int, default=6,
                     help="replicas per size class timed one at a time")
     args = ap.parse_args()
@@ -557,7 +559,8 @@ def run_ensemble_bench(args):
     import torch
     from thermal_inflation_phase_transition_b200 import ensemble as EN
     torch.cuda.set_device(0)
-    specs = EN.mixed_lattice_specs()
+    sc = max(1, args.ens_scale)
+    specs = EN.mixed_lattice_specs(n128=1024 // sc, n64=512 // sc, n96=256 // sc)
     ens = EN.Ensemble(specs, check_every=10)
     torch.cuda.synchronize()
     t0 = time.perf_counter()

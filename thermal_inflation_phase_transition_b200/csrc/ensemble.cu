@@ -111,18 +111,21 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
 #pragma unroll
                         for (int u = 0; u < 4; ++u)
                             nb[u] = __ldg(reinterpret_cast<const float2*>(b + g + o4[u]));
-                        nb[4] = make_float2(cc.y, __ldg(b + gkr));  // k+1
-                        nb[5] = make_float2(__ldg(b + gkl), cc.x);  // k-1
+                        const float kr = __ldg(b + gkr), kl = __ldg(b + gkl);  // k+1, k-1
+                        // the order of stencil_sums_k: i and j terms, then the k pair
                         float2 acc;
                         if ((f & 1) == 0) {  // hi: sum (hi_n - hi_c)
-                            acc = v_sub(nb[0], cc);
-#pragma unroll
-                            for (int n = 1; n < 6; ++n) acc = v_add(acc, v_sub(nb[n], cc));
+                            acc = v_add(v_sub(nb[0], cc), v_sub(nb[1], cc));
+                            acc = v_add(acc, v_sub(nb[2], cc));
+                            acc = v_add(acc, v_sub(nb[3], cc));
+                            const float2 kk = make_float2(
+                                __fadd_rn(__fsub_rn(cc.y, cc.x), __fsub_rn(kl, cc.x)),
+                                __fadd_rn(__fsub_rn(kr, cc.y), __fsub_rn(cc.x, cc.y)));
+                            acc = v_add(acc, kk);
                         } else {             // lo: fma(-6, lo_c, sum lo_n)
-                            acc = nb[0];
-#pragma unroll
-                            for (int n = 1; n < 6; ++n) acc = v_add(acc, nb[n]);
-                            acc = v_fma(vs<float2>(-6.0f), cc, acc);
+                            acc = v_add(v_add(v_add(nb[0], nb[1]), nb[2]), nb[3]);
+                            const float2 kk = make_float2(__fadd_rn(cc.y, kl), __fadd_rn(kr, cc.x));
+                            acc = v_fma(vs<float2>(-6.0f), cc, v_add(acc, kk));
                         }
                         dsum[f] = acc;
                         cen[f] = cc;
@@ -187,8 +190,8 @@ __global__ void __launch_bounds__(256) ensemble_stage_kernel(EnsParams e) {
                     vl[u] = __ldg(pi + N + idx[u]);
                 }
                 F32CIn<float> x;
-                stencil_sums(hh, hl, x.dh_phi, x.dl_phi);
-                stencil_sums(vh, vl, x.dh_pi, x.dl_pi);
+                stencil_sums_k(hh, hl, x.dh_phi, x.dl_phi);
+                stencil_sums_k(vh, vl, x.dh_pi, x.dl_pi);
                 x.phh = hh[0];
                 x.phl = hl[0];
                 x.pih = vh[0];

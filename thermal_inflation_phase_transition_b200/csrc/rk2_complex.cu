@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) complex_stage_generic(ComplexStageParams 
             CplxIn<float> in;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                stencil_sums(hi[f], lo[f], in.dh[f], in.dl[f]);
+                stencil_sums_k(hi[f], lo[f], in.dh[f], in.dl[f]);
                 in.ch[f] = hi[f][0];
                 in.cl[f] = lo[f][0];
             }

@@ -122,7 +122,8 @@ __device__ __forceinline__ V cvprime_v(const ComplexStageParams& p, const float*
         const V d = v_fma(v_mul(v_mul(vs<V>((float)p.c3), x), x), x, v_mul(vs<V>((float)p.c1), x));
         return p.c2 != 0.0 ? v_fma(v_mul(vs<V>((float)p.c2), x), x, d) : d;
     }
-    return lerp_table_f32<V>(s_tab, v_mul(v_sub(x, vs<V>(tmin)), vs<V>(dinv)),
+    // fractional index x dinv - tmin dinv (one rounding; the compensated-FP32 rule)
+    return lerp_table_f32<V>(s_tab, v_fma(x, vs<V>(dinv), vs<V>(-tmin * dinv)),
                              (float)(p.npts - 2));
 }
 
@@ -168,19 +169,20 @@ __device__ __forceinline__ void complex_update_f32c(const ComplexStageParams& p,
     const float h2f = (float)p.h2;
     const V h2h = vs<V>(h2f);
     const V h2l = vs<V>((float)(p.h2 - (double)h2f));
-    const V inv_dx2 = vs<V>((float)p.inv_dx2);
-    const V inv_a2 = vs<V>((float)p.inv_a2), eta = vs<V>((float)p.eta),
-            inv_mu2 = vs<V>((float)p.inv_mu2);
+    // Laplacians times inv_a2 (inv_a2 inv_dx2 applied once); forces as two fused
+    // multiply-adds
+    const V lsc = vs<V>((float)(p.inv_a2 * p.inv_dx2));
+    const V neg_eta = vs<V>((float)(-p.eta)), neg_imu2 = vs<V>((float)(-p.inv_mu2));
     V lap[4], c[4];
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
-        lap[f] = v_mul(v_add(x.dh[f], x.dl[f]), inv_dx2);
+        lap[f] = v_mul(v_add(x.dh[f], x.dl[f]), lsc);
         c[f] = v_add(x.ch[f], x.cl[f]);
     }
     V d1, d2;
     force(c[0], c[1], 0, d1, d2);
-    const V k1[2] = {force_v(inv_a2, eta, inv_mu2, lap[0], c[2], d1),
-                     force_v(inv_a2, eta, inv_mu2, lap[1], c[3], d2)};
+    const V k1[2] = {force_fma(neg_eta, neg_imu2, lap[0], c[2], d1),
+                     force_fma(neg_eta, neg_imu2, lap[1], c[3], d2)};
     V t_hi[2], t_lo[2], pit[2], q[2];
 #pragma unroll
     for (int a = 0; a < 2; ++a) {
@@ -191,15 +193,14 @@ __device__ __forceinline__ void complex_update_f32c(const ComplexStageParams& p,
         q[a] = v_add(x.ch[a], v_fma(h1, c[2 + a], x.cl[a]));
     }
     force(q[0], q[1], 1, d1, d2);
-    const V k2[2] = {force_v(inv_a2, eta, inv_mu2, v_fma(h1, lap[2], lap[0]), pit[0], d1),
-                     force_v(inv_a2, eta, inv_mu2, v_fma(h1, lap[3], lap[1]), pit[1], d2)};
+    const V k2[2] = {force_fma(neg_eta, neg_imu2, v_fma(h1, lap[2], lap[0]), pit[0], d1),
+                     force_fma(neg_eta, neg_imu2, v_fma(h1, lap[3], lap[1]), pit[1], d2)};
 #pragma unroll
     for (int a = 0; a < 2; ++a) {
         const V d_hi = v_mul(h2h, t_hi[a]);
         const V d_lo = v_add(v_fma(h2h, t_hi[a], v_neg(d_hi)), v_fma(h2h, t_lo[a], v_mul(h2l, t_hi[a])));
         ff_add(x.ch[a], x.cl[a], d_hi, d_lo, oh[a], ol[a]);
-        ff_add(x.ch[2 + a], x.cl[2 + a], v_fma(h2h, k2[a], kick[a]), vs<V>(0.0f), oh[2 + a],
-               ol[2 + a]);
+        ff_add1(x.ch[2 + a], x.cl[2 + a], v_fma(h2h, k2[a], kick[a]), oh[2 + a], ol[2 + a]);
     }
 }
 

@@ -524,21 +524,19 @@ __global__ void __maxnreg__(kMarchRegs)
             // the centre plane is resident: its values and V' at the centre and
             // the midpoint are evaluated before the wait as well
             F32CPre<float2> pre[2];
-            {
-                float4 cen[2][2];  // [field][hi, lo]
+            float4 cen[2][2];  // [field][hi, lo], kept for the stencil after the wait
 #pragma unroll
-                for (int f = 0; f < 2; ++f)
+            for (int f = 0; f < 2; ++f)
 #pragma unroll
-                    for (int c = 0; c < 2; ++c)
-                        cen[f][c] = *reinterpret_cast<const float4*>(blk(pc.stage, f, c) + orow + k0);
+                for (int c = 0; c < 2; ++c)
+                    cen[f][c] = *reinterpret_cast<const float4*>(blk(pc.stage, f, c) + orow + k0);
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const auto pick = [h](const float4& v) {
-                        return h ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
-                    };
-                    pre[h] = pre_f32c<float2, TH>(p, kc, s_tab, pick(cen[0][0]), pick(cen[0][1]),
-                                                  pick(cen[1][0]), pick(cen[1][1]));
-                }
+            for (int h = 0; h < 2; ++h) {
+                const auto pick = [h](const float4& v) {
+                    return h ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+                };
+                pre[h] = pre_f32c<float2, TH>(p, kc, s_tab, pick(cen[0][0]), pick(cen[0][1]),
+                                              pick(cen[1][0]), pick(cen[1][1]));
             }
             if (!mbar_wait(&full[pp.stage], pp.phase)) {
                 if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
@@ -550,7 +548,7 @@ __global__ void __maxnreg__(kMarchRegs)
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
                     const float* sc = blk(pc.stage, f, c);
-                    const float4 ce = *reinterpret_cast<const float4*>(sc + orow + k0);
+                    const float4 ce = cen[f][c];
                     const float4 jm = *reinterpret_cast<const float4*>(sc + urow + k0);
                     const float4 jp = *reinterpret_cast<const float4*>(sc + drow + k0);
                     const float4 im = *reinterpret_cast<const float4*>(blk(pm.stage, f, c) + orow + k0);
@@ -559,25 +557,34 @@ __global__ void __maxnreg__(kMarchRegs)
                     // than lane shuffles, which this issue-bound kernel prefers to the
                     // 4-way bank conflict they remove)
                     const float kl = sc[orow + kml], kr = sc[orow + kpr];
-                    // site pairs (0,1) and (2,3): centre and the six neighbours
+                    // site pairs (0,1) and (2,3): centre and the i and j neighbours
                     const float2 cc[2] = {make_float2(ce.x, ce.y), make_float2(ce.z, ce.w)};
-                    const float2 nb[2][6] = {
+                    const float2 nb[2][4] = {
                         {make_float2(ip.x, ip.y), make_float2(im.x, im.y), make_float2(jp.x, jp.y),
-                         make_float2(jm.x, jm.y), make_float2(ce.y, ce.z), make_float2(kl, ce.x)},
+                         make_float2(jm.x, jm.y)},
                         {make_float2(ip.z, ip.w), make_float2(im.z, im.w), make_float2(jp.z, jp.w),
-                         make_float2(jm.z, jm.w), make_float2(ce.w, kr), make_float2(ce.y, ce.z)}};
+                         make_float2(jm.z, jm.w)}};
+                    // the four sites' values with their k neighbours: v[1..4] own, v[0], v[5]
+                    const float v[6] = {kl, ce.x, ce.y, ce.z, ce.w, kr};
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
+                        // lanes: sites 2h, 2h+1 (v indices 2h+1, 2h+2); the k pair of a
+                        // site is formed in its own lane (order of stencil_sums_k)
+                        const int a = 2 * h + 1, b = 2 * h + 2;
                         float2 acc;
                         if (c == 0) {  // dh = sum (hi_n - hi_c)
-                            acc = v_sub(nb[h][0], cc[h]);
-#pragma unroll
-                            for (int n = 1; n < 6; ++n) acc = v_add(acc, v_sub(nb[h][n], cc[h]));
+                            acc = v_add(v_sub(nb[h][0], cc[h]), v_sub(nb[h][1], cc[h]));
+                            acc = v_add(acc, v_sub(nb[h][2], cc[h]));
+                            acc = v_add(acc, v_sub(nb[h][3], cc[h]));
+                            const float2 kk = make_float2(
+                                __fadd_rn(__fsub_rn(v[a + 1], v[a]), __fsub_rn(v[a - 1], v[a])),
+                                __fadd_rn(__fsub_rn(v[b + 1], v[b]), __fsub_rn(v[b - 1], v[b])));
+                            acc = v_add(acc, kk);
                         } else {       // dl = fma(-6, lo_c, sum lo_n)
-                            acc = nb[h][0];
-#pragma unroll
-                            for (int n = 1; n < 6; ++n) acc = v_add(acc, nb[h][n]);
-                            acc = v_fma(vs<float2>(-6.0f), cc[h], acc);
+                            acc = v_add(v_add(v_add(nb[h][0], nb[h][1]), nb[h][2]), nb[h][3]);
+                            const float2 kk = make_float2(__fadd_rn(v[a + 1], v[a - 1]),
+                                                          __fadd_rn(v[b + 1], v[b - 1]));
+                            acc = v_fma(vs<float2>(-6.0f), cc[h], v_add(acc, kk));
                         }
                         if (f == 0) {
                             if (c == 0) { in[h].dh_phi = acc; in[h].phh = cc[h]; }
@@ -1056,20 +1063,22 @@ __global__ void __maxnreg__(kMarchRegs)
                     float kr = __shfl_down_sync(0xffffffffu, ce.x, 1);
                     if (lane == 0 || edge_l) kl = (split && edge_l) ? hv[2 * f + c] : sc[orow + kml];
                     if (lane == 31 || edge_r) kr = (split && edge_r) ? hv[2 * f + c] : sc[orow + kpr];
-                    // lanes = sites k0, k0+1; neighbours in the order ip, im, jp, jm, kp, km
-                    const float2 nb[6] = {ip, im, jp, jm, make_float2(ce.y, kr), make_float2(kl, ce.x)};
+                    // lanes = sites k0, k0+1; the i and j neighbours in the order ip, im,
+                    // jp, jm, then each site's k pair formed in its own lane (the order of
+                    // stencil_sums_k)
                     float2 acc;
                     if (c == 0) {  // dh = sum (hi_n - hi_c)
-                        acc = v_sub(nb[0], ce);
-#pragma unroll
-                        for (int n = 1; n < 6; ++n) acc = v_add(acc, v_sub(nb[n], ce));
-                        in.dh[f] = acc;
+                        acc = v_add(v_add(v_add(v_sub(ip, ce), v_sub(im, ce)), v_sub(jp, ce)),
+                                    v_sub(jm, ce));
+                        const float2 kk = make_float2(
+                            __fadd_rn(__fsub_rn(ce.y, ce.x), __fsub_rn(kl, ce.x)),
+                            __fadd_rn(__fsub_rn(kr, ce.y), __fsub_rn(ce.x, ce.y)));
+                        in.dh[f] = v_add(acc, kk);
                         in.ch[f] = ce;
                     } else {       // dl = fma(-6, lo_c, sum lo_n)
-                        acc = nb[0];
-#pragma unroll
-                        for (int n = 1; n < 6; ++n) acc = v_add(acc, nb[n]);
-                        in.dl[f] = v_fma(vs<float2>(-6.0f), ce, acc);
+                        acc = v_add(v_add(v_add(ip, im), jp), jm);
+                        const float2 kk = make_float2(__fadd_rn(ce.y, kl), __fadd_rn(kr, ce.x));
+                        in.dl[f] = v_fma(vs<float2>(-6.0f), ce, v_add(acc, kk));
                         in.cl[f] = ce;
                     }
                 }

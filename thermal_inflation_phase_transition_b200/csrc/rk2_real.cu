@@ -81,8 +81,8 @@ __global__ void __launch_bounds__(256) rk2_stage_generic(RealStageParams p_in) {
                 vl[q] = __ldg(pi + N + idx[q]);
             }
             F32CIn<float> x;
-            stencil_sums(hh, hl, x.dh_phi, x.dl_phi);
-            stencil_sums(vh, vl, x.dh_pi, x.dl_pi);
+            stencil_sums_k(hh, hl, x.dh_phi, x.dl_phi);
+            stencil_sums_k(vh, vl, x.dh_pi, x.dl_pi);
             x.phh = hh[0];
             x.phl = hl[0];
             x.pih = vh[0];

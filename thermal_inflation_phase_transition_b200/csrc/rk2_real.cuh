@@ -397,6 +397,22 @@ __device__ __forceinline__ void stencil_sums(const float hi[7], const float lo[7
     dl = __fmaf_rn(-6.0f, lo[0], dl);
 }
 
+// The real-field RK2 stage's order: the i and j terms in sequence, the two k
+// terms summed first and added last,
+//   dh = (((ip-c) + (im-c)) + (jp-c)) + (jm-c) + ((kp-c) + (km-c)),
+//   dl = fma(-6, lo_c, (((ip + im) + jp) + jm) + (kp + km));
+// the marching kernel forms the k pair of a site in its own lane (the site's
+// k neighbours lie in the neighbouring lanes of its packed pair).
+__device__ __forceinline__ void stencil_sums_k(const float hi[7], const float lo[7], float& dh,
+                                               float& dl) {
+    dh = __fadd_rn(__fsub_rn(hi[1], hi[0]), __fsub_rn(hi[2], hi[0]));
+    dh = __fadd_rn(dh, __fsub_rn(hi[3], hi[0]));
+    dh = __fadd_rn(dh, __fsub_rn(hi[4], hi[0]));
+    dh = __fadd_rn(dh, __fadd_rn(__fsub_rn(hi[5], hi[0]), __fsub_rn(hi[6], hi[0])));
+    dl = __fadd_rn(__fadd_rn(__fadd_rn(lo[1], lo[2]), lo[3]), lo[4]);
+    dl = __fmaf_rn(-6.0f, lo[0], __fadd_rn(dl, __fadd_rn(lo[5], lo[6])));
+}
+
 // Noise increment for one F32C site: array value * nfac, or ns * z (FP32 z).
 __device__ __forceinline__ float site_kick_f32c(const RealStageParams& p, const F32CConst& kc,
                                                 uint64_t site) {

@@ -315,6 +315,18 @@ int tipt_ensemble_step(int storage, const void* phi, const void* pi, void* phi_o
                        int32_t n_chunks, const int32_t* active, const tipt_step_params* sp,
                        const uint64_t* counter, int64_t offset, void* stream);
 
+/* The same step for the replicas rids[0..n_rids) of one 3-D shape class
+ * (n0 x n1 x n2, n2 % 4 == 0, n0 >= 2), compensated-FP32 storage, on the
+ * marching stage (shared-memory tiles fed by bulk copies); bitwise equal to
+ * tipt_ensemble_step for those replicas.  The packed buffers (and n_total * 4
+ * bytes) must be 16-byte aligned; the replicas' offsets multiples of 4 sites. */
+int tipt_ensemble_march_supported(int32_t n0, int32_t n1, int32_t n2);  /* 1 or 0 */
+int tipt_ensemble_step_march(const void* phi, const void* pi, void* phi_out, void* pi_out,
+                             int64_t n_total, const tipt_replica* replicas, const int32_t* rids,
+                             int32_t n_rids, int32_t n0, int32_t n1, int32_t n2,
+                             const int32_t* active, const tipt_step_params* sp,
+                             const uint64_t* counter, int64_t offset, void* stream);
+
 /* Per replica (one block each, fixed order): frac_out[r] = fraction of sites
  * with phi > thr.  An active replica whose fraction exceeds stop_frac for the
  * first time gets first_step[r] = step (+ *counter + offset; first_step starts

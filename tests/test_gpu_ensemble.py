@@ -114,3 +114,25 @@ def test_single_lattice_poly_vs_oracle(storage):
     scale = max(np.abs(ref_phi).max(), np.abs(ref_pi).max())
     err = max(np.abs(a - ref_phi).max(), np.abs(b - ref_pi).max()) / scale
     assert err < TOL[storage], err
+
+
+@pytest.mark.parametrize("storage", ["f32c"])
+def test_marching_classes_equal_chunk_kernel(storage):
+    """Replicas of the 3-D shape classes step on the marching stage (shared-memory
+    tiles), one launch per class; bitwise the chunk work-list kernel's result,
+    retired replicas included (their items are skipped by both warp roles)."""
+    specs = ([EN.ReplicaSpec((16, 16, 16), 0.99 + 0.003 * r, 0.05, 60 + r) for r in range(5)]
+             + [EN.ReplicaSpec((24, 12, 32), 1.0, 0.045, 70 + r) for r in range(3)]
+             + [EN.ReplicaSpec((32, 32, 1), 0.985, 0.05, 80), EN.ReplicaSpec((10, 6, 14), 0.98, 0.06, 81)])
+    kw = dict(storage=storage, stop_frac=0.02, retire_frac=0.02, check_every=6, init_seed=4)
+    a = EN.Ensemble(specs, use_march=True, **kw)
+    b = EN.Ensemble(specs, use_march=False, **kw)
+    assert len(a._march) == 2 and len(b._march) == 0
+    fa = a.run(60, poll_every=1)
+    fb = b.run(60, poll_every=1)
+    assert np.array_equal(fa, fb)
+    for r in range(len(specs)):
+        x, y = a.replica_state(r), b.replica_state(r)
+        assert torch.equal(x[0], y[0]) and torch.equal(x[1], y[1]), r
+    from thermal_inflation_phase_transition_b200 import _lib as L
+    assert L.device_status() == 0

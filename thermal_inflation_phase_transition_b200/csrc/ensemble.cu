@@ -20,6 +20,7 @@
 // (its chunks are skipped from then on).
 #include <cstring>
 
+#include "rk2_march.cuh"
 #include "rk2_real.cuh"
 #include "tipt_internal.h"
 
@@ -320,4 +321,52 @@ extern "C" int tipt_ensemble_observe(int storage, const void* phi, int64_t n_tot
             reinterpret_cast<const unsigned long long*>(counter), offset, first_step, frac_out);
     cudaError_t err = cudaGetLastError();
     return err == cudaSuccess ? TIPT_OK : fail_cuda(err, "ensemble_observe launch");
+}
+
+// The replicas of one 3-D shape class in compensated FP32 on the marching stage
+// (shared-memory tiles, TMA/bulk-copy ring): bitwise the same step as
+// tipt_ensemble_step for those replicas.
+extern "C" int tipt_ensemble_step_march(const void* phi, const void* pi, void* phi_out,
+                                        void* pi_out, int64_t n_total,
+                                        const tipt_replica* replicas, const int32_t* rids,
+                                        int32_t n_rids, int32_t n0, int32_t n1, int32_t n2,
+                                        const int32_t* active, const tipt_step_params* sp,
+                                        const uint64_t* counter, int64_t offset, void* stream) {
+    int rc;
+    if ((rc = check_state_sites(TIPT_F32C, phi, pi, phi_out, pi_out, n_total))) return rc;
+    if (!replicas || !rids || !active || !sp) return fail(TIPT_ERR_ARG, "NULL argument");
+    if (n_rids < 0) return fail(TIPT_ERR_ARG, "n_rids < 0");
+    if (n_rids == 0) return TIPT_OK;
+    if (!ensemble_march_supported(n0, n1, n2))
+        return fail(TIPT_ERR_UNSUPPORTED, "replica shape %d x %d x %d has no marching tiles", n0,
+                    n1, n2);
+    const uintptr_t a = reinterpret_cast<uintptr_t>(phi) | reinterpret_cast<uintptr_t>(pi) |
+                        reinterpret_cast<uintptr_t>(phi_out) | reinterpret_cast<uintptr_t>(pi_out);
+    if (a % 16 || (n_total * 4) % 16) return fail(TIPT_ERR_ALIGN, "packed buffers must be 16-byte aligned");
+    RealStageParams p;
+    memset(&p, 0, sizeof(p));
+    p.phi = phi;
+    p.pi = pi;
+    p.phi_out = phi_out;
+    p.pi_out = pi_out;
+    p.n0 = n0;
+    p.n1 = n1;
+    p.n2 = n2;
+    p.h1 = 0.5 * sp->dt;
+    p.h2 = sp->dt;
+    p.inv_dx2 = 1.0 / (sp->dx * sp->dx);
+    p.eta = sp->eta_eff;
+    p.inv_mu2 = 1.0 / (sp->mu * sp->mu);
+    p.inv_a2 = sp->inv_a2;
+    p.nfac = 1.0;
+    p.step = sp->noise_step;
+    return launch_ensemble_march(p, replicas, rids, n_rids, active, n_total,
+                                 reinterpret_cast<const unsigned long long*>(counter),
+                                 (long long)offset, (cudaStream_t)stream);
+}
+
+// 1 when replicas of shape n0 x n1 x n2 (n2 contiguous) can step on the marching
+// stage (tipt_ensemble_step_march), 0 otherwise.
+extern "C" int tipt_ensemble_march_supported(int32_t n0, int32_t n1, int32_t n2) {
+    return ensemble_march_supported(n0, n1, n2) ? 1 : 0;
 }

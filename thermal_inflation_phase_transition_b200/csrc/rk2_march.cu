@@ -389,6 +389,19 @@ __global__ void __maxnreg__(kMarchRegs)
     }
 }
 
+// Batched-ensemble arguments of the compensated-FP32 marching stage (unused for
+// a single lattice).
+struct EnsMarch {
+    const tipt_replica* reps;
+    const int32_t* rids;          // the class's replica ids
+    const int32_t* active;
+    int64_t n_total;              // sites of the packed buffers
+    int items_per_rep;            // work items of one replica
+    uint64_t step;
+    const unsigned long long* ctr;  // device step counter or nullptr
+    long long offset;
+};
+
 // Planar compensated-FP32 marching kernel.  Same ring, roles and work items as
 // rk2_stage_march; a field is two FP32 planes (hi, then lo N sites later), so
 // the TMA map spans 2*n0 planes and a ring stage holds [phi, pi][hi, lo]
@@ -396,11 +409,19 @@ __global__ void __maxnreg__(kMarchRegs)
 // 16-byte vector per plane and neighbour) and evaluates them as two site
 // pairs in the lanes of the packed FP32x2 instructions; the stencil sums run
 // in the order of the generic kernel, so results are bitwise identical.
-template <bool WIDE, bool TH, bool RG>
+//
+// ENS: the replicas of one shape class of a batched ensemble (packed buffers:
+// the hi planes of all n_total sites, then the lo planes), each with its own
+// polynomial V', noise amplitude and seed; work items run over (replica,
+// j-block, i-chunk) and both warp roles skip the items of retired replicas.
+// The per-site arithmetic is the single-lattice kernel's, so a replica's
+// result is bitwise that of the lattice stepped alone.
+template <bool WIDE, bool TH, bool RG, bool ENS>
 __global__ void __maxnreg__(kMarchRegs)
-    rk2_stage_march_f32c(RealStageParams p_in, MarchGeom g) {
+    rk2_stage_march_f32c(RealStageParams p_in, MarchGeom g, EnsMarch em) {
     RealStageParams p = p_in;
-    resolve_schedule(p);
+    if constexpr (ENS) p.step = em.step + (em.ctr ? *em.ctr + (unsigned long long)em.offset : 0ull);
+    else resolve_schedule(p);
     if constexpr (RG) reset_next_range(p);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
@@ -447,9 +468,28 @@ __global__ void __maxnreg__(kMarchRegs)
         RingPos w{0, 0};
         uint32_t issued = 0;
         bool ok = true;
+        const int64_t plane_n = (int64_t)n0 * n1 * n2;
         for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
-            const int ic = item / g.nJB;
-            const int j0 = (item - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
+            int it = item;
+            const float *phi_hi = src_phi, *phi_lo = src_phi + plane_n;
+            const float *pi_hi = src_pi, *pi_lo = src_pi + plane_n;
+            if constexpr (ENS) {
+                const int rl = item / em.items_per_rep;
+                const int rid = em.rids[rl];
+                if (!em.active[rid]) continue;
+                it = item - rl * em.items_per_rep;
+                const int64_t off = em.reps[rid].offset;
+                if (off & 3) {  // bulk-copy sources must be 16-byte aligned: skipped
+                    atomicExch(&g_device_status, (int)TIPT_ERR_ALIGN);
+                    continue;
+                }
+                phi_hi = src_phi + off;
+                phi_lo = src_phi + em.n_total + off;
+                pi_hi = src_pi + off;
+                pi_lo = src_pi + em.n_total + off;
+            }
+            const int ic = it / g.nJB;
+            const int j0 = (it - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
             const int npl = min(g.CI, p.i_end - i0) + 2;
             for (int q = 0; q < npl; ++q) {
                 if (issued == stop_at) {  // nothing is issued from here on
@@ -463,11 +503,11 @@ __global__ void __maxnreg__(kMarchRegs)
                 mbar_expect_tx(&full[w.stage], plane_tx);
                 int iw = i0 - 1 + q;
                 iw = iw < 0 ? iw + n0 : (iw >= n0 ? iw - n0 : iw);
-                // planes iw (hi) and n0 + iw (lo) of the planar pair
-                copy_tile_rows(blk(w.stage, 0, 0), src_phi, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
-                copy_tile_rows(blk(w.stage, 0, 1), src_phi, n0 + iw, j0, rows, n1, n2, pitch, &full[w.stage]);
-                copy_tile_rows(blk(w.stage, 1, 0), src_pi, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
-                copy_tile_rows(blk(w.stage, 1, 1), src_pi, n0 + iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                // plane iw of the hi and lo planes of each field
+                copy_tile_rows(blk(w.stage, 0, 0), phi_hi, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                copy_tile_rows(blk(w.stage, 0, 1), phi_lo, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                copy_tile_rows(blk(w.stage, 1, 0), pi_hi, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
+                copy_tile_rows(blk(w.stage, 1, 1), pi_lo, iw, j0, rows, n1, n2, pitch, &full[w.stage]);
                 ++issued;
                 w.next(NS);
             }
@@ -488,17 +528,41 @@ __global__ void __maxnreg__(kMarchRegs)
     const int k0 = 4 * (t - (r - 1) * tpr);    // first of the four own columns
     const int kml = k0 == 0 ? n2 - 1 : k0 - 1;
     const int kpr = k0 + 4 == n2 ? 0 : k0 + 4;
-    const F32CConst kc = f32c_const(p);
-    float* const phi_out = static_cast<float*>(p.phi_out);
-    float* const pi_out = static_cast<float*>(p.pi_out);
-    const int64_t N = (int64_t)n0 * n1 * n2;
+    F32CConst kc = f32c_const(p);
+    float* phi_out = static_cast<float*>(p.phi_out);
+    float* pi_out = static_cast<float*>(p.pi_out);
+    // lo planes N sites after the hi planes (the lattice's, or the packed buffer's)
+    int64_t N = (int64_t)n0 * n1 * n2;
+    if constexpr (ENS) N = em.n_total;
     const int orow = r * pitch, urow = (r - 1) * pitch, drow = (r + 1) * pitch;
+    // the batched replicas' own polynomial, amplitude and seed (set per item)
+    float2 ec1 = make_float2(0.0f, 0.0f), ec2 = ec1, ec3 = ec1;
+    bool ehas_c2 = false;
+    uint64_t eseed = 0;
 
     RangeAcc racc;
     RingPos pm{0, 0};
     for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
-        const int ic = item / g.nJB;
-        const int j0 = (item - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
+        int it = item;
+        if constexpr (ENS) {
+            const int rl = item / em.items_per_rep;
+            const int rid = em.rids[rl];
+            if (!em.active[rid]) continue;
+            it = item - rl * em.items_per_rep;
+            const tipt_replica& rp = em.reps[rid];
+            if (rp.offset & 3) continue;  // skipped by the producer too
+            phi_out = static_cast<float*>(p.phi_out) + rp.offset;
+            pi_out = static_cast<float*>(p.pi_out) + rp.offset;
+            const float f1 = (float)rp.c1, f2 = (float)rp.c2, f3 = (float)rp.c3;
+            ec1 = make_float2(f1, f1);
+            ec2 = make_float2(f2, f2);
+            ec3 = make_float2(f3, f3);
+            ehas_c2 = rp.c2 != 0.0;
+            kc.ns = (float)rp.noise_scale;
+            eseed = rp.seed;
+        }
+        const int ic = it / g.nJB;
+        const int j0 = (it - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
         const int ni = min(g.CI, p.i_end - i0);
         const int jw = j0 + r - 1;
         RingPos pc = pm, pp;
@@ -519,7 +583,15 @@ __global__ void __maxnreg__(kMarchRegs)
                 uint64_t site;
                 if constexpr (WIDE) site = (uint64_t)(rowoff + p.site_offset + 2 * h);
                 else site = (uint32_t)(rowoff + p.site_offset) + (uint32_t)(2 * h);
-                kick[h] = site_kick_f32c2(p, kc, site);
+                if constexpr (ENS) {
+                    // the replica's own seed and amplitude (site_kick_f32c2's hash branch)
+                    kick[h] = kc.ns == 0.0f ? make_float2(0.0f, 0.0f)
+                                            : v_mul(vs<float2>(kc.ns),
+                                                    gauss_cos_f2(noise_key(site, p.step, p.mul, eseed),
+                                                                 noise_key(site + 1, p.step, p.mul, eseed)));
+                } else {
+                    kick[h] = site_kick_f32c2(p, kc, site);
+                }
             }
             // the centre plane is resident: its values and V' at the centre and
             // the midpoint are evaluated before the wait as well
@@ -535,8 +607,14 @@ __global__ void __maxnreg__(kMarchRegs)
                 const auto pick = [h](const float4& v) {
                     return h ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
                 };
-                pre[h] = pre_f32c<float2, TH>(p, kc, s_tab, pick(cen[0][0]), pick(cen[0][1]),
-                                              pick(cen[1][0]), pick(cen[1][1]));
+                if constexpr (ENS)
+                    pre[h] = pre_f32c_vp<float2>(p, pick(cen[0][0]), pick(cen[0][1]), pick(cen[1][0]),
+                                                 pick(cen[1][1]), [&](float2 x) {
+                                                     return poly_vprime_v<float2>(ec1, ec2, ec3, ehas_c2, x);
+                                                 });
+                else
+                    pre[h] = pre_f32c<float2, TH>(p, kc, s_tab, pick(cen[0][0]), pick(cen[0][1]),
+                                                  pick(cen[1][0]), pick(cen[1][1]));
             }
             if (!mbar_wait(&full[pp.stage], pp.phase)) {
                 if (lane == 0) atomicExch(&g_device_status, (int)TIPT_ERR_TIMEOUT);
@@ -1261,9 +1339,9 @@ bool march_supported(int storage, const RealStageParams& p) {
     return geometry(storage, p, tb, g, smem);
 }
 
-template <typename Kern>
+template <typename Kern, typename... Extra>
 static int launch_march_k(Kern kern, const RealStageParams& p, const MarchGeom& g, int64_t smem,
-                          cudaStream_t st) {
+                          cudaStream_t st, Extra... extra) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess)
@@ -1278,9 +1356,59 @@ static int launch_march_k(Kern kern, const RealStageParams& p, const MarchGeom& 
                     "bytes of shared memory)", threads, (long long)smem);
     int grid = num_sms() * per_sm;
     if (grid > g.items) grid = g.items;
-    kern<<<grid, threads, (size_t)smem, st>>>(p, g);
+    kern<<<grid, threads, (size_t)smem, st>>>(p, g, extra...);
     e = cudaGetLastError();
     return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "marching kernel launch");
+}
+
+// The batched ensemble's replicas of one 3-D shape class (n0, n1, n2 with
+// n2 % 4 == 0) on the compensated-FP32 marching stage: rids[0..n_rids) are the
+// class's replica ids; p carries the shared step constants (dt, dx, eta, mu,
+// inv_a2), the packed state pointers and the class shape.
+int launch_ensemble_march(const RealStageParams& p_in, const tipt_replica* reps,
+                          const int32_t* rids, int n_rids, const int32_t* active, int64_t n_total,
+                          const unsigned long long* ctr, long long offset, cudaStream_t st) {
+    RealStageParams p = p_in;
+    p.i_begin = 0;
+    p.i_end = p.n0;
+    p.vkind = TIPT_VP_POLY;
+    p.table_in_smem = 0;
+    p.mul = kPass2Mul;
+    set_f32c_pairs(p);
+    MarchGeom g;
+    int64_t smem;
+    if (!geometry(TIPT_F32C, p, 0, g, smem))
+        return fail(TIPT_ERR_UNSUPPORTED, "no marching geometry for the replica shape");
+    EnsMarch em;
+    em.reps = reps;
+    em.rids = rids;
+    em.active = active;
+    em.n_total = n_total;
+    em.items_per_rep = g.items;
+    em.step = p.step;
+    em.ctr = ctr;
+    em.offset = offset;
+    if ((int64_t)g.items * n_rids > 0x7FFFFFFF)
+        return fail(TIPT_ERR_UNSUPPORTED, "too many work items");
+    g.items *= n_rids;
+    // 64-bit noise-key sites when a replica's site index can exceed 32 bits
+    const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
+    return wide ? launch_march_k(rk2_stage_march_f32c<true, false, false, true>, p, g, smem, st, em)
+                : launch_march_k(rk2_stage_march_f32c<false, false, false, true>, p, g, smem, st, em);
+}
+
+bool ensemble_march_supported(int n0, int n1, int n2) {
+    if (n0 < 2 || n2 % 4 != 0) return false;
+    RealStageParams p;
+    memset(&p, 0, sizeof(p));
+    p.n0 = n0;
+    p.n1 = n1;
+    p.n2 = n2;
+    p.i_begin = 0;
+    p.i_end = n0;
+    MarchGeom g;
+    int64_t smem;
+    return geometry(TIPT_F32C, p, 0, g, smem);
 }
 
 int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cudaStream_t st) {
@@ -1293,20 +1421,20 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
                       0xFFFFFFFFll;
     if (storage == TIPT_F32C && p.vkind == TIPT_VP_THERMAL) {
         if (p.range)
-            return wide ? launch_march_k(rk2_stage_march_f32c<true, true, true>, p, g, smem, st)
-                        : launch_march_k(rk2_stage_march_f32c<false, true, true>, p, g, smem, st);
-        return wide ? launch_march_k(rk2_stage_march_f32c<true, true, false>, p, g, smem, st)
-                    : launch_march_k(rk2_stage_march_f32c<false, true, false>, p, g, smem, st);
+            return wide ? launch_march_k(rk2_stage_march_f32c<true, true, true, false>, p, g, smem, st, EnsMarch{})
+                        : launch_march_k(rk2_stage_march_f32c<false, true, true, false>, p, g, smem, st, EnsMarch{});
+        return wide ? launch_march_k(rk2_stage_march_f32c<true, true, false, false>, p, g, smem, st, EnsMarch{})
+                    : launch_march_k(rk2_stage_march_f32c<false, true, false, false>, p, g, smem, st, EnsMarch{});
     }
     if (storage == TIPT_F32C) {
         RealStageParams q = p;
         q.test_withhold = g_test_withhold;
         g_test_withhold = 0;
         if (q.range)
-            return wide ? launch_march_k(rk2_stage_march_f32c<true, false, true>, q, g, smem, st)
-                        : launch_march_k(rk2_stage_march_f32c<false, false, true>, q, g, smem, st);
-        return wide ? launch_march_k(rk2_stage_march_f32c<true, false, false>, q, g, smem, st)
-                    : launch_march_k(rk2_stage_march_f32c<false, false, false>, q, g, smem, st);
+            return wide ? launch_march_k(rk2_stage_march_f32c<true, false, true, false>, q, g, smem, st, EnsMarch{})
+                        : launch_march_k(rk2_stage_march_f32c<false, false, true, false>, q, g, smem, st, EnsMarch{});
+        return wide ? launch_march_k(rk2_stage_march_f32c<true, false, false, false>, q, g, smem, st, EnsMarch{})
+                    : launch_march_k(rk2_stage_march_f32c<false, false, false, false>, q, g, smem, st, EnsMarch{});
     }
     if (storage != TIPT_F32C && p.range)
         return fail(TIPT_ERR_UNSUPPORTED, "the FP64 / float32 marching stage takes no range output");

@@ -8,6 +8,13 @@ namespace tipt {
 bool march_supported(int storage, const RealStageParams& p);
 int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cudaStream_t st);
 
+// Batched ensemble: the replicas rids[0..n_rids) of one 3-D shape class on the
+// compensated-FP32 marching stage.
+bool ensemble_march_supported(int n0, int n1, int n2);
+int launch_ensemble_march(const RealStageParams& p, const tipt_replica* reps, const int32_t* rids,
+                          int n_rids, const int32_t* active, int64_t n_total,
+                          const unsigned long long* ctr, long long offset, cudaStream_t st);
+
 // Overdamped / BAOAB passes (mode kOD, kBA1, kBA2) of the real or complex
 // field, compensated FP32.
 struct AltParams;

@@ -332,17 +332,34 @@ struct F32CPre {
     V pvc, v1, v2;  // pi (hi + lo), V'(phi), V'(phi + h1 pi)
 };
 
-template <typename V, bool TH = true>
-__device__ __forceinline__ F32CPre<V> pre_f32c(const RealStageParams& p, const F32CConst& kc,
-                                               const float* s_tab, V phh, V phl, V pih, V pil) {
+// The same with the V' source as a functor vp(x) (the batched ensemble's
+// per-replica polynomial).
+template <typename V, typename VP>
+__device__ __forceinline__ F32CPre<V> pre_f32c_vp(const RealStageParams& p, V phh, V phl, V pih,
+                                                  V pil, VP vp) {
     const V h1 = kvec<V>(p.k2.h1);
     const V phc = v_add(phh, phl);
     F32CPre<V> r;
     r.pvc = v_add(pih, pil);
     const V pht = v_add(phh, v_fma(h1, r.pvc, phl));
-    r.v1 = vprime_v<V, TH>(p, kc, s_tab, phc);
-    r.v2 = vprime_v<V, TH>(p, kc, s_tab, pht);
+    r.v1 = vp(phc);
+    r.v2 = vp(pht);
     return r;
+}
+
+template <typename V, bool TH = true>
+__device__ __forceinline__ F32CPre<V> pre_f32c(const RealStageParams& p, const F32CConst& kc,
+                                               const float* s_tab, V phh, V phl, V pih, V pil) {
+    return pre_f32c_vp<V>(p, phh, phl, pih, pil,
+                          [&](V x) { return vprime_v<V, TH>(p, kc, s_tab, x); });
+}
+
+// Polynomial V'(x) = c1 x + c2 x^2 + c3 x^3 in lane vectors from FP32 pairs: the
+// polynomial branch of vprime_v with coefficients given per call.
+template <typename V>
+__device__ __forceinline__ V poly_vprime_v(float2 c1, float2 c2, float2 c3, bool has_c2, V x) {
+    const V d = v_fma(v_mul(v_mul(kvec<V>(c3), x), x), x, v_mul(kvec<V>(c1), x));
+    return has_c2 ? v_fma(v_mul(kvec<V>(c2), x), x, d) : d;
 }
 
 // The rest of the site update, from the stencil sums, the centre values and the

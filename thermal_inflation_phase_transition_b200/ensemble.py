@@ -78,7 +78,7 @@ class Ensemble:
 
     def __init__(self, specs, *, storage="f32c", dt=0.05, dx=1.0, eta=1.0, mu=1.0, inv_a2=1.0,
                  thr=1.0, stop_frac=0.5, retire_frac=None, init_sigma=0.01, init_seed=0,
-                 chunk_sites=8192, check_every=10, device="cuda"):
+                 chunk_sites=8192, check_every=10, use_march=True, device="cuda"):
         if storage not in ("f32c", "f64"):
             raise ValueError("ensemble storage is 'f32c' or 'f64'")
         self.specs = list(specs)
@@ -93,6 +93,9 @@ class Ensemble:
         chunks = []
         off = 0
         self.sizes = np.zeros(self.R, np.int64)
+        self.offsets = np.zeros(self.R, np.int64)
+        # Replica offsets are multiples of 4 sites (16-byte aligned rows for the bulk
+        # copies of the marching stage).
         for r, sp in enumerate(self.specs):
             n0, n1, n2 = _canonical(sp.shape)
             n = n0 * n1 * n2
@@ -102,21 +105,33 @@ class Ensemble:
             ns = math.sqrt(2.0 * eta * sp.T * dt / dx ** 3)
             reps[r] = L.Replica(n0, n1, n2, _magic(n1), _magic(n2), 0, off, c1, c2, c3, ns,
                                 int(sp.seed) & (2 ** 64 - 1))
+            self.sizes[r] = n
+            self.offsets[r] = off
+            off += (n + 3) & ~3
+        self.n_total = off
+        # 3-D shape classes in compensated storage step on the marching stage (shared-
+        # memory tiles fed by bulk copies), one launch per class; the rest (2-D
+        # lattices, FP64, shapes without marching tiles) on the chunk work-list kernel
+        classes = {}
+        for r, sp in enumerate(self.specs):
+            n0, n1, n2 = _canonical(sp.shape)
+            n = n0 * n1 * n2
+            if self.st == L.TIPT_F32C and use_march and \
+                    L.lib().tipt_ensemble_march_supported(n0, n1, n2):
+                classes.setdefault((n0, n1, n2), []).append(r)
+                continue
             for b in range(0, n, chunk_sites):
                 chunks.append((r, min(chunk_sites, n - b), b))
-            self.sizes[r] = n
-            off += n
-        self.n_total = off
+        self._march = [(shape, torch.tensor(rids, dtype=torch.int32, device=self.dev))
+                       for shape, rids in classes.items()]
         self._reps = torch.frombuffer(bytearray(bytes(reps)), dtype=torch.uint8).to(self.dev)
-        ch = (L.Chunk * len(chunks))(*[L.Chunk(*c) for c in chunks])
+        ch = (L.Chunk * max(len(chunks), 1))(*[L.Chunk(*c) for c in chunks])
         self._chunks = torch.frombuffer(bytearray(bytes(ch)), dtype=torch.uint8).to(self.dev)
         self.n_chunks = len(chunks)
-        phi = torch.empty(self.n_total, dtype=torch.float64, device=self.dev)
-        o = 0
+        phi = torch.zeros(self.n_total, dtype=torch.float64, device=self.dev)
         for r, sp in enumerate(self.specs):
-            n = int(self.sizes[r])
+            n, o = int(self.sizes[r]), int(self.offsets[r])
             phi[o:o + n] = replica_initial_phi(n, sp.seed, init_seed, init_sigma, self.dev)
-            o += n
         if storage == "f32c":
             hi = phi.float()
             lo = (phi - hi.double()).float()
@@ -142,6 +157,12 @@ class Ensemble:
         st = stream_handle()
         for q in range(K):
             a, b = q & 1, (q + 1) & 1
+            for (n0, n1, n2), rids in self._march:
+                L.check(lib.tipt_ensemble_step_march(
+                    ptr(self.phi[a]), ptr(self.pi[a]), ptr(self.phi[b]), ptr(self.pi[b]),
+                    self.n_total, ptr(self._reps), ptr(rids), rids.numel(), n0, n1, n2,
+                    ptr(self.active), self._sp, ptr(self._counter), q, st),
+                    "tipt_ensemble_step_march")
             L.check(lib.tipt_ensemble_step(
                 self.st, ptr(self.phi[a]), ptr(self.pi[a]), ptr(self.phi[b]), ptr(self.pi[b]),
                 self.n_total, ptr(self._reps), ptr(self._chunks), self.n_chunks,
@@ -191,7 +212,7 @@ class Ensemble:
     def replica_state(self, r):
         """(phi, pi) of replica r as FP64 tensors with its canonical shape."""
         n0, n1, n2 = _canonical(self.specs[r].shape)
-        o = int(self.sizes[:r].sum())
+        o = int(self.offsets[r])
         n = int(self.sizes[r])
 
         def f64(t):

@@ -323,9 +323,15 @@ int tipt_ensemble_step(int storage, const void* phi, const void* pi, void* phi_o
 int tipt_ensemble_march_supported(int32_t n0, int32_t n1, int32_t n2);  /* 1 or 0 */
 int tipt_ensemble_step_march(const void* phi, const void* pi, void* phi_out, void* pi_out,
                              int64_t n_total, const tipt_replica* replicas, const int32_t* rids,
-                             int32_t n_rids, int32_t n0, int32_t n1, int32_t n2,
-                             const int32_t* active, const tipt_step_params* sp,
+                             int32_t n_rids, const int32_t* n_rids_dev, int32_t n0, int32_t n1,
+                             int32_t n2, const int32_t* active, const tipt_step_params* sp,
                              const uint64_t* counter, int64_t offset, void* stream);
+/* n_rids_dev (optional, a device int32 <= n_rids): the number of rids to step,
+ * read by the launch -- with tipt_ensemble_compact the class's work items then
+ * cover its active replicas only, spread over the SMs.  Ordered compaction:
+ * rids_out[0..*n_out) = the rids[q] whose active flag is set. */
+int tipt_ensemble_compact(const int32_t* rids, int32_t n, const int32_t* active,
+                          int32_t* rids_out, int32_t* n_out, void* stream);
 
 /* Per replica (one block each, fixed order): frac_out[r] = fraction of sites
  * with phi > thr.  An active replica whose fraction exceeds stop_frac for the

@@ -142,8 +142,9 @@ _SIGS = {
     "tipt_device_status": [C.POINTER(C.c_int), _i],
     "tipt_test_withhold_plane": [_i],
     "tipt_ensemble_march_supported": [C.c_int32, C.c_int32, C.c_int32],
-    "tipt_ensemble_step_march": [_p, _p, _p, _p, _i64, _p, _p, C.c_int32, C.c_int32, C.c_int32,
-                                 C.c_int32, _p, C.POINTER(StepParams), _p, _i64, _p],
+    "tipt_ensemble_step_march": [_p, _p, _p, _p, _i64, _p, _p, C.c_int32, _p, C.c_int32,
+                                 C.c_int32, C.c_int32, _p, C.POINTER(StepParams), _p, _i64, _p],
+    "tipt_ensemble_compact": [_p, C.c_int32, _p, _p, _p, _p],
 }
 _RESTYPE = {"tipt_version": C.c_char_p, "tipt_status_string": C.c_char_p,
             "tipt_last_error": C.c_char_p, "tipt_observables_workspace_size": C.c_int64,

@@ -329,9 +329,10 @@ extern "C" int tipt_ensemble_observe(int storage, const void* phi, int64_t n_tot
 extern "C" int tipt_ensemble_step_march(const void* phi, const void* pi, void* phi_out,
                                         void* pi_out, int64_t n_total,
                                         const tipt_replica* replicas, const int32_t* rids,
-                                        int32_t n_rids, int32_t n0, int32_t n1, int32_t n2,
-                                        const int32_t* active, const tipt_step_params* sp,
-                                        const uint64_t* counter, int64_t offset, void* stream) {
+                                        int32_t n_rids, const int32_t* n_rids_dev, int32_t n0,
+                                        int32_t n1, int32_t n2, const int32_t* active,
+                                        const tipt_step_params* sp, const uint64_t* counter,
+                                        int64_t offset, void* stream) {
     int rc;
     if ((rc = check_state_sites(TIPT_F32C, phi, pi, phi_out, pi_out, n_total))) return rc;
     if (!replicas || !rids || !active || !sp) return fail(TIPT_ERR_ARG, "NULL argument");
@@ -360,7 +361,7 @@ extern "C" int tipt_ensemble_step_march(const void* phi, const void* pi, void* p
     p.inv_a2 = sp->inv_a2;
     p.nfac = 1.0;
     p.step = sp->noise_step;
-    return launch_ensemble_march(p, replicas, rids, n_rids, active, n_total,
+    return launch_ensemble_march(p, replicas, rids, n_rids, n_rids_dev, active, n_total,
                                  reinterpret_cast<const unsigned long long*>(counter),
                                  (long long)offset, (cudaStream_t)stream);
 }
@@ -369,4 +370,47 @@ extern "C" int tipt_ensemble_step_march(const void* phi, const void* pi, void* p
 // stage (tipt_ensemble_step_march), 0 otherwise.
 extern "C" int tipt_ensemble_march_supported(int32_t n0, int32_t n1, int32_t n2) {
     return ensemble_march_supported(n0, n1, n2) ? 1 : 0;
+}
+
+// Ordered compaction of a class's replica ids: rids_out[0..*n_out) = the ids
+// rids[q] (in order) whose active flag is set.  One block.
+__global__ void __launch_bounds__(1024) ensemble_compact_kernel(const int32_t* rids, int32_t n,
+                                                                 const int32_t* active,
+                                                                 int32_t* rids_out,
+                                                                 int32_t* n_out) {
+    __shared__ int32_t s_warp[32];
+    __shared__ int32_t s_base;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int b = 0; b < n; b += blockDim.x) {
+        const int q = b + (int)threadIdx.x;
+        const bool keep = q < n && active[rids[q]] != 0;
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_warp[wid] = __popc(m);
+        __syncthreads();
+        int before = s_base;
+        for (int w = 0; w < wid; ++w) before += s_warp[w];
+        if (keep) rids_out[before + __popc(m & ((1u << lane) - 1u))] = rids[q];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tot = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += s_warp[w];
+            s_base += tot;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *n_out = s_base;
+}
+
+// The active replicas of a class, compacted in order (for tipt_ensemble_step_march's
+// device count): rids_out receives them, *n_out their number.
+extern "C" int tipt_ensemble_compact(const int32_t* rids, int32_t n, const int32_t* active,
+                                     int32_t* rids_out, int32_t* n_out, void* stream) {
+    if (!rids || !active || !rids_out || !n_out) return fail(TIPT_ERR_ARG, "NULL argument");
+    if (n < 0) return fail(TIPT_ERR_ARG, "n < 0");
+    ensemble_compact_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(rids, n, active, rids_out,
+                                                                  n_out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TIPT_OK : fail_cuda(e, "ensemble_compact launch");
 }

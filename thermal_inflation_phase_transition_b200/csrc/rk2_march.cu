@@ -393,7 +393,8 @@ __global__ void __maxnreg__(kMarchRegs)
 // a single lattice).
 struct EnsMarch {
     const tipt_replica* reps;
-    const int32_t* rids;          // the class's replica ids
+    const int32_t* rids;          // the class's replica ids (its active ones, compacted)
+    const int32_t* n_rids;        // device count of rids (nullptr: g.items covers them all)
     const int32_t* active;
     int64_t n_total;              // sites of the packed buffers
     int items_per_rep;            // work items of one replica
@@ -469,7 +470,11 @@ __global__ void __maxnreg__(kMarchRegs)
         uint32_t issued = 0;
         bool ok = true;
         const int64_t plane_n = (int64_t)n0 * n1 * n2;
-        for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
+        int n_items = g.items;
+        if constexpr (ENS) {
+            if (em.n_rids) n_items = min(g.items, *em.n_rids * em.items_per_rep);
+        }
+        for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
             int it = item;
             const float *phi_hi = src_phi, *phi_lo = src_phi + plane_n;
             const float *pi_hi = src_pi, *pi_lo = src_pi + plane_n;
@@ -542,7 +547,11 @@ __global__ void __maxnreg__(kMarchRegs)
 
     RangeAcc racc;
     RingPos pm{0, 0};
-    for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
+    int n_items = g.items;  // the producer reads the same count
+    if constexpr (ENS) {
+        if (em.n_rids) n_items = min(g.items, *em.n_rids * em.items_per_rep);
+    }
+    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
         int it = item;
         if constexpr (ENS) {
             const int rl = item / em.items_per_rep;
@@ -1366,7 +1375,8 @@ static int launch_march_k(Kern kern, const RealStageParams& p, const MarchGeom& 
 // class's replica ids; p carries the shared step constants (dt, dx, eta, mu,
 // inv_a2), the packed state pointers and the class shape.
 int launch_ensemble_march(const RealStageParams& p_in, const tipt_replica* reps,
-                          const int32_t* rids, int n_rids, const int32_t* active, int64_t n_total,
+                          const int32_t* rids, int n_rids, const int32_t* n_rids_dev,
+                          const int32_t* active, int64_t n_total,
                           const unsigned long long* ctr, long long offset, cudaStream_t st) {
     RealStageParams p = p_in;
     p.i_begin = 0;
@@ -1379,9 +1389,17 @@ int launch_ensemble_march(const RealStageParams& p_in, const tipt_replica* reps,
     int64_t smem;
     if (!geometry(TIPT_F32C, p, 0, g, smem))
         return fail(TIPT_ERR_UNSUPPORTED, "no marching geometry for the replica shape");
+    // 32-plane chunks: work items small enough to spread a few active replicas
+    // over the SMs
+    if (g_force_ci == 0 && g.CI > 32) {
+        g.CI = 32;
+        g.nIC = (p.n0 + g.CI - 1) / g.CI;
+        g.items = g.nJB * g.nIC;
+    }
     EnsMarch em;
     em.reps = reps;
     em.rids = rids;
+    em.n_rids = n_rids_dev;
     em.active = active;
     em.n_total = n_total;
     em.items_per_rep = g.items;

@@ -12,8 +12,9 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
 // compensated-FP32 marching stage.
 bool ensemble_march_supported(int n0, int n1, int n2);
 int launch_ensemble_march(const RealStageParams& p, const tipt_replica* reps, const int32_t* rids,
-                          int n_rids, const int32_t* active, int64_t n_total,
-                          const unsigned long long* ctr, long long offset, cudaStream_t st);
+                          int n_rids, const int32_t* n_rids_dev, const int32_t* active,
+                          int64_t n_total, const unsigned long long* ctr, long long offset,
+                          cudaStream_t st);
 
 // Overdamped / BAOAB passes (mode kOD, kBA1, kBA2) of the real or complex
 // field, compensated FP32.

@@ -122,7 +122,11 @@ class Ensemble:
                 continue
             for b in range(0, n, chunk_sites):
                 chunks.append((r, min(chunk_sites, n - b), b))
-        self._march = [(shape, torch.tensor(rids, dtype=torch.int32, device=self.dev))
+        # per class: all its replica ids, the active ones (compacted at the start of
+        # every check interval) and their device count
+        self._march = [(shape, torch.tensor(rids, dtype=torch.int32, device=self.dev),
+                        torch.empty(len(rids), dtype=torch.int32, device=self.dev),
+                        torch.zeros(1, dtype=torch.int32, device=self.dev))
                        for shape, rids in classes.items()]
         self._reps = torch.frombuffer(bytearray(bytes(reps)), dtype=torch.uint8).to(self.dev)
         ch = (L.Chunk * max(len(chunks), 1))(*[L.Chunk(*c) for c in chunks])
@@ -155,13 +159,16 @@ class Ensemble:
     def _chunk(self, K):
         lib = L.lib()
         st = stream_handle()
+        for _, rids, act, n_act in self._march:
+            L.check(lib.tipt_ensemble_compact(ptr(rids), rids.numel(), ptr(self.active), ptr(act),
+                                              ptr(n_act), st), "tipt_ensemble_compact")
         for q in range(K):
             a, b = q & 1, (q + 1) & 1
-            for (n0, n1, n2), rids in self._march:
+            for (n0, n1, n2), rids, act, n_act in self._march:
                 L.check(lib.tipt_ensemble_step_march(
                     ptr(self.phi[a]), ptr(self.pi[a]), ptr(self.phi[b]), ptr(self.pi[b]),
-                    self.n_total, ptr(self._reps), ptr(rids), rids.numel(), n0, n1, n2,
-                    ptr(self.active), self._sp, ptr(self._counter), q, st),
+                    self.n_total, ptr(self._reps), ptr(act), act.numel(), ptr(n_act), n0, n1,
+                    n2, ptr(self.active), self._sp, ptr(self._counter), q, st),
                     "tipt_ensemble_step_march")
             L.check(lib.tipt_ensemble_step(
                 self.st, ptr(self.phi[a]), ptr(self.pi[a]), ptr(self.phi[b]), ptr(self.pi[b]),

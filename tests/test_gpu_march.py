@@ -23,6 +23,7 @@ def _reset_policy():
     L.set_kernel_policy(0)
     L.set_march_tiles(0, 0, 0)
     L.set_march_kseg(0)
+    L.set_march_fixed(True)
 
 
 def _state(shape, storage, seed):
@@ -73,6 +74,43 @@ def test_march_equals_generic(shape, storage):
     ref = _run(1, shape, storage)
     got = _run(2, shape, storage)
     assert torch.equal(ref[0], got[0]) and torch.equal(ref[1], got[1])
+    assert L.device_status() == 0
+
+
+# rows of 512 sites in 4-row tiles and of 256 sites in 8-row tiles: the automatic
+# geometry takes the kernels compiled for them
+FIXED_SHAPES = [(8, 16, 512), (9, 4, 512), (6, 16, 256), (40, 8, 256)]
+
+
+@pytest.mark.parametrize("shape", FIXED_SHAPES)
+@pytest.mark.parametrize("table2d", [False, True])
+def test_fixed_geometry_equals_runtime_geometry(shape, table2d):
+    L.set_march_fixed(False)
+    ref = _run(2, shape, "f32c", table2d=table2d)
+    L.set_march_fixed(True)
+    got = _run(2, shape, "f32c", table2d=table2d)
+    assert torch.equal(ref[0], got[0]) and torch.equal(ref[1], got[1])
+    assert L.device_status() == 0
+
+
+@pytest.mark.parametrize("shape", FIXED_SHAPES[:3])
+def test_fixed_geometry_range_variant(shape):
+    """The range-folding form of the fixed-geometry kernels: the same field as the
+    run-time-geometry kernel and the same range words."""
+    t1, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.01), 0.0, 3.0, 4096)
+    vs = table_source(torch.from_numpy(t1).to(DEV), tmin, dinv, 4096)
+    out = []
+    for fixed in (False, True):
+        L.set_march_fixed(fixed)
+        L.set_kernel_policy(2)
+        phi, pi = _state(shape, "f32c", 21)
+        po, qo = torch.empty_like(phi), torch.empty_like(pi)
+        rng = RF.PhiRange()
+        RF.rk2_step_table_into(phi, pi, po, qo, 0.05, 1.0, 0.9, 1.0, 1.0, vs, noise_scale=0.3,
+                               noise_step=4, seed=2, phi_range=rng)
+        torch.cuda.synchronize()
+        out.append((po, qo, rng.last.clone()))
+    assert all(torch.equal(a, b) for a, b in zip(out[0], out[1]))
     assert L.device_status() == 0
 
 

@@ -139,6 +139,7 @@ _SIGS = {
     "tipt_set_kernel_policy": [_i],
     "tipt_set_march_tiles": [_i, _i, _i],
     "tipt_set_march_kseg": [_i],
+    "tipt_set_march_fixed": [_i],
     "tipt_device_status": [C.POINTER(C.c_int), _i],
     "tipt_test_withhold_plane": [_i],
     "tipt_ensemble_march_supported": [C.c_int32, C.c_int32, C.c_int32],
@@ -195,6 +196,12 @@ def set_kernel_policy(policy: int) -> None:
 def set_march_tiles(rows: int = 0, planes: int = 0, stages: int = 0) -> None:
     """Marching-kernel tile shape (0 = automatic); performance only."""
     call("tipt_set_march_tiles", int(rows), int(planes), int(stages))
+
+
+def set_march_fixed(enable: bool) -> None:
+    """Fixed-geometry compensated-FP32 stage kernels (512- / 256-site rows) on or off;
+    performance only (tests/tuning)."""
+    call("tipt_set_march_fixed", int(bool(enable)))
 
 
 def set_march_kseg(kseg: int) -> None:

@@ -417,9 +417,15 @@ struct EnsMarch {
 // j-block, i-chunk) and both warp roles skip the items of retired replicas.
 // The per-site arithmetic is the single-lattice kernel's, so a replica's
 // result is bitwise that of the lattice stepped alone.
-template <bool WIDE, bool TH, bool RG, bool ENS>
+//
+// KN2, KTJ > 0: the geometry fixed at compile time (rows of KN2 sites, pitch
+// KN2, KTJ-row tiles), so every shared-memory offset but the ring stage's is an
+// immediate and the row arithmetic is shifts; the launcher picks it when the
+// run-time geometry is exactly that one.
+template <bool WIDE, bool TH, bool RG, bool ENS, int KN2 = 0, int KTJ = 0>
 __global__ void __maxnreg__(kMarchRegs)
     rk2_stage_march_f32c(RealStageParams p_in, MarchGeom g, EnsMarch em) {
+    static_assert((KN2 == 0) == (KTJ == 0), "fixed geometry: both KN2 and KTJ");
     RealStageParams p = p_in;
     if constexpr (ENS) p.step = em.step + (em.ctr ? *em.ctr + (unsigned long long)em.offset : 0ull);
     else resolve_schedule(p);
@@ -431,9 +437,9 @@ __global__ void __maxnreg__(kMarchRegs)
     uint64_t* empty = full + 8;
     unsigned char* ring = smem + g.tab_bytes + 128;
 
-    const int n0 = p.n0, n1 = p.n1, n2 = p.n2;
-    const int pitch = g.pitch;
-    const int TJ = g.TJ;
+    const int n0 = p.n0, n1 = p.n1, n2 = KN2 ? KN2 : p.n2;
+    const int pitch = KN2 ? KN2 : g.pitch;
+    const int TJ = KTJ ? KTJ : g.TJ;
     const uint32_t NS = (uint32_t)g.S;
     const int rows = TJ + 2;
     const int tpr = n2 >> 2;
@@ -450,10 +456,12 @@ __global__ void __maxnreg__(kMarchRegs)
     if (p.table_in_smem) stage_table<float>(p, s_tab);  // ends with __syncthreads
     else __syncthreads();
 
-    const size_t plane_blk = (size_t)(g.stage_bytes >> 2);  // one [rows][pitch] block
+    // one [rows][pitch] block (bytes); a stage holds four
+    const size_t plane_blk = KN2 ? (size_t)(KTJ + 2) * KN2 * 4 : (size_t)(g.stage_bytes >> 2);
+    const size_t stage_b = 4 * plane_blk;
     // stage -> field f (0 phi, 1 pi) -> component c (0 hi, 1 lo)
     auto blk = [&](uint32_t stage, int f, int c) -> float* {
-        return reinterpret_cast<float*>(ring + (size_t)stage * g.stage_bytes +
+        return reinterpret_cast<float*>(ring + (size_t)stage * stage_b +
                                         (size_t)(2 * f + c) * plane_blk);
     };
 
@@ -825,6 +833,20 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
         }
         for (int q = 0; q < ni; ++q) {
             const int64_t rowoff = ((int64_t)(i0 + q) * n1 + jw) * n2 + k0;
+            // pi at the thread's own four sites (BAOAB passes), loaded before the
+            // noise so the loads are in flight during it, the wait and the stencil
+            // (the complex first pass, short of registers there, loads after the stencil)
+            constexpr bool kPiEarly = !(CPLX && MODE == kBA1);
+            float4 piv[NF][2];  // [field][hi, lo]
+            const auto load_pi = [&]() {
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    const float* pif = static_cast<const float*>(p.f[NF + f]);
+                    piv[f][0] = *reinterpret_cast<const float4*>(pif + rowoff);
+                    piv[f][1] = *reinterpret_cast<const float4*>(pif + N + rowoff);
+                }
+            };
+            if constexpr (MODE != kOD && kPiEarly) load_pi();
             // the noise reads no tile: drawn before the wait for the next plane
             float2 zz[2][NF];
 #pragma unroll
@@ -887,6 +909,7 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[pm.stage]);  // plane i-1 is no longer read
+            if constexpr (MODE != kOD && !kPiEarly) load_pi();
             float ah[NF][4], al[NF][4], bh[NF][4], bl[NF][4];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -911,10 +934,9 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
                 for (int f = 0; f < NF; ++f) {
                     float vh[2] = {0.0f, 0.0f}, vl[2] = {0.0f, 0.0f};
                     if constexpr (MODE != kOD) {
-                        const float* pif = static_cast<const float*>(p.f[NF + f]);
-                        const float2 a = *reinterpret_cast<const float2*>(pif + rowoff + 2 * h);
-                        const float2 b = *reinterpret_cast<const float2*>(pif + N + rowoff + 2 * h);
-                        vh[0] = a.x; vh[1] = a.y; vl[0] = b.x; vl[1] = b.y;
+                        const float4 a = piv[f][0], b = piv[f][1];
+                        vh[0] = h ? a.z : a.x; vh[1] = h ? a.w : a.y;
+                        vl[0] = h ? b.z : b.x; vl[1] = h ? b.w : b.y;
                     }
                     alt_real_site_f32c<MODE>(p, cen[h][f][0].x, cen[h][f][1].x, dsum[h][f][0].x,
                                              dsum[h][f][1].x, vp[f].x, z[f].x, vh[0], vl[0],
@@ -1157,9 +1179,12 @@ __global__ void __maxnreg__(kMarchRegs)
                     if (c == 0) {  // dh = sum (hi_n - hi_c)
                         acc = v_add(v_add(v_add(v_sub(ip, ce), v_sub(im, ce)), v_sub(jp, ce)),
                                     v_sub(jm, ce));
-                        const float2 kk = make_float2(
-                            __fadd_rn(__fsub_rn(ce.y, ce.x), __fsub_rn(kl, ce.x)),
-                            __fadd_rn(__fsub_rn(kr, ce.y), __fsub_rn(ce.x, ce.y)));
+                        // k pairs from the neighbour differences em, e0, e1: km - c is
+                        // -(the difference on the left) exactly, so (kp - c) + (km - c)
+                        // rounds once as e_right - e_left (the same bits)
+                        const float em = __fsub_rn(ce.x, kl), e0 = __fsub_rn(ce.y, ce.x),
+                                    e1 = __fsub_rn(kr, ce.y);
+                        const float2 kk = make_float2(__fsub_rn(e0, em), __fsub_rn(e1, e0));
                         in.dh[f] = v_add(acc, kk);
                         in.ch[f] = ce;
                     } else {       // dl = fma(-6, lo_c, sum lo_n)
@@ -1429,6 +1454,26 @@ bool ensemble_march_supported(int n0, int n1, int n2) {
     return geometry(TIPT_F32C, p, 0, g, smem);
 }
 
+// Compensated-FP32 stage with a table or polynomial V': the kernel compiled for
+// 512-site rows in 4-row tiles or 256-site rows in 8-row tiles when the run-time
+// geometry is exactly that one (the automatic choice at 512^3 and 256^3), else
+// the run-time-geometry kernel.  Both give the same bits.
+static bool g_fixed_geom = true;  // tipt_set_march_fixed()
+
+template <bool WIDE, bool RG>
+static int launch_f32c_stage(const RealStageParams& q, const MarchGeom& g, int64_t smem,
+                             cudaStream_t st) {
+    const bool exact = g_fixed_geom && g.pitch == q.n2 &&
+                       g.stage_bytes == 4 * (g.TJ + 2) * g.pitch * 4;
+    if (exact && q.n2 == 512 && g.TJ == 4)
+        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false, 512, 4>, q, g, smem, st,
+                              EnsMarch{});
+    if (exact && q.n2 == 256 && g.TJ == 8)
+        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false, 256, 8>, q, g, smem, st,
+                              EnsMarch{});
+    return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false>, q, g, smem, st, EnsMarch{});
+}
+
 int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cudaStream_t st) {
     MarchGeom g;
     int64_t smem;
@@ -1449,10 +1494,10 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
         q.test_withhold = g_test_withhold;
         g_test_withhold = 0;
         if (q.range)
-            return wide ? launch_march_k(rk2_stage_march_f32c<true, false, true, false>, q, g, smem, st, EnsMarch{})
-                        : launch_march_k(rk2_stage_march_f32c<false, false, true, false>, q, g, smem, st, EnsMarch{});
-        return wide ? launch_march_k(rk2_stage_march_f32c<true, false, false, false>, q, g, smem, st, EnsMarch{})
-                    : launch_march_k(rk2_stage_march_f32c<false, false, false, false>, q, g, smem, st, EnsMarch{});
+            return wide ? launch_f32c_stage<true, true>(q, g, smem, st)
+                        : launch_f32c_stage<false, true>(q, g, smem, st);
+        return wide ? launch_f32c_stage<true, false>(q, g, smem, st)
+                    : launch_f32c_stage<false, false>(q, g, smem, st);
     }
     if (storage != TIPT_F32C && p.range)
         return fail(TIPT_ERR_UNSUPPORTED, "the FP64 / float32 marching stage takes no range output");
@@ -1648,6 +1693,13 @@ using namespace tipt;
 extern "C" int tipt_set_march_kseg(int kseg) {
     if (kseg < 0) return fail(TIPT_ERR_ARG, "bad row segment");
     g_force_kseg = kseg;
+    return TIPT_OK;
+}
+
+// Fixed-geometry compensated-FP32 stage kernels (512- and 256-site rows) on or
+// off; performance only (both kernels give the same bits).
+extern "C" int tipt_set_march_fixed(int enable) {
+    g_fixed_geom = enable != 0;
     return TIPT_OK;
 }
 

@@ -147,7 +147,9 @@ __device__ __forceinline__ float2 v_neg(float2 a) { return make_float2(-a.x, -a.
 // 53-bit integers m1, m2 (u = m * 2^-53):
 //  * log(u1), from the halves h1 = m1 >> 32 (< 2^21) and l1 = m1 mod 2^32: the
 //    atanh series of log(1 + g), g = u1 - 1 formed exactly from the halves,
-//    for u1 >= 1/2; the hardware base-2 logarithm for u1 < 1/2 (log_u1 below).
+//    for u1 >= 1/2; the hardware base-2 logarithm for u1 < 1/2 (neg2_log_u1
+//    below, which returns v = -2 log(u1), the factor folded into the last
+//    operation of each branch: an exact scaling by -2).
 //    The reference's clamp u1 >= 1e-12 is applied to the FP32 value of u1.
 //  * the angle 2 pi u2, from the top 31 bits t2 of m2 (u2 = t2 2^-31 to within
 //    2^-31, an angle error below 3e-9): cos alone (real field) by the nearest
@@ -176,7 +178,7 @@ __device__ __forceinline__ void hash_words(uint64_t x, uint32_t& h1, uint32_t& l
 }
 
 
-// log(u1) for one lane from the halves h, l of m1 (u1 = m1 2^-53):
+// -2 log(u1) for one lane from the halves h, l of m1 (u1 = m1 2^-53):
 //  * u1 >= 1/2: g = u1 - 1 = (h - 2^21) 2^-21 + l 2^-53 (exact to 2^-45), and
 //    log(1 + g) = 2 atanh(s), s = g / (2 + g) in [-1/3, 0], summed as
 //    2 s (1 + s^2/3 + ... + s^12/13) (the atanh series, truncated below 1e-8);
@@ -185,6 +187,7 @@ __device__ __forceinline__ void hash_words(uint64_t x, uint32_t& h1, uint32_t& l
 //    error below 2e-7), u1 first clamped to 1e-12 (R:2336).
 // Both are formed and one is selected, so the lanes of a warp do not diverge.
 constexpr float kLn2 = 0.693147182464599609375f;     // ln 2 rounded to FP32
+constexpr float kNeg2Ln2 = -2.0f * kLn2;             // exact
 
 __device__ __forceinline__ float lg2_approx(float x) {
     float y;
@@ -198,10 +201,10 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return y;
 }
 
-// The arithmetic of log_u1 in lane vectors (one or two lanes; the packed
+// The arithmetic of neg2_log_u1 in lane vectors (one or two lanes; the packed
 // instructions round each lane as the scalar ones, so both give the same bits).
 template <typename V>
-__device__ __forceinline__ V log_u1_v(V hf, V lo) {
+__device__ __forceinline__ V neg2_log_u1_v(V hf, V lo) {
     const V g = v_fma(v_sub(hf, vs<V>(0x1p21f)), vs<V>(0x1p-21f), lo);
     const V d = v_add(vs<V>(2.0f), g);
     V r;
@@ -215,39 +218,43 @@ __device__ __forceinline__ V log_u1_v(V hf, V lo) {
     poly = v_fma(w, poly, vs<V>(1.0f / 5.0f));
     poly = v_fma(w, poly, vs<V>(1.0f / 3.0f));
     poly = v_mul(w, poly);
-    const V two_s = v_add(s, s);
-    return v_fma(two_s, poly, two_s);  // log(1 + g): the u1 >= 1/2 branch
+    const V m4s = v_mul(s, vs<V>(-4.0f));
+    return v_fma(m4s, poly, m4s);  // -2 log(1 + g): the u1 >= 1/2 branch
 }
 
-// log(u1) of the u1 < 1/2 branch for one lane from u1 in FP32
-__device__ __forceinline__ float log_far(float u) {
-    return __fmul_rn(lg2_approx(fmaxf(u, 1e-12f)), kLn2);
+// -2 log(u1) of the u1 < 1/2 branch for one lane from u1 in FP32
+__device__ __forceinline__ float neg2_log_far(float u) {
+    return __fmul_rn(lg2_approx(fmaxf(u, 1e-12f)), kNeg2Ln2);
 }
 
-__device__ __forceinline__ float log_u1(uint32_t h, uint32_t l) {
+__device__ __forceinline__ float neg2_log_u1(uint32_t h, uint32_t l) {
     const float lo = __fmul_rn((float)l, 0x1p-53f);
     const float hf = (float)h;  // exact: h < 2^21
-    const float near = log_u1_v<float>(hf, lo);
-    const float far = log_far(__fmaf_rn(hf, 0x1p-21f, lo));
+    const float near = neg2_log_u1_v<float>(hf, lo);
+    const float far = neg2_log_far(__fmaf_rn(hf, 0x1p-21f, lo));
     return h >= (1u << 20) ? near : far;
 }
 
-// log_u1 for two keys in the lanes of a float2.
-__device__ __forceinline__ float2 log_u1_2(uint32_t ha, uint32_t la, uint32_t hb, uint32_t lb) {
+// neg2_log_u1 for two keys in the lanes of a float2.
+__device__ __forceinline__ float2 neg2_log_u1_2(uint32_t ha, uint32_t la, uint32_t hb,
+                                                uint32_t lb) {
     const float2 lo = v_mul(make_float2((float)la, (float)lb), vs<float2>(0x1p-53f));
     const float2 hf = make_float2((float)ha, (float)hb);
-    const float2 near = log_u1_v<float2>(hf, lo);
+    const float2 near = neg2_log_u1_v<float2>(hf, lo);
     const float2 u = v_fma(hf, vs<float2>(0x1p-21f), lo);
-    return make_float2(ha >= (1u << 20) ? near.x : log_far(u.x),
-                       hb >= (1u << 20) ? near.y : log_far(u.y));
+    return make_float2(ha >= (1u << 20) ? near.x : neg2_log_far(u.x),
+                       hb >= (1u << 20) ? near.y : neg2_log_far(u.y));
 }
 
 // Quarter-turn reduction of 2 pi u2 (u2 = t 2^-31): q = round(4 u2) and the
-// remainder x = 2 pi u2 - q pi/2 in [-pi/4, pi/4].
+// remainder x = 2 pi u2 - q pi/2 in [-pi/4, pi/4].  The remainder
+// rh = t - q 2^29 is the low 29 bits of t read as a signed number, so
+// (int)(t << 3) = 8 rh exactly; its conversion is 8 (float)rh and the constant
+// carries the 2^-3, so x is bitwise (float)rh (pi/2) 2^-29.
 __device__ __forceinline__ void angle_reduce(uint32_t t, uint32_t& q, float& x) {
     q = (t + (1u << 28)) >> 29;                        // nearest multiple of 2^29
-    const int rh = (int)t - (int)(q << 29);            // |rh| <= 2^28
-    x = __fmul_rn((float)rh, 0x1.921fb6p-29f /* (pi/2) 2^-29, rounded to FP32 */);
+    const int r8 = (int)(t << 3);                      // 8 rh, |rh| <= 2^28
+    x = __fmul_rn((float)r8, 0x1.921fb6p-32f /* (pi/2) 2^-29 2^-3, rounded to FP32 */);
 }
 
 __device__ __forceinline__ void sincos_series1(float x, float& sn, float& cs) {
@@ -282,9 +289,9 @@ __device__ __forceinline__ void quarter_turn(uint32_t q, float sn, float cs, flo
     s = (qq >= 2u) ? -b : b;
 }
 
+// sqrt(v) for v = -2 log(u1) > 0
 template <typename V>
-__device__ __forceinline__ V radius_from_log(V lg) {
-    const V v = v_mul(vs<V>(-2.0f), lg);  // > 0
+__device__ __forceinline__ V radius_from_v(V v) {
     V y;
     if constexpr (sizeof(V) == 4) y = rsqrtf(v);
     else y = make_float2(rsqrtf(v.x), rsqrtf(v.y));
@@ -294,12 +301,14 @@ __device__ __forceinline__ V radius_from_log(V lg) {
 
 // cos(2 pi u2) alone (the real field draws only the cos branch): half-turn
 // reduction 2 u2 = q + x/pi with q = round(2 u2) in {0, 1, 2} and
-// x in [-pi/2, pi/2], cos = (-1)^q cos x.  Returns the sign bit (q odd) with x.
+// x in [-pi/2, pi/2], cos = (-1)^q cos x.  Returns x and a word whose bit 31 is
+// q's parity (the other bits are not defined).  As in angle_reduce, the
+// remainder rh = t - q 2^30 is the low 30 bits of t read as a signed number:
+// (int)(t << 2) = 4 rh, and the constant carries the 2^-2.
 __device__ __forceinline__ void half_turn_reduce(uint32_t t, uint32_t& sign, float& x) {
-    const uint32_t q = (t + (1u << 29)) >> 30;         // nearest multiple of 2^30
-    const int rh = (int)t - (int)(q << 30);            // |rh| <= 2^29
-    x = __fmul_rn((float)rh, 0x1.921fb6p-29f /* pi 2^-30, rounded to FP32 */);
-    sign = q << 31;                                    // q = 2 shifts out: even
+    const int r4 = (int)(t << 2);                      // 4 rh, |rh| <= 2^29
+    x = __fmul_rn((float)r4, 0x1.921fb6p-31f /* pi 2^-30 2^-2, rounded to FP32 */);
+    sign = (t + (1u << 29)) << 1;                      // bit 31 = bit 30 of t + 2^29 = q & 1
 }
 
 template <typename V>
@@ -313,8 +322,10 @@ __device__ __forceinline__ V cos_series(V x) {
     return v_fma(x2, c, vs<V>(1.0f));
 }
 
+// v with its sign flipped where bit 31 of `sign` is set (the other bits of
+// `sign` are ignored)
 __device__ __forceinline__ float flip_sign(float v, uint32_t sign) {
-    return __uint_as_float(__float_as_uint(v) ^ sign);
+    return __uint_as_float(__float_as_uint(v) ^ (sign & 0x80000000u));
 }
 
 // z (cos branch) for one key, FP32.
@@ -322,9 +333,9 @@ __device__ __forceinline__ float gauss_cos_f(uint64_t key) {
     uint32_t h1, l1, t2, sg;
     hash_words(key, h1, l1, t2);
     float x;
-    const float lg = log_u1(h1, l1);
+    const float v = neg2_log_u1(h1, l1);
     half_turn_reduce(t2, sg, x);
-    return __fmul_rn(radius_from_log<float>(lg), flip_sign(cos_series<float>(x), sg));
+    return __fmul_rn(radius_from_v<float>(v), flip_sign(cos_series<float>(x), sg));
 }
 
 // z for two keys in the two lanes of a float2 (bitwise the same as two calls
@@ -334,12 +345,12 @@ __device__ __forceinline__ float2 gauss_cos_f2(uint64_t key0, uint64_t key1) {
     hash_words(key0, h1a, l1a, t2a);
     hash_words(key1, h1b, l1b, t2b);
     float xa, xb;
-    const float2 lg = log_u1_2(h1a, l1a, h1b, l1b);
+    const float2 v = neg2_log_u1_2(h1a, l1a, h1b, l1b);
     half_turn_reduce(t2a, sa, xa);
     half_turn_reduce(t2b, sb, xb);
     const float2 cx = cos_series<float2>(make_float2(xa, xb));
     const float2 c = make_float2(flip_sign(cx.x, sa), flip_sign(cx.y, sb));
-    return v_mul(radius_from_log<float2>(lg), c);
+    return v_mul(radius_from_v<float2>(v), c);
 }
 
 // (z1, z2) = r (cos, sin) for one key (complex field, one pair per site).
@@ -347,11 +358,11 @@ __device__ __forceinline__ void gauss_pair_f(uint64_t key, float& z1, float& z2)
     uint32_t h1, l1, t2, q;
     hash_words(key, h1, l1, t2);
     float x, sn, cs, c, s;
-    const float lg = log_u1(h1, l1);
+    const float v = neg2_log_u1(h1, l1);
     angle_reduce(t2, q, x);
     sincos_series<float>(x, sn, cs);
     quarter_turn(q, sn, cs, c, s);
-    const float r = radius_from_log<float>(lg);
+    const float r = radius_from_v<float>(v);
     z1 = __fmul_rn(r, c);
     z2 = __fmul_rn(r, s);
 }
@@ -364,7 +375,7 @@ __device__ __forceinline__ void gauss_pair_f2(uint64_t key0, uint64_t key1, floa
     hash_words(key0, h1a, l1a, t2a);
     hash_words(key1, h1b, l1b, t2b);
     float xa, xb;
-    const float2 lg = log_u1_2(h1a, l1a, h1b, l1b);
+    const float2 v = neg2_log_u1_2(h1a, l1a, h1b, l1b);
     angle_reduce(t2a, qa, xa);
     angle_reduce(t2b, qb, xb);
     float2 sn, cs;
@@ -372,7 +383,7 @@ __device__ __forceinline__ void gauss_pair_f2(uint64_t key0, uint64_t key1, floa
     float2 c, s;
     quarter_turn(qa, sn.x, cs.x, c.x, s.x);
     quarter_turn(qb, sn.y, cs.y, c.y, s.y);
-    const float2 r = radius_from_log<float2>(lg);
+    const float2 r = radius_from_v<float2>(v);
     z1 = v_mul(r, c);
     z2 = v_mul(r, s);
 }

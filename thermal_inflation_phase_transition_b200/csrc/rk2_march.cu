@@ -1000,13 +1000,18 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
 // per plane and neighbour) and evaluates them in the two lanes of the packed
 // FP32x2 instructions with the arithmetic of the generic kernel
 // (complex_update_f32c), so the results are bitwise identical.
-template <bool WIDE, bool RG>
+//
+// KKS, KTJ > 0: segments of KKS sites (pitch KKS) in KTJ-row tiles fixed at
+// compile time, as the real stage's fixed geometry (the launcher takes it when
+// the run-time geometry is exactly that one).
+template <bool WIDE, bool RG, int KKS = 0, int KTJ = 0>
 __global__ void __maxnreg__(kMarchRegs)
     complex_stage_march_f32c(const __grid_constant__ CUtensorMap tm0,
                              const __grid_constant__ CUtensorMap tm1,
                              const __grid_constant__ CUtensorMap tm2,
                              const __grid_constant__ CUtensorMap tm3, ComplexStageParams p,
                              MarchGeom g) {
+    static_assert((KKS == 0) == (KTJ == 0) && KKS % 32 == 0, "fixed geometry: KKS and KTJ");
     if constexpr (RG) reset_range_words(p.range_next);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* smem = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
@@ -1016,11 +1021,11 @@ __global__ void __maxnreg__(kMarchRegs)
     unsigned char* ring = smem + g.tab_bytes + 128;
 
     const int n0 = p.n0, n1 = p.n1, n2 = p.n2;
-    const int pitch = g.pitch;
-    const int TJ = g.TJ;
+    const int pitch = KKS ? KKS : g.pitch;
+    const int TJ = KTJ ? KTJ : g.TJ;
     const uint32_t NS = (uint32_t)g.S;
     const int rows = TJ + 2;
-    const int KS = g.KS;
+    const int KS = KKS ? KKS : g.KS;
     const bool split = g.nKS > 1;
     const int tpr = KS >> 1;
     const int nc = TJ * tpr;
@@ -1038,17 +1043,19 @@ __global__ void __maxnreg__(kMarchRegs)
         for (int q = t; q < p.npts; q += blockDim.x) s_tab[q] = (float)__ldg(p.table + q);
     __syncthreads();
 
-    const size_t plane_blk = (size_t)((g.halo_off) >> 3);  // one [rows][pitch] block, bytes
+    // one [rows][pitch] block, bytes; a stage holds eight
+    const size_t plane_blk = KKS ? (size_t)(KTJ + 2) * KKS * 4 : (size_t)((g.halo_off) >> 3);
+    const size_t stage_b = KKS ? 8 * plane_blk : (size_t)g.stage_bytes;
     // stage -> field f (phi1, phi2, pi1, pi2) -> component c (0 hi, 1 lo)
     auto blk = [&](uint32_t stage, int f, int c) -> float* {
-        return reinterpret_cast<float*>(ring + (size_t)stage * g.stage_bytes +
+        return reinterpret_cast<float*>(ring + (size_t)stage * stage_b +
                                         (size_t)(2 * f + c) * plane_blk);
     };
     // split rows: the k-1 neighbour of a segment's first site and the k+1 neighbour of its
     // last site are copied from global memory by the two edge threads of each tile row
     // (cp.async, one plane ahead) into a per-thread double buffer after the ring:
     // [TJ rows][2 sides][2 slots][8 = field x component]
-    float* halo = reinterpret_cast<float*>(ring + (size_t)NS * g.stage_bytes);
+    float* halo = reinterpret_cast<float*>(ring + (size_t)NS * stage_b);
 
     // ------------------------------------------------------------ producer
     if (t >= nc) {
@@ -1700,8 +1707,16 @@ int launch_complex_march(const ComplexStageParams& p, cudaStream_t st) {
     for (int f = 0; f < 4; ++f)
         if (!make_map(&tm[f], p.f[f], 2 * p.n0, p.n1, p.n2, 4, g.BK))
             return fail(TIPT_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    auto kern = p.range ? (wide ? complex_stage_march_f32c<true, true> : complex_stage_march_f32c<false, true>)
-                        : (wide ? complex_stage_march_f32c<true, false> : complex_stage_march_f32c<false, false>);
+    // 256-site segments in 4-row tiles (the automatic choice at 256^3 and 512^3)
+    // compiled with that geometry fixed
+    const bool fixed = g_fixed_geom && g.KS == 256 && g.TJ == 4 && g.pitch == 256 &&
+                       g.halo_off == 8 * 6 * 256 * 4 && g.stage_bytes == g.halo_off;
+    auto kern = fixed ? (p.range ? (wide ? complex_stage_march_f32c<true, true, 256, 4>
+                                         : complex_stage_march_f32c<false, true, 256, 4>)
+                                 : (wide ? complex_stage_march_f32c<true, false, 256, 4>
+                                         : complex_stage_march_f32c<false, false, 256, 4>))
+            : p.range ? (wide ? complex_stage_march_f32c<true, true> : complex_stage_march_f32c<false, true>)
+                      : (wide ? complex_stage_march_f32c<true, false> : complex_stage_march_f32c<false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess)

@@ -145,7 +145,8 @@ def _run_real(kind, shape, policy, vpoly, steps=3):
 
 
 @pytest.mark.parametrize("kind", ["overdamped", "baoab"])
-@pytest.mark.parametrize("shape", [(8, 12, 64), (5, 6, 32), (33, 8, 128), (3, 4, 8)])
+@pytest.mark.parametrize("shape", [(8, 12, 64), (5, 6, 32), (33, 8, 128), (3, 4, 8),
+                                   (4, 8, 512)])  # 512-site rows: the fixed-geometry kernels
 @pytest.mark.parametrize("vpoly", [None, (-0.02, -0.15, 0.1)])
 def test_real_integrators_marching_equals_generic(kind, shape, vpoly):
     """Compensated FP32 with nz % 4 == 0 runs on the marching ring: bitwise the
@@ -196,7 +197,7 @@ def _run_complex(kind, shape, policy, vpoly, zn, eps4, steps=3):
 
 
 @pytest.mark.parametrize("kind", ["overdamped", "baoab"])
-@pytest.mark.parametrize("shape", [(8, 12, 64), (5, 6, 32), (3, 4, 8)])
+@pytest.mark.parametrize("shape", [(8, 12, 64), (5, 6, 32), (3, 4, 8), (4, 8, 512)])
 @pytest.mark.parametrize("vpoly,zn,eps4", [(None, (0.0, 0.0, 0.0), 1e-3),
                                            ((-0.02, -0.15, 0.1), (0.0, 0.0, 0.0), 0.0),
                                            (None, (4.0, 0.01, 1.0), 0.0)])

@@ -750,7 +750,9 @@ __global__ void __maxnreg__(kMarchRegs)
 // give the same bits.
 // SRC: kCsrcAny dispatches on the V' source at run time; kCsrcTab (and, for the
 // complex force, kCsrcTabEps) fix the staged table at compile time.
-template <int MODE, bool CPLX, bool WIDE, int SRC = kCsrcAny>
+// KN2, KTJ > 0: rows of KN2 sites in KTJ-row tiles fixed at compile time (as
+// the RK2 stage's fixed geometry).
+template <int MODE, bool CPLX, bool WIDE, int SRC = kCsrcAny, int KN2 = 0, int KTJ = 0>
 __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g) {
     constexpr int NF = CPLX ? 2 : 1;  // stencil fields
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -760,9 +762,9 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
     uint64_t* empty = full + 8;
     unsigned char* ring = smem + g.tab_bytes + 128;
 
-    const int n0 = p.n0, n1 = p.n1, n2 = p.n2;
-    const int pitch = g.pitch;
-    const int TJ = g.TJ;
+    const int n0 = p.n0, n1 = p.n1, n2 = KN2 ? KN2 : p.n2;
+    const int pitch = KN2 ? KN2 : g.pitch;
+    const int TJ = KTJ ? KTJ : g.TJ;
     const uint32_t NS = (uint32_t)g.S;
     const int rows = TJ + 2;
     const int tpr = n2 >> 2;
@@ -780,9 +782,12 @@ __global__ void __maxnreg__(kMarchRegs) alt_march_f32c(AltParams p, MarchGeom g)
         for (int q = t; q < p.v.npts; q += blockDim.x) s_tab[q] = (float)__ldg(p.v.table + q);
     __syncthreads();
 
-    const size_t plane_blk = (size_t)(g.stage_bytes / (2 * NF));  // one [rows][pitch] block
+    // one [rows][pitch] block (bytes); a stage holds 2 NF
+    const size_t plane_blk =
+        KN2 ? (size_t)(KTJ + 2) * KN2 * 4 : (size_t)(g.stage_bytes / (2 * NF));
+    const size_t stage_b = KN2 ? 2 * NF * plane_blk : (size_t)g.stage_bytes;
     auto blk = [&](uint32_t stage, int f, int c) -> float* {     // field f, c: 0 hi, 1 lo
-        return reinterpret_cast<float*>(ring + (size_t)stage * g.stage_bytes +
+        return reinterpret_cast<float*>(ring + (size_t)stage * stage_b +
                                         (size_t)(2 * f + c) * plane_blk);
     };
 
@@ -1576,7 +1581,18 @@ static int launch_alt_march_k(const AltParams& p, cudaStream_t st) {
     // force with or without the eps term)
     const bool tab = p.v.vkind != TIPT_VP_POLY && p.v.table_in_smem;
     const int src = !tab ? kCsrcAny : (CPLX && p.v.eps4 != 0.0) ? kCsrcTabEps : kCsrcTab;
-    auto kern = src == kCsrcTab
+    // rows of 512 sites in 4-row tiles (the automatic choice at 512^3) with the
+    // staged table: the geometry fixed at compile time as well
+    constexpr int NF = CPLX ? 2 : 1;
+    const bool fixed = g_fixed_geom && tab && p.n2 == 512 && g.pitch == 512 && g.TJ == 4 &&
+                       g.stage_bytes == 2 * NF * 6 * 512 * 4;
+    constexpr int TS = CPLX ? kCsrcTabEps : kCsrcTab;
+    auto kern = fixed ? (src == kCsrcTab
+                             ? (wide ? alt_march_f32c<MODE, CPLX, true, kCsrcTab, 512, 4>
+                                     : alt_march_f32c<MODE, CPLX, false, kCsrcTab, 512, 4>)
+                             : (wide ? alt_march_f32c<MODE, CPLX, true, TS, 512, 4>
+                                     : alt_march_f32c<MODE, CPLX, false, TS, 512, 4>))
+                : src == kCsrcTab
                     ? (wide ? alt_march_f32c<MODE, CPLX, true, kCsrcTab>
                             : alt_march_f32c<MODE, CPLX, false, kCsrcTab>)
                 : src == kCsrcTabEps

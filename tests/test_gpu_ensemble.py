@@ -116,6 +116,26 @@ def test_single_lattice_poly_vs_oracle(storage):
     assert err < TOL[storage], err
 
 
+def test_marching_fixed_geometry_classes_equal_chunk_kernel():
+    """The configuration's 3-D classes (64-site rows in 32-row tiles, 96-site rows in
+    16-row tiles) run kernels compiled for their geometry: bitwise the chunk
+    kernel's result."""
+    specs = ([EN.ReplicaSpec((8, 64, 64), 0.99 + 0.004 * r, 0.05, 90 + r) for r in range(2)]
+             + [EN.ReplicaSpec((6, 96, 96), 1.0, 0.045, 95 + r) for r in range(2)])
+    kw = dict(storage="f32c", stop_frac=0.5, retire_frac=0.5, check_every=5, init_seed=6)
+    a = EN.Ensemble(specs, use_march=True, **kw)
+    b = EN.Ensemble(specs, use_march=False, **kw)
+    assert len(a._march) == 2
+    fa = a.run(20, poll_every=1)
+    fb = b.run(20, poll_every=1)
+    assert np.array_equal(fa, fb)
+    for r in range(len(specs)):
+        x, y = a.replica_state(r), b.replica_state(r)
+        assert torch.equal(x[0], y[0]) and torch.equal(x[1], y[1]), r
+    from thermal_inflation_phase_transition_b200 import _lib as L
+    assert L.device_status() == 0
+
+
 @pytest.mark.parametrize("storage", ["f32c"])
 def test_marching_classes_equal_chunk_kernel(storage):
     """Replicas of the 3-D shape classes step on the marching stage (shared-memory

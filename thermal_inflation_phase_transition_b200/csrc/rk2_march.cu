@@ -1294,6 +1294,9 @@ static bool make_map(CUtensorMap* tm, const void* base, int planes, int n1, int 
 
 // Tile shape; 0 = choose automatically.  Set by tipt_set_march_tiles().
 static int g_force_tj = 0, g_force_ci = 0, g_force_stages = 0;
+// Kernels compiled for a fixed geometry used where the run-time geometry is
+// theirs (tipt_set_march_fixed(); on by default).
+static bool g_fixed_geom = true;
 
 // One-shot test of the bounded waits (tipt_test_withhold_plane): the next
 // compensated-FP32 marching stage launch withholds a ring position in block 0.
@@ -1468,6 +1471,16 @@ int launch_ensemble_march(const RealStageParams& p_in, const tipt_replica* reps,
     g.items *= n_rids;
     // 64-bit noise-key sites when a replica's site index can exceed 32 bits
     const bool wide = (int64_t)p.n0 * p.n1 * p.n2 > 0xFFFFFFFFll;
+    // the classes of the batched configuration (64^3: 32-row tiles, 96^3: 16-row
+    // tiles) run kernels compiled for their geometry
+    const bool exact = g_fixed_geom && !wide && g.pitch == p.n2 &&
+                       g.stage_bytes == 4 * (g.TJ + 2) * g.pitch * 4;
+    if (exact && p.n2 == 64 && g.TJ == 32)
+        return launch_march_k(rk2_stage_march_f32c<false, false, false, true, 64, 32>, p, g, smem, st,
+                              em);
+    if (exact && p.n2 == 96 && g.TJ == 16)
+        return launch_march_k(rk2_stage_march_f32c<false, false, false, true, 96, 16>, p, g, smem, st,
+                              em);
     return wide ? launch_march_k(rk2_stage_march_f32c<true, false, false, true>, p, g, smem, st, em)
                 : launch_march_k(rk2_stage_march_f32c<false, false, false, true>, p, g, smem, st, em);
 }
@@ -1492,8 +1505,6 @@ bool ensemble_march_supported(int n0, int n1, int n2) {
 // exactly that one (the automatic choice at 512^3 and 256^3), else the
 // run-time-geometry TAB kernel; otherwise the dispatching kernel.  All give the
 // same bits.
-static bool g_fixed_geom = true;  // tipt_set_march_fixed()
-
 template <bool WIDE, bool RG>
 static int launch_f32c_stage(const RealStageParams& q, const MarchGeom& g, int64_t smem,
                              cudaStream_t st) {

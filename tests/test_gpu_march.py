@@ -122,8 +122,11 @@ def test_march_tilings_agree(tiles):
     assert torch.equal(ref[0], got[0]) and torch.equal(ref[1], got[1])
 
 
-def test_march_2d_table():
-    shape = (20, 12, 96)
+@pytest.mark.parametrize("shape", [(20, 12, 96), (8, 16, 512), (6, 16, 256)])
+def test_march_2d_table(shape):
+    """The generic kernel (the FP32 row staged as values) against the marching
+    kernel (the specialised forms stage (value, slope) pairs; 512- and 256-site
+    rows take the fixed-geometry kernels)."""
     ref = _run(1, shape, "f32c", table2d=True)
     got = _run(2, shape, "f32c", table2d=True)
     assert torch.equal(ref[0], got[0]) and torch.equal(ref[1], got[1])

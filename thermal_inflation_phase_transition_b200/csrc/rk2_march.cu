@@ -459,7 +459,8 @@ __global__ void __maxnreg__(kMarchRegs)
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (p.table_in_smem) stage_table<float>(p, s_tab);  // ends with __syncthreads
+    if constexpr (TAB) stage_table_pairs(p, reinterpret_cast<float2*>(s_tab));  // (value, slope)
+    else if (p.table_in_smem) stage_table<float>(p, s_tab);  // ends with __syncthreads
     else __syncthreads();
 
     // one [rows][pitch] block (bytes); a stage holds four
@@ -644,8 +645,9 @@ __global__ void __maxnreg__(kMarchRegs)
                 else if constexpr (TAB)  // the V' row staged in shared memory: vprime_v's branch
                     pre[h] = pre_f32c_vp<float2>(p, pick(cen[0][0]), pick(cen[0][1]), pick(cen[1][0]),
                                                  pick(cen[1][1]), [&](float2 x) {
-                                                     return lerp_table_f32<float2>(
-                                                         s_tab, v_fma(x, p.k2.dinv, p.k2.tmd), kc.last);
+                                                     return lerp_pairs_f32<float2>(
+                                                         reinterpret_cast<const float2*>(s_tab),
+                                                         v_fma(x, p.k2.dinv, p.k2.tmd), kc.last);
                                                  });
                 else
                     pre[h] = pre_f32c<float2, TH>(p, kc, s_tab, pick(cen[0][0]), pick(cen[0][1]),
@@ -1506,12 +1508,15 @@ bool ensemble_march_supported(int n0, int n1, int n2) {
 // run-time-geometry TAB kernel; otherwise the dispatching kernel.  All give the
 // same bits.
 template <bool WIDE, bool RG>
-static int launch_f32c_stage(const RealStageParams& q, const MarchGeom& g, int64_t smem,
-                             cudaStream_t st) {
+static int launch_f32c_stage(const RealStageParams& q, const MarchGeom& g0, int64_t smem0,
+                             int64_t smem_table, cudaStream_t st) {
     const bool tab = q.table_in_smem && (q.vkind == TIPT_VP_TABLE || q.vkind == TIPT_VP_TABLE2D) &&
                      !q.noise;
-    if (!tab)
-        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false>, q, g, smem, st,
+    // the TAB kernels stage the row as (value, slope) pairs: twice the table bytes
+    MarchGeom g;
+    int64_t smem;
+    if (!tab || !geometry(TIPT_F32C, q, 2 * smem_table, g, smem))
+        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false>, q, g0, smem0, st,
                               EnsMarch{});
     const bool exact = g_fixed_geom && g.pitch == q.n2 &&
                        g.stage_bytes == 4 * (g.TJ + 2) * g.pitch * 4;
@@ -1545,10 +1550,10 @@ int launch_march(int storage, const RealStageParams& p, int64_t smem_table, cuda
         q.test_withhold = g_test_withhold;
         g_test_withhold = 0;
         if (q.range)
-            return wide ? launch_f32c_stage<true, true>(q, g, smem, st)
-                        : launch_f32c_stage<false, true>(q, g, smem, st);
-        return wide ? launch_f32c_stage<true, false>(q, g, smem, st)
-                    : launch_f32c_stage<false, false>(q, g, smem, st);
+            return wide ? launch_f32c_stage<true, true>(q, g, smem, smem_table, st)
+                        : launch_f32c_stage<false, true>(q, g, smem, smem_table, st);
+        return wide ? launch_f32c_stage<true, false>(q, g, smem, smem_table, st)
+                    : launch_f32c_stage<false, false>(q, g, smem, smem_table, st);
     }
     if (storage != TIPT_F32C && p.range)
         return fail(TIPT_ERR_UNSUPPORTED, "the FP64 / float32 marching stage takes no range output");

@@ -114,23 +114,42 @@ __device__ __forceinline__ void table2d_row(const RealStageParams& p, int& it, d
 // Stage the V' row into shared memory as TT (blending the two bracketing T
 // rows for a 2-D table).  Called by every thread of the block; ends with a
 // barrier.
+// Entry q of the row: the 1-D table's value, or the blend of the 2-D table's
+// bracketing rows a = it and a + 1 with weight w.
+__device__ __forceinline__ double staged_value(const RealStageParams& p, const double* a, double w,
+                                               int q) {
+    if (p.vkind == TIPT_VP_TABLE) return __ldg(p.table + q);
+    const double va = __ldg(a + q), vb = __ldg(a + p.npts + q);
+    return va + w * (vb - va);
+}
+
 template <typename TT>
 __device__ __forceinline__ void stage_table(const RealStageParams& p, TT* s_tab) {
-    if (p.vkind == TIPT_VP_TABLE) {
+    if (p.vkind == TIPT_VP_TABLE || p.vkind == TIPT_VP_TABLE2D) {
+        int it = 0;
+        double w = 0.0;
+        if (p.vkind == TIPT_VP_TABLE2D) table2d_row(p, it, w);
+        const double* a = p.table + (int64_t)it * p.npts;
         for (int q = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
              q < p.npts; q += blockDim.x * blockDim.y * blockDim.z)
-            s_tab[q] = (TT)__ldg(p.table + q);
-    } else if (p.vkind == TIPT_VP_TABLE2D) {
-        int it;
-        double w;
-        table2d_row(p, it, w);
-        const double* a = p.table + (int64_t)it * p.npts;
-        const double* b = a + p.npts;
-        for (int q = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-             q < p.npts; q += blockDim.x * blockDim.y * blockDim.z) {
-            double va = __ldg(a + q), vb = __ldg(b + q);
-            s_tab[q] = (TT)(va + w * (vb - va));
-        }
+            s_tab[q] = (TT)staged_value(p, a, w, q);
+    }
+    __syncthreads();
+}
+
+// The FP32 row as (value, slope) pairs for lerp_pairs_f32: pair q holds the FP32
+// value v[q] of stage_table<float> and v[q+1] - v[q] rounded to FP32 (q < npts - 1;
+// the lookup never reads the last pair's slope).  Twice the shared memory.
+__device__ __forceinline__ void stage_table_pairs(const RealStageParams& p, float2* s_tab2) {
+    int it = 0;
+    double w = 0.0;
+    if (p.vkind == TIPT_VP_TABLE2D) table2d_row(p, it, w);
+    const double* a = p.table + (int64_t)it * p.npts;
+    for (int q = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); q < p.npts;
+         q += blockDim.x * blockDim.y * blockDim.z) {
+        const float v = (float)staged_value(p, a, w, q);
+        const float d = q + 1 < p.npts ? __fsub_rn((float)staged_value(p, a, w, q + 1), v) : 0.0f;
+        s_tab2[q] = make_float2(v, d);
     }
     __syncthreads();
 }

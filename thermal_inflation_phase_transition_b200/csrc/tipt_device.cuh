@@ -476,6 +476,27 @@ __device__ __forceinline__ V lerp_table_f32(const float* s_tab, V fidx, float la
     return v_fma(v_sub(fidx, fi), v_sub(b, a), a);
 }
 
+// The same lookup from a table of (value, slope) pairs, slope[q] = v[q+1] - v[q]
+// rounded to FP32 when the table is staged: one 8-byte load per lane, and the
+// bits of lerp_table_f32 (its b - a is that same FP32 difference).
+template <typename V>
+__device__ __forceinline__ V lerp_pairs_f32(const float2* s_tab2, V fidx, float last) {
+    constexpr int NL = sizeof(V) / sizeof(float);
+    V c;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) vset(c, l, fminf(fmaxf(vlane(fidx, l), 0.0f), last));
+    const V t = v_add_rz(c, vs<V>(0x1p23f));
+    V a, d;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        const float2 e = s_tab2[__float_as_uint(vlane(t, l)) - 0x4B000000u];
+        vset(a, l, e.x);
+        vset(d, l, e.y);
+    }
+    const V fi = v_sub(t, vs<V>(0x1p23f));
+    return v_fma(v_sub(fidx, fi), d, a);
+}
+
 // Polynomial V'(x) = c1 x + c2 x^2 + c3 x^3 (zero-coupling inline V', R:2228:
 // dV = lam*ph*ph*ph - mphi_sq*ph, evaluated in that order).
 template <typename R>

@@ -544,10 +544,12 @@ int tipt_set_kernel_policy(int policy);
  * stages (each 0 = automatic).  Performance only; used by the autotuner. */
 int tipt_set_march_tiles(int rows, int planes, int stages);
 
-/* Compensated-FP32 marching stage kernels compiled for a fixed geometry (rows
- * of 512 sites in 4-row tiles, 256 sites in 8-row tiles), used when the
- * automatic geometry is one of them: enable != 0 (the default) or 0 for the
- * run-time-geometry kernel.  Performance only: both give the same bits. */
+/* Compensated-FP32 marching kernels compiled for a fixed geometry, used when the
+ * automatic geometry is theirs: the real stage (rows of 512 sites in 4-row
+ * tiles, 256 sites in 8-row tiles), the complex stage (256-site segments in
+ * 4-row tiles), the integrators (512 sites, 4 rows) and the ensemble classes
+ * (64 sites, 32 rows; 96 sites, 16 rows).  enable != 0 (the default) or 0 for
+ * the run-time-geometry kernels.  Performance only: both give the same bits. */
 int tipt_set_march_fixed(int enable);
 
 /* Row segment of the complex marching kernel (sites per segment, a divisor of

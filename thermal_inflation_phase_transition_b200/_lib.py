@@ -199,8 +199,8 @@ def set_march_tiles(rows: int = 0, planes: int = 0, stages: int = 0) -> None:
 
 
 def set_march_fixed(enable: bool) -> None:
-    """Fixed-geometry compensated-FP32 stage kernels (512- / 256-site rows) on or off;
-    performance only (tests/tuning)."""
+    """Compensated-FP32 marching kernels compiled for fixed geometries (real, complex,
+    integrator and ensemble-class stages) on or off; performance only (tests/tuning)."""
     call("tipt_set_march_fixed", int(bool(enable)))
 
 

@@ -282,8 +282,9 @@ def test_complex_march_row_segments_equal_generic(shape, kseg, tiles):
 
 
 def test_bounded_wait_expires_and_reports():
-    """A plane that never arrives: block 0's producer withholds ring position 5 (no
-    copy is issued for it or after it, so none is left in flight).  Its consumers'
+    """A plane that never arrives: block 0's producer withholds ring position 1, the
+    first plane its consumers compute (no copy is issued for it or after it, so none
+    is left in flight; every block's work needs at least positions 0-2).  Its consumers'
     bounded waits run out, the launch returns, the device status reads
     TIPT_ERR_TIMEOUT (6), and the context stays usable: the next steps on it equal
     the generic kernel's bit for bit and leave the status clear."""
@@ -294,7 +295,7 @@ def test_bounded_wait_expires_and_reports():
     t1, tmin, dinv = O.build_table(lambda x: O.toy_vprime(x, 1.01), 0.0, 3.0, 4096)
     vs = table_source(torch.from_numpy(t1).to(DEV), tmin, dinv, 4096)
     po, qo = torch.empty_like(phi), torch.empty_like(pi)
-    L.test_withhold_plane(5)
+    L.test_withhold_plane(1)
     RF.rk2_step_table_into(phi, pi, po, qo, 0.05, 1.0, 0.9, 1.0, 1.0, vs, noise_scale=0.3,
                            noise_step=0, seed=7)
     torch.cuda.synchronize()

@@ -128,6 +128,11 @@ struct MarchGeom {
     int items;
     int tab_bytes;    // staged V' row (bytes, 128-aligned)
     int stage_bytes;  // one ring stage: phi and pi tiles
+    // compensated-FP32 single-lattice stage only: 1 = each CTA takes an equal
+    // share of the nJB x planes (j-block, plane) units, j-block major, as one or
+    // more runs of planes (items is then the number of units); 0 = items of CI
+    // planes.  Every geometry starts with 0; only launch_f32c_stage sets it.
+    int bal = 0;
     // complex kernel: rows split into nKS segments of KS sites (with nKS > 1 the
     // k-1 / k+1 neighbours of a segment's end sites are copied by the edge
     // threads); halo_off = bytes of the eight plane blocks of a stage
@@ -403,6 +408,30 @@ struct EnsMarch {
     long long offset;
 };
 
+// The runs of planes of one CTA under MarchGeom::bal: CTA b of G takes the units
+// [U b / G, U (b + 1) / G) of the U = nJB x planes (j-block, plane) units, j-block
+// major, split where a j-block ends.  Producer and consumers walk the same runs.
+struct BalRun {
+    int64_t u, u_end;
+    int npl, i_begin;
+    __device__ __forceinline__ BalRun(const MarchGeom& g, const RealStageParams& p, int b, int G) {
+        npl = p.i_end - p.i_begin;
+        i_begin = p.i_begin;
+        const int64_t U = (int64_t)g.nJB * npl;
+        u = g.bal ? U * b / G : 0;
+        u_end = g.bal ? U * (b + 1) / G : 0;
+    }
+    __device__ __forceinline__ bool more() const { return u < u_end; }
+    // the next run: j-block jb, first plane i0, ni planes
+    __device__ __forceinline__ void next(int& jb, int& i0, int& ni) {
+        jb = (int)(u / npl);
+        const int off = (int)(u - (int64_t)jb * npl);
+        ni = (int)min((int64_t)(npl - off), u_end - u);
+        i0 = i_begin + off;
+        u += ni;
+    }
+};
+
 // Planar compensated-FP32 marching kernel.  Same ring, roles and work items as
 // rk2_stage_march; a field is two FP32 planes (hi, then lo N sites later), so
 // the TMA map spans 2*n0 planes and a ring stage holds [phi, pi][hi, lo]
@@ -489,7 +518,9 @@ __global__ void __maxnreg__(kMarchRegs)
         if constexpr (ENS) {
             if (em.n_rids) n_items = min(g.items, *em.n_rids * em.items_per_rep);
         }
-        for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
+        BalRun br(g, p, blockIdx.x, gridDim.x);
+        for (int item = blockIdx.x; ((!ENS && g.bal) ? br.more() : item < n_items) && ok;
+             item += gridDim.x) {
             int it = item;
             const float *phi_hi = src_phi, *phi_lo = src_phi + plane_n;
             const float *pi_hi = src_pi, *pi_lo = src_pi + plane_n;
@@ -508,9 +539,17 @@ __global__ void __maxnreg__(kMarchRegs)
                 pi_hi = src_pi + off;
                 pi_lo = src_pi + em.n_total + off;
             }
-            const int ic = it / g.nJB;
-            const int j0 = (it - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
-            const int npl = min(g.CI, p.i_end - i0) + 2;
+            int j0, i0, ni;
+            if (!ENS && g.bal) {
+                br.next(j0, i0, ni);
+                j0 *= TJ;
+            } else {
+                const int ic = it / g.nJB;
+                j0 = (it - ic * g.nJB) * TJ;
+                i0 = p.i_begin + ic * g.CI;
+                ni = min(g.CI, p.i_end - i0);
+            }
+            const int npl = ni + 2;
             for (int q = 0; q < npl; ++q) {
                 if (issued == stop_at) {  // nothing is issued from here on
                     ok = false;
@@ -566,7 +605,8 @@ __global__ void __maxnreg__(kMarchRegs)
     if constexpr (ENS) {
         if (em.n_rids) n_items = min(g.items, *em.n_rids * em.items_per_rep);
     }
-    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    BalRun br(g, p, blockIdx.x, gridDim.x);  // the producer's sequence of runs
+    for (int item = blockIdx.x; (!ENS && g.bal) ? br.more() : item < n_items; item += gridDim.x) {
         int it = item;
         if constexpr (ENS) {
             const int rl = item / em.items_per_rep;
@@ -585,9 +625,16 @@ __global__ void __maxnreg__(kMarchRegs)
             kc.ns = (float)rp.noise_scale;
             eseed = rp.seed;
         }
-        const int ic = it / g.nJB;
-        const int j0 = (it - ic * g.nJB) * TJ, i0 = p.i_begin + ic * g.CI;
-        const int ni = min(g.CI, p.i_end - i0);
+        int j0, i0, ni;
+        if (!ENS && g.bal) {
+            br.next(j0, i0, ni);
+            j0 *= TJ;
+        } else {
+            const int ic = it / g.nJB;
+            j0 = (it - ic * g.nJB) * TJ;
+            i0 = p.i_begin + ic * g.CI;
+            ni = min(g.CI, p.i_end - i0);
+        }
         const int jw = j0 + r - 1;
         RingPos pc = pm, pp;
         pc.next(NS);
@@ -1299,6 +1346,8 @@ static int g_force_tj = 0, g_force_ci = 0, g_force_stages = 0;
 // Kernels compiled for a fixed geometry used where the run-time geometry is
 // theirs (tipt_set_march_fixed(); on by default).
 static bool g_fixed_geom = true;
+// The compensated-FP32 stage's balanced split of the work (MarchGeom::bal).
+static bool g_balance = true;
 
 // One-shot test of the bounded waits (tipt_test_withhold_plane): the next
 // compensated-FP32 marching stage launch withholds a ring position in block 0.
@@ -1354,6 +1403,7 @@ static bool geometry_dims(int n1, int n2, int nplanes, int es, int comps, int64_
     g.tab_bytes = round128((int)smem_table);
     g.CI = g_force_ci > 0 ? g_force_ci : 64;
     if (g.CI > nplanes) g.CI = nplanes;
+    g.bal = 0;
     // Candidates: TJ with TJ*tpr consumers a multiple of 32 in [32, 512], ring
     // depth S in [3, 5].  Score = consumer warps per SM x TJ/(TJ+2) (the share
     // of loaded rows that are not halo), deeper rings preferred on ties.
@@ -1458,6 +1508,7 @@ int launch_ensemble_march(const RealStageParams& p_in, const tipt_replica* reps,
         g.nIC = (p.n0 + g.CI - 1) / g.CI;
         g.items = g.nJB * g.nIC;
     }
+    g.bal = 0;  // replica work items only
     EnsMarch em;
     em.reps = reps;
     em.rids = rids;
@@ -1512,12 +1563,27 @@ static int launch_f32c_stage(const RealStageParams& q, const MarchGeom& g0, int6
                              int64_t smem_table, cudaStream_t st) {
     const bool tab = q.table_in_smem && (q.vkind == TIPT_VP_TABLE || q.vkind == TIPT_VP_TABLE2D) &&
                      !q.noise;
+    // lattices with fewer CI-plane items than SMs: every CTA an equal share of the
+    // (j-block, plane) units, so every SM works.  (With more items the round-robin
+    // items stay: they keep the CTAs of neighbouring j-blocks at the same planes,
+    // so a tile's halo rows are still in L2 from the neighbour's reads; the
+    // j-block-major shares lose that reuse and measured 6 % slower at 512^3.)
+    const auto balance = [&](MarchGeom& b) {
+        if (!g_balance || b.items >= num_sms()) return;
+        b.bal = 1;
+        const int64_t units = (int64_t)b.nJB * (q.i_end - q.i_begin);
+        b.items = units < 0x7FFFFFFF ? (int)units : 0x7FFFFFFF;
+    };
     // the TAB kernels stage the row as (value, slope) pairs: twice the table bytes
     MarchGeom g;
     int64_t smem;
-    if (!tab || !geometry(TIPT_F32C, q, 2 * smem_table, g, smem))
-        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false>, q, g0, smem0, st,
+    if (!tab || !geometry(TIPT_F32C, q, 2 * smem_table, g, smem)) {
+        MarchGeom b = g0;
+        balance(b);
+        return launch_march_k(rk2_stage_march_f32c<WIDE, false, RG, false>, q, b, smem0, st,
                               EnsMarch{});
+    }
+    balance(g);
     const bool exact = g_fixed_geom && g.pitch == q.n2 &&
                        g.stage_bytes == 4 * (g.TJ + 2) * g.pitch * 4;
     if (exact && q.n2 == 512 && g.TJ == 4)

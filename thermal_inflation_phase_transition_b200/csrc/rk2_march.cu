@@ -1847,8 +1847,9 @@ extern "C" int tipt_set_march_kseg(int kseg) {
     return TIPT_OK;
 }
 
-// Fixed-geometry compensated-FP32 stage kernels (512- and 256-site rows) on or
-// off; performance only (both kernels give the same bits).
+// The compensated-FP32 marching kernels compiled for fixed geometries (real and
+// complex stages, integrators, ensemble classes) on or off; performance only
+// (they give the run-time-geometry kernels' bits).
 extern "C" int tipt_set_march_fixed(int enable) {
     g_fixed_geom = enable != 0;
     return TIPT_OK;

@@ -87,3 +87,35 @@ def test_fullsize_step_vs_oracle(setup):
     gq = (got_pi[0].double() + got_pi[1].double()).cpu().numpy()
     assert np.abs(gp - a).max() <= 2e-6 * np.abs(a).max()
     assert np.abs(gq - b).max() <= 2e-6 * max(np.abs(b).max(), 1.0)
+
+
+def test_fullsize_complex_marching_equals_generic(setup):
+    """The complex-field configuration at full size (512^3, V'(|Phi|) table + eps Re Phi^4,
+    hash noise): the marching kernel the complex bench times (256-site segments in
+    4-row tiles, compiled for that geometry) equals the generic kernel bit for bit."""
+    from thermal_inflation_phase_transition_b200 import complex_field as CF
+    t1, tmin, dinv = O.build_table(lambda x: O.toy_vprime_rho(x, 0.98), 0.0, 3.0, 4096)
+    vs = table_source(torch.from_numpy(t1).to(DEV), tmin, dinv, 4096)
+    g = torch.Generator(device=DEV)
+    g.manual_seed(77)
+    init = [RF.to_f32c(0.4 * torch.randn((N, N, N), dtype=torch.float64, device=DEV, generator=g))
+            for _ in range(4)]
+    res = []
+    for policy in (1, 2):
+        L.set_kernel_policy(policy)
+        if policy == 2:  # the complex bench's tiles: 4 rows, 128 planes, 4 stages, 256-site segments
+            L.set_march_tiles(4, 128, 4)
+            L.set_march_kseg(256)
+        a = [x.clone() for x in init]
+        b = [torch.empty_like(x) for x in init]
+        CF.rk2_step_table_into(a, b, DT, DX, ETA, 1.0, 1.0, vs, eps4=1e-3,
+                               noise_scale=math.sqrt(2 * ETA * 0.98 * DT), noise_step=3, seed=2)
+        torch.cuda.synchronize()
+        res.append(b)
+        del a
+    L.set_kernel_policy(0)
+    L.set_march_tiles(0, 0, 0)
+    L.set_march_kseg(0)
+    for x, y in zip(*res):
+        assert torch.equal(x, y)
+    assert L.device_status() == 0
